@@ -1,0 +1,312 @@
+"""Benchmark of the RK4 Hall-MHD step (the reference's stepon/setdt loop, t3dsdsc.f:136-202).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dasha|reference]
+                    [--config c0..c4] [--precision fp32|fp64]
+
+One "step" is one RK4 step (setdt + stepon) of the whole grid.  Default workload: the largest
+precision-form throughput configuration, 1024x512x1024 sinh-stretched Harris sheet, FP32
+perturbation state with Kahan-compensated RK4, Hall on, filter every step.  The inputs (8
+fields, 17 GB in FP32) are far larger than L2, so no L2 flush is needed between steps.
+
+`value`  cell-updates/s on the device: CUDA events on the library's stream around K steps.
+`e2e`    the same metric through the C-ABI with host buffers, the reference's main loop as a
+         Fortran caller runs it: dasha_set_state from host memory, K x (dasha_setdt with its
+         dt read-back + dasha_stepon), dasha_get_state back to host memory.
+Multi-GPU: the path does not shard (one on-device domain), so N ranks run N replicas;
+`value` is the total over ranks and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RK4 cell-updates/s"
+A_STEP = {"fp32": 768.0, "fp64": 1408.0}            # algorithmic bytes per cell-update
+A_FILTER = {"fp32": 64.0, "fp64": 128.0}            # post-step filter, per application
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def pin_device(local_rank: int, world: int):
+    """Give each rank its own GPU before the CUDA runtime of libdasha starts."""
+    if world <= 1:
+        return
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    devs = vis.split(",") if vis else [str(i) for i in range(64)]
+    os.environ["CUDA_VISIBLE_DEVICES"] = devs[local_rank]
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self):
+        self.p = None
+        self.path = os.path.join("/tmp", f"dasha_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            idx = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]
+            self.p = subprocess.Popen(["nvidia-smi", "-i", idx, f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_state(cfg):
+    from dasha_b200 import harris
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
+    H = harris.gem_state_halo(x, y, z, threads=os.cpu_count() or 8)
+    return x, y, z, H
+
+
+def make_ctx(cfg, precision, x, y, z, H):
+    from dasha_b200 import capi, harris
+    d = capi.Dasha(x, y, z, capi.make_params(cfg, 0 if precision == "fp64" else 1))
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    d.set_equilibrium(rho0, b0, p0)
+    d.set_state_halo(H)
+    return d
+
+
+def cpu_port_rate(steps=2, grid=(256, 128, 256), warm=0):
+    """The CPU oracle (port of the reference) on the host cores: cell-updates/s."""
+    from dasha_b200 import harris
+    from oracle.oracle import gem_oracle
+    import dataclasses
+    cfg = dataclasses.replace(harris.CONFIGS["c1"], mx=grid[0], my=grid[1], mz=grid[2], filter_every=1)
+    o = gem_oracle(cfg)
+    t, n = 0.0, 0
+    for _ in range(warm):
+        dt = o.setdt()
+        o.stepon(t, dt, n)
+        t += dt
+        n += 1
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        dt = o.setdt()
+        o.stepon(t, dt, n)
+        t += dt
+        n += 1
+    el = time.perf_counter() - t0
+    return cfg.cells * steps / el, el
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU path on the host cores: the oracle restatement (the Fortran
+    reference cannot be built here), each step a bounded sample grid."""
+    if rank != 0:
+        return
+    from dasha_b200 import harris
+    kw = args.steps + args.warmup
+    grid = (256, 128, 256) if kw <= 16 else ((128, 64, 128) if kw <= 120 else (64, 32, 64))
+    rate, el = cpu_port_rate(steps=args.steps, grid=grid, warm=args.warmup)
+    cfg = harris.CONFIGS[args.config]
+    cores = os.cpu_count() or 1
+    sample = f"{grid[0]}x{grid[1]}x{grid[2]} Harris/GEM grid, {args.warmup} warm-up + {args.steps} timed RK4 steps"
+    line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Harris sheet + GEM perturbation)",
+            "config": {"workload": cfg.name, "sample_grid": "x".join(map(str, grid)), "precision": "fp64"},
+            "cpu_baseline": {"value": rate, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_dasha(args, rank, world):
+    from dasha_b200 import harris
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    cfg = harris.CONFIGS[args.config]
+    prec = args.precision
+    x, y, z, H = build_state(cfg)
+    d = make_ctx(cfg, prec, x, y, z, H)
+    t, n = 0.0, 0
+    for _ in range(args.warmup):
+        dt = d.setdt(t)
+        d.stepon(t, dt, n)
+        t += dt
+        n += 1
+    d.setdt(t)
+    if dist:
+        dist.barrier()
+    clocks = Clocks()
+    clocks.start()
+    d.timer_start()
+    for _ in range(args.steps):
+        dt = d.setdt(t)
+        d.stepon(t, dt, n)
+        t += dt
+        n += 1
+    ms = d.timer_stop()
+    ck = clocks.stop()
+    if dist:
+        import torch
+        tt = torch.tensor([ms], dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    cells = cfg.cells
+    value = world * cells * args.steps / (ms / 1e3)
+
+    # per-kernel breakdown: one profiled step (events around every launch)
+    d.profile(True)
+    dt = d.setdt(t)
+    d.stepon(t, dt, n)
+    d.setdt(t + dt)
+    prof = d.profile_read()
+    d.profile(False)
+    launches_per_step = sum(v[1] for v in prof.values())
+    tot = sum(v[0] for v in prof.values())
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n, dom_bytes) = dom
+    peak, peak_kind = peaks()
+    ach = dom_bytes / (dom_ms / dom_n / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+    if os.path.exists(tpath):
+        try:
+            tr = json.load(open(tpath))
+            key = f"{dom_name}.{prec}"
+            if key in tr:
+                traffic = tr[key] * cells
+        except Exception:
+            traffic = None
+    a_step = A_STEP[prec] + A_FILTER[prec] / max(cfg.filter_every, 1)
+    step_ach = a_step * (cells * args.steps / (ms / 1e3)) / 1e9
+
+    # e2e through the C-ABI with host buffers
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    d.set_state_halo(H)
+    te, ne = 0.0, 0
+    for _ in range(args.steps):
+        dt = d.setdt(te)
+        d.stepon(te, dt, ne)
+        te += dt
+        ne += 1
+    from dasha_b200 import capi
+    lib = d.lib
+    rc = lib.dasha_get_state(d.h, H.ctypes.data_as(capi._D), H.shape[3], H.shape[2])
+    if rc:
+        raise capi.DashaError(rc, "get_state")
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        import torch
+        tt = torch.tensor([e2e_s], dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    state_bytes = 8 * cells * 8
+    e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": state_bytes / args.steps + 8,
+           "note": "set_state from host + K x (setdt with dt read-back + stepon) + get_state to host, wall clock"}
+
+    line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64",
+            "data": "synthetic (seeded Harris sheet + GEM perturbation)",
+            "config": {"workload": cfg.name, "grid": [cfg.mx, cfg.my, cfg.mz], "precision": prec,
+                       "state": "FP32 perturbation + Kahan RK4" if prec == "fp32" else "FP64",
+                       "hall": cfg.hall, "filter_every": cfg.filter_every, "eta": cfg.eta, "di": cfg.di,
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas{world}"},
+            "e2e": e2e,
+            "gpu_launches": int(launches_per_step * args.steps),
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms / dom_n,
+                         "share_of_step": dom_ms / tot},
+            "step_roofline": {"algorithmic_bytes_per_cell_update": a_step, "achieved": step_ach,
+                              "peak": peak, "unit": "GB/s", "frac": step_ach / peak},
+            "kernels": {k: {"ms_per_step": v[0], "launches": v[1], "GBps": v[2] * v[1] / (v[0] / 1e3) / 1e9}
+                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "clocks": ck}
+    d.close()
+    del H
+    if rank == 0 and world == 1 and not args.no_cpu:
+        rate, el = cpu_port_rate(steps=2)
+        line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": os.cpu_count() or 1,
+                                "kind": "port",
+                                "sample": f"256x128x256 Harris/GEM grid, 2 RK4 steps ({el:.1f} s), "
+                                          "CPU FP64 oracle with OpenMP, scaled per cell"}
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="dasha", choices=["dasha", "reference"])
+    ap.add_argument("--config", default="c4", choices=["c0", "c1", "c2", "c3", "c4"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = env_rank()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    pin_device(local, world)
+    run_dasha(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

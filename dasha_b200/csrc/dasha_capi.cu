@@ -1,0 +1,371 @@
+// dasha_capi.cu -- host side of libdasha.so: context, device buffers, coefficient set-up and
+// the C-ABI declared in include/dasha_capi.h.  All device work is in mhd_kernels.cuh.
+#include "dasha_capi.h"
+#include "mhd_kernels.cuh"
+#include "engine.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <new>
+
+using namespace dasha;
+
+// ---------------------------------------------------------------------------------------
+// Stencil coefficients.  The reference builds its 5-point coefficients from closed forms
+// (first derivative t3dsdsc.f:439-504, second derivative t3dsdsc.f:336-437).  Both are the
+// unique 5-point weights a,b,c,d of
+//     D f = a (f+ - f0) + b (f0 - f-) + c (f++ - f0) + d (f0 - f--)
+// that are exact for (x - x0)^n, n = 1..4 (n=1 -> 1 for the first derivative, n=2 -> 2 for
+// the second).  Here they are obtained by solving that 4x4 system directly (partial
+// pivoting), an independent route to the same numbers.
+static bool solve4(double A[4][4], double rhs[4], double out[4]) {
+    double M[4][5];
+    for (int r = 0; r < 4; ++r) { for (int c = 0; c < 4; ++c) M[r][c] = A[r][c]; M[r][4] = rhs[r]; }
+    for (int c = 0; c < 4; ++c) {
+        int best = c;
+        for (int r = c + 1; r < 4; ++r) if (std::fabs(M[r][c]) > std::fabs(M[best][c])) best = r;
+        if (M[best][c] == 0.0) return false;
+        if (best != c) for (int q = 0; q < 5; ++q) std::swap(M[best][q], M[c][q]);
+        for (int r = c + 1; r < 4; ++r) {
+            double f = M[r][c] / M[c][c];
+            for (int q = c; q < 5; ++q) M[r][q] -= f * M[c][q];
+        }
+    }
+    for (int r = 3; r >= 0; --r) {
+        double s = M[r][4];
+        for (int q = r + 1; q < 4; ++q) s -= M[r][q] * out[q];
+        out[r] = s / M[r][r];
+    }
+    return true;
+}
+
+// offsets hp1 = x+1 - x0, hm1 = x0 - x-1, hp2 = x+2 - x0, hm2 = x0 - x-2 (all > 0)
+static bool stencil_weights(double hp1, double hm1, double hp2, double hm2, int order, double w[4]) {
+    double A[4][4], b[4];
+    for (int n = 1; n <= 4; ++n) {
+        A[n - 1][0] = std::pow(hp1, n);
+        A[n - 1][1] = -std::pow(-hm1, n);
+        A[n - 1][2] = std::pow(hp2, n);
+        A[n - 1][3] = -std::pow(-hm2, n);
+        b[n - 1] = (order == 1) ? (n == 1 ? 1.0 : 0.0) : (n == 2 ? 2.0 : 0.0);
+    }
+    return solve4(A, b, w);
+}
+
+struct Axis {
+    int n;
+    bool periodic;
+    std::vector<double> c;    // coordinates
+    double L = 0;             // period
+    double at(int i) const {  // coordinate continued across the wrap
+        if (!periodic) return c[i];
+        int q = 0;
+        while (i < 0) { i += n; --q; }
+        while (i >= n) { i -= n; ++q; }
+        return c[i] + q * L;
+    }
+};
+
+namespace dasha {
+template <class T>
+static EngineBase* make_engine(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st,
+                               const HostTables& H, Status& s) {
+    Engine<T>* e = new Engine<T>();
+    s = e->init(mx, my, mz, p, st, H);
+    return e;
+}
+EngineBase* make_engine_f64(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const HostTables& H,
+                            Status& s) {
+    return make_engine<double>(mx, my, mz, p, st, H, s);
+}
+EngineBase* make_engine_f32(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const HostTables& H,
+                            Status& s) {
+    return make_engine<float>(mx, my, mz, p, st, H, s);
+}
+}  // namespace dasha
+
+// ---------------------------------------------------------------------------------------
+struct dasha_ctx {
+    int mx = 0, my = 0, mz = 0;
+    long N = 0;
+    dasha_params_c P{};
+    int device = 0;
+    cudaStream_t st = nullptr;
+    std::string err;
+    int sticky = 0;
+    Axis ax, ay, az;
+    EngineBase* eng = nullptr;
+    bool eq_set = false, state_set = false;
+    double dt0 = 0.;
+    bool have_dt0 = false;
+};
+
+static int fail(dasha_ctx* c, int code, const std::string& msg) {
+    if (c) {
+        c->err = msg;
+        if (code == DASHA_E_CUDA) c->sticky = code;
+    }
+    return code;
+}
+
+#define CAPI_GUARD(ctx)                                                                       \
+    if (!(ctx)) return DASHA_E_INVALID;                                                       \
+    if ((ctx)->sticky) return (ctx)->sticky;
+
+static int from_status(dasha_ctx* c, const Status& s) {
+    if (s.code == DASHA_OK) return DASHA_OK;
+    return fail(c, s.code, s.msg);
+}
+
+extern "C" {
+
+int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_ctx** out) {
+    if (!out) return DASHA_E_INVALID;
+    *out = nullptr;
+    if (!grid || !params || !grid->x || !grid->y || !grid->z) return DASHA_E_INVALID;
+    if (grid->mx < 5 || grid->my < 5 || grid->mz < 7) return DASHA_E_INVALID;
+    if (!(grid->periodic[0] == 1 && grid->periodic[1] == 1 && grid->periodic[2] == 0)) return DASHA_E_UNSUPPORTED;
+    const dasha_params_c& p = *params;
+    if (p.precision != 0 && p.precision != 1) return DASHA_E_INVALID;
+    if (p.total_e != 1 || p.rcr > 0.0) return DASHA_E_UNSUPPORTED;
+    if (p.j0_mode != 0 && p.j0_mode != 1) return DASHA_E_INVALID;
+    if (!(p.gamma > 1.0) || !(p.cfl > 0.0) || p.filter_every < 0) return DASHA_E_INVALID;
+    dasha_ctx* c = new (std::nothrow) dasha_ctx();
+    if (!c) return DASHA_E_NOMEM;
+    try {
+        c->mx = grid->mx; c->my = grid->my; c->mz = grid->mz;
+        c->N = (long)c->mx * c->my * c->mz;
+        c->P = p;
+        c->ax.n = c->mx; c->ax.periodic = true; c->ax.c.assign(grid->x, grid->x + c->mx);
+        c->ay.n = c->my; c->ay.periodic = true; c->ay.c.assign(grid->y, grid->y + c->my);
+        c->az.n = c->mz; c->az.periodic = false; c->az.c.assign(grid->z, grid->z + c->mz);
+        // a periodic axis continues with its first spacing across the wrap (t3dsdsc.f:278-283)
+        c->ax.L = c->ax.c[c->mx - 1] - c->ax.c[0] + (c->ax.c[1] - c->ax.c[0]);
+        c->ay.L = c->ay.c[c->my - 1] - c->ay.c[0] + (c->ay.c[1] - c->ay.c[0]);
+        for (const Axis* a : {&c->ax, &c->ay, &c->az})
+            for (int i = 0; i + 1 < a->n; ++i)
+                if (!(a->c[i + 1] > a->c[i])) { delete c; return DASHA_E_INVALID; }
+        if (cudaGetDevice(&c->device) != cudaSuccess) { delete c; return DASHA_E_CUDA; }
+        if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return DASHA_E_CUDA; }
+
+        // host coefficient tables (FP64)
+        HostTables H;
+        H.mx = c->mx; H.my = c->my; H.mz = c->mz;
+        const Axis* axes[3] = {&c->ax, &c->ay, &c->az};
+        for (int d = 0; d < 3; ++d) {
+            const Axis& a = *axes[d];
+            int n = a.n;
+            for (int q = 0; q < 8; ++q) H.coef[d][q].assign(n, 0.0);
+            H.wp[d].assign(n, 0.0); H.wm[d].assign(n, 0.0);
+            H.spacing[d].assign(n, 0.0); H.weight[d].assign(n, 0.0);
+            for (int i = 0; i < n; ++i) {
+                bool interior = a.periodic || (i >= 2 && i <= n - 3);
+                if (interior) {
+                    double x0 = a.at(i);
+                    double hp1 = a.at(i + 1) - x0, hm1 = x0 - a.at(i - 1);
+                    double hp2 = a.at(i + 2) - x0, hm2 = x0 - a.at(i - 2);
+                    double w1[4], w2[4];
+                    if (!stencil_weights(hp1, hm1, hp2, hm2, 1, w1) || !stencil_weights(hp1, hm1, hp2, hm2, 2, w2)) {
+                        delete c; return DASHA_E_INVALID;
+                    }
+                    for (int q = 0; q < 4; ++q) { H.coef[d][q][i] = w1[q]; H.coef[d][4 + q][i] = w2[q]; }
+                }
+                bool inner1 = a.periodic || (i >= 1 && i <= n - 2);
+                if (inner1) {
+                    double xm = a.at(i - 1), x0 = a.at(i), xp = a.at(i + 1);
+                    H.wp[d][i] = 2.0 * (xp - x0) / (xp - xm);
+                    H.wm[d][i] = 2.0 * (x0 - xm) / (xp - xm);
+                }
+                // forward spacing of node i (dxt of gridpntnew2), used by setdt
+                H.spacing[d][i] = (a.periodic || i + 1 < n) ? a.at(i + 1) - a.at(i) : a.c[n - 1] - a.c[n - 2];
+                // trapezoid volume weight
+                if (a.periodic) H.weight[d][i] = 0.5 * (a.at(i + 1) - a.at(i - 1));
+                else H.weight[d][i] = 0.5 * (a.c[std::min(i + 1, n - 1)] - a.c[std::max(i - 1, 0)]);
+            }
+            H.coord[d] = a.c;
+        }
+        H.cbx.assign(c->mx, 0.0);
+        for (int i = 0; i < c->mx; ++i) H.cbx[i] = (1.0 / 32.0) * (1.0 - std::tanh((c->ax.c[i] + 3.0) / 8.0));
+
+        Status s;
+        if (p.precision == 0) c->eng = make_engine_f64(c->mx, c->my, c->mz, p, c->st, H, s);
+        else c->eng = make_engine_f32(c->mx, c->my, c->mz, p, c->st, H, s);
+        if (s.code != DASHA_OK) {
+            int code = s.code;
+            delete c->eng; c->eng = nullptr;
+            cudaStreamDestroy(c->st);
+            delete c;
+            return code;
+        }
+    } catch (...) {
+        if (c->eng) delete c->eng;
+        if (c->st) cudaStreamDestroy(c->st);
+        delete c;
+        return DASHA_E_NOMEM;
+    }
+    *out = c;
+    return DASHA_OK;
+}
+
+void dasha_destroy(dasha_ctx* c) {
+    if (!c) return;
+    if (c->eng) { cudaStreamSynchronize(c->st); delete c->eng; }
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+const char* dasha_last_error(dasha_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int dasha_set_equilibrium(dasha_ctx* c, const double* rho0, const double* b0, const double* p0) {
+    CAPI_GUARD(c);
+    if (!rho0 || !b0 || !p0) return fail(c, DASHA_E_INVALID, "null equilibrium profile");
+    for (int k = 0; k < c->mz; ++k)
+        if (!(rho0[k] > 0.0)) return fail(c, DASHA_E_INVALID, "rho0 must be positive");
+    try {
+        int rc = from_status(c, c->eng->set_equilibrium(rho0, b0, p0, nullptr));
+        if (rc == DASHA_OK) c->eq_set = true;
+        return rc;
+    } catch (...) { return fail(c, DASHA_E_NOMEM, "host allocation failed"); }
+}
+
+int dasha_set_equilibrium_current(dasha_ctx* c, const double* j0) {
+    CAPI_GUARD(c);
+    if (!j0) return fail(c, DASHA_E_INVALID, "null j0");
+    if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium first");
+    try { return from_status(c, c->eng->set_j0(j0)); }
+    catch (...) { return fail(c, DASHA_E_NOMEM, "host allocation failed"); }
+}
+
+static int check_ld(dasha_ctx* c, const void* p, long ld1, long ld2) {
+    if (!p) return fail(c, DASHA_E_INVALID, "null host array");
+    if (ld1 < c->mx + 4 || ld2 < c->my) return fail(c, DASHA_E_INVALID, "leading dimensions too small");
+    return DASHA_OK;
+}
+
+int dasha_set_state(dasha_ctx* c, const double* x_f, long ld1, long ld2) {
+    CAPI_GUARD(c);
+    if (int rc = check_ld(c, x_f, ld1, ld2)) return rc;
+    if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium before the state");
+    int rc = from_status(c, c->eng->set_state(x_f, ld1, ld2));
+    if (rc == DASHA_OK) c->state_set = true;
+    return rc;
+}
+
+int dasha_get_state(dasha_ctx* c, double* x_f, long ld1, long ld2) {
+    CAPI_GUARD(c);
+    if (int rc = check_ld(c, x_f, ld1, ld2)) return rc;
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return from_status(c, c->eng->get_state(x_f, ld1, ld2));
+}
+
+int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {
+    CAPI_GUARD(c);
+    (void)time;
+    if (!dt_out) return fail(c, DASHA_E_INVALID, "null dt_out");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    int blowup = 0;
+    double dt = 0.;
+    int rc = from_status(c, c->eng->setdt(&dt, &blowup));
+    if (rc) return rc;
+    *dt_out = dt;
+    if (blowup) return fail(c, DASHA_E_BLOWUP, "max Jy on the mid-y plane reached 1e7 (or is not finite)");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DASHA_E_DT_COLLAPSE, "dt is not a positive finite number");
+    if (!c->have_dt0) { c->dt0 = dt; c->have_dt0 = true; }
+    else if (dt < 0.1 * c->dt0) return fail(c, DASHA_E_DT_COLLAPSE, "dt fell below 0.1*dt0");
+    return DASHA_OK;
+}
+
+int dasha_stepon(dasha_ctx* c, double time, double dt, int nstep) {
+    CAPI_GUARD(c);
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DASHA_E_INVALID, "dt must be positive and finite");
+    return from_status(c, c->eng->stepon(time, dt, nstep));
+}
+
+int dasha_current(dasha_ctx* c, double* cur_f, long ld1, long ld2) {
+    CAPI_GUARD(c);
+    if (int rc = check_ld(c, cur_f, ld1, ld2)) return rc;
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return from_status(c, c->eng->current(cur_f, ld1, ld2));
+}
+
+int dasha_rhs(dasha_ctx* c, double t, double* xdif_f, long ld1, long ld2) {
+    CAPI_GUARD(c);
+    if (int rc = check_ld(c, xdif_f, ld1, ld2)) return rc;
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return from_status(c, c->eng->rhs(t, xdif_f, ld1, ld2));
+}
+
+int dasha_diagnostics(dasha_ctx* c, double* out) {
+    CAPI_GUARD(c);
+    if (!out) return fail(c, DASHA_E_INVALID, "null out");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return from_status(c, c->eng->diagnostics(out));
+}
+
+int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int snaps, double* dPhi_deta,
+                            double* dPhi_dpsi) {
+    CAPI_GUARD(c);
+    if (nsteps < 0 || (nsteps > 0 && !dt_seq) || snaps < 1 || !dPhi_deta || !dPhi_dpsi)
+        return fail(c, DASHA_E_INVALID, "bad adjoint arguments");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    if (c->P.precision != 0) return fail(c, DASHA_E_UNSUPPORTED, "the adjoint runs on FP64 contexts only");
+    return from_status(c, c->eng->adjoint_flux_grad(nsteps, dt_seq, snaps, dPhi_deta, dPhi_dpsi));
+}
+
+int dasha_timer(dasha_ctx* c, int op, double* ms) {
+    CAPI_GUARD(c);
+    EngineBase* e = c->eng;
+    if (!e->t0) {
+        if (cudaEventCreate(&e->t0) != cudaSuccess || cudaEventCreate(&e->t1) != cudaSuccess)
+            return fail(c, DASHA_E_CUDA, "cudaEventCreate failed");
+    }
+    if (op == 0) {
+        if (cudaEventRecord(e->t0, c->st) != cudaSuccess) return fail(c, DASHA_E_CUDA, "cudaEventRecord failed");
+        return DASHA_OK;
+    }
+    if (op != 1 || !ms) return fail(c, DASHA_E_INVALID, "dasha_timer: op must be 0 or 1 (with ms)");
+    if (cudaEventRecord(e->t1, c->st) != cudaSuccess || cudaEventSynchronize(e->t1) != cudaSuccess)
+        return fail(c, DASHA_E_CUDA, "cudaEventSynchronize failed");
+    float f = 0.f;
+    if (cudaEventElapsedTime(&f, e->t0, e->t1) != cudaSuccess) return fail(c, DASHA_E_CUDA, "cudaEventElapsedTime failed");
+    *ms = f;
+    return DASHA_OK;
+}
+
+int dasha_profile(dasha_ctx* c, int enable) {
+    CAPI_GUARD(c);
+    c->eng->prof.on = enable != 0;
+    return DASHA_OK;
+}
+
+int dasha_profile_read(dasha_ctx* c, int* n, char* names, double* ms, long* launches, double* bytes) {
+    CAPI_GUARD(c);
+    if (!n || *n < 0 || (*n > 0 && (!names || !ms || !launches || !bytes))) return fail(c, DASHA_E_INVALID, "bad arguments");
+    Profiler& p = c->eng->prof;
+    if (cudaStreamSynchronize(c->st) != cudaSuccess) return fail(c, DASHA_E_CUDA, "stream synchronize failed");
+    size_t nt = p.names.size();
+    std::vector<double> tot(nt, 0.0);
+    std::vector<long> cnt(nt, 0);
+    for (auto& r : p.recs) {
+        float f = 0.f;
+        cudaEventElapsedTime(&f, r.a, r.b);
+        tot[r.tag] += f;
+        cnt[r.tag] += 1;
+    }
+    int rows = (int)std::min<size_t>(nt, (size_t)*n);
+    for (int q = 0; q < rows; ++q) {
+        std::memset(names + 32 * q, 0, 32);
+        std::strncpy(names + 32 * q, p.names[q].c_str(), 31);
+        ms[q] = tot[q]; launches[q] = cnt[q]; bytes[q] = p.bytes[q];
+    }
+    *n = (int)nt;
+    p.recs.clear();
+    p.used = 0;
+    return DASHA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,520 @@
+// engine.cuh -- device buffers and the launch sequence of one RK4 step (stepon, right,
+// current, setdt, diagn of t3dsdsc.f), templated on the storage type (double / float).
+#pragma once
+#include "dasha_capi.h"
+#include "mhd_kernels.cuh"
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+
+namespace dasha {
+
+struct Status {
+    int code = 0;
+    std::string msg;
+    static Status ok() { return Status(); }
+    static Status err(int c, const std::string& m) { Status s; s.code = c; s.msg = m; return s; }
+};
+
+#define DASHA_CK(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return Status::err(DASHA_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// FP64 host tables built by dasha_create: per axis d (0=x,1=y,2=z)
+struct HostTables {
+    int mx, my, mz;
+    std::vector<double> coef[3][8];   // a1 b1 c1 d1 a2 b2 c2 d2
+    std::vector<double> wp[3], wm[3]; // difc weights
+    std::vector<double> spacing[3];   // forward spacing (setdt)
+    std::vector<double> weight[3];    // trapezoid weights (diagnostics)
+    std::vector<double> coord[3];
+    std::vector<double> cbx;          // (1/32)(1 - tanh((x+3)/8))
+};
+
+// Optional per-launch CUDA-event profiler (dasha_profile).
+struct Profiler {
+    bool on = false;
+    struct Rec { int tag; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<std::string> names;
+    std::vector<double> bytes;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    int tag_of(const char* name, double b) {
+        for (size_t q = 0; q < names.size(); ++q) if (names[q] == name) return (int)q;
+        names.push_back(name); bytes.push_back(b);
+        return (int)names.size() - 1;
+    }
+    cudaEvent_t ev() {
+        if (used == pool.size()) { cudaEvent_t e; cudaEventCreate(&e); pool.push_back(e); }
+        return pool[used++];
+    }
+    ~Profiler() { for (auto e : pool) cudaEventDestroy(e); }
+};
+
+struct EngineBase {
+    Profiler prof;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    virtual ~EngineBase() {
+        if (t0) cudaEventDestroy(t0);
+        if (t1) cudaEventDestroy(t1);
+    }
+    virtual Status set_equilibrium(const double* rho0, const double* b0, const double* p0, const double* j0) = 0;
+    virtual Status set_j0(const double* j0) = 0;
+    virtual Status set_state(const double* x, long ld1, long ld2) = 0;
+    virtual Status get_state(double* x, long ld1, long ld2) = 0;
+    virtual Status setdt(double* dt, int* blowup) = 0;
+    virtual Status stepon(double time, double dt, int nstep) = 0;
+    virtual Status current(double* cur, long ld1, long ld2) = 0;
+    virtual Status rhs(double t, double* xdif, long ld1, long ld2) = 0;
+    virtual Status diagnostics(double* out) = 0;
+    virtual Status adjoint_flux_grad(int nsteps, const double* dt_seq, int snaps, double* deta, double* dpsi) = 0;
+};
+
+EngineBase* make_engine_f64(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const HostTables& H,
+                            Status& s);
+EngineBase* make_engine_f32(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const HostTables& H,
+                            Status& s);
+
+// Launch with optional event bracketing; bytes = algorithmic bytes of the launch.
+#define DASHA_LAUNCH(tag, bytes, ...)                                                          \
+    do {                                                                                       \
+        int tg_ = -1;                                                                          \
+        cudaEvent_t a_ = nullptr;                                                              \
+        if (prof.on) { tg_ = prof.tag_of(tag, (double)(bytes)); a_ = prof.ev(); cudaEventRecord(a_, st); } \
+        __VA_ARGS__;                                                                           \
+        if (prof.on) { cudaEvent_t b_ = prof.ev(); cudaEventRecord(b_, st); prof.recs.push_back({tg_, a_, b_}); } \
+    } while (0)
+
+// radial smoothing coefficient per node, computed in FP64 then stored as T
+template <class T>
+__global__ void k_init_cr(int mx, int my, int mz, const double* xc, const double* yc, const double* zc, T* cr) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mx) return;
+    int j = blockIdx.y, k = blockIdx.z;
+    double r = sqrt(xc[i] * xc[i] + yc[j] * yc[j] + zc[k] * zc[k]);
+    cr[(long)i + (long)mx * (j + (long)my * k)] = T(1.0 / 32.0 + (1.0 / 8.0 - 1.0 / 32.0) * 0.5 * (1 + tanh((r - 3.) / 3.)));
+}
+
+template <class T>
+class Engine : public EngineBase {
+public:
+    static constexpr bool KAHAN = sizeof(T) == 4;
+    int mx, my, mz;
+    long N;
+    dasha_params_c P;
+    cudaStream_t st;
+    // device memory
+    void* pool = nullptr;
+    T *X[8], *S[8], *A[8], *K[8], *C[8];
+    T *cur[2][3], *E[2][3], *Hh[2][3];
+    T* cr = nullptr;
+    T* tab = nullptr;            // 1-D tables in T
+    double* dtab = nullptr;      // 1-D tables in FP64
+    double* red = nullptr;       // reduction scratch
+    int* flag = nullptr;         // blow-up flag
+    double* hpin = nullptr;      // pinned host scratch
+    Geo<T> g{};
+    // FP64 device pointers for setdt / diagnostics
+    const double *xc, *yc, *zc, *dxs, *dys, *dzs, *wx, *wy, *wz;
+    std::vector<double> zcoord, coefz[8];
+    std::vector<double> rho0h, b0h[3], p0h, j0h[3];
+    bool j0_given = false;
+    long nred = 0;
+    dim3 blk, grd;
+
+    ~Engine() override {
+        if (pool) cudaFree(pool);
+        if (tab) cudaFree(tab);
+        if (dtab) cudaFree(dtab);
+        if (red) cudaFree(red);
+        if (flag) cudaFree(flag);
+        if (hpin) cudaFreeHost(hpin);
+    }
+
+    Status init(int mx_, int my_, int mz_, const dasha_params_c& p, cudaStream_t st_, const HostTables& H) {
+        mx = mx_; my = my_; mz = mz_; N = (long)mx * my * mz; P = p; st = st_;
+        int nfield = 8 * 4 + (KAHAN ? 8 : 0) + 18 + 1;
+        size_t fbytes = ((size_t)N * sizeof(T) + 255) & ~(size_t)255;
+        size_t freeb = 0, totb = 0;
+        DASHA_CK(cudaMemGetInfo(&freeb, &totb));
+        if ((double)fbytes * nfield > 0.97 * (double)freeb)
+            return Status::err(DASHA_E_NOMEM, "grid needs " + std::to_string((double)fbytes * nfield / 1e9) +
+                                                  " GB of device memory, " + std::to_string(freeb / 1e9) + " GB free");
+        cudaError_t e = cudaMalloc(&pool, fbytes * nfield);
+        if (e != cudaSuccess) { pool = nullptr; cudaGetLastError(); return Status::err(DASHA_E_NOMEM, "cudaMalloc of the field pool failed"); }
+        char* q = (char*)pool;
+        auto take = [&]() { T* r = (T*)q; q += fbytes; return r; };
+        for (int m = 0; m < 8; ++m) X[m] = take();
+        for (int m = 0; m < 8; ++m) S[m] = take();
+        for (int m = 0; m < 8; ++m) A[m] = take();
+        for (int m = 0; m < 8; ++m) K[m] = take();
+        for (int m = 0; m < 8; ++m) C[m] = KAHAN ? take() : nullptr;
+        for (int b = 0; b < 2; ++b) for (int m = 0; m < 3; ++m) cur[b][m] = take();
+        for (int b = 0; b < 2; ++b) for (int m = 0; m < 3; ++m) E[b][m] = take();
+        for (int b = 0; b < 2; ++b) for (int m = 0; m < 3; ++m) Hh[b][m] = take();
+        cr = take();
+        DASHA_CK(cudaMemsetAsync(pool, 0, fbytes * nfield, st));
+
+        // T tables: per axis 8 coefficients + wp + wm, plus cbx
+        int nx[3] = {mx, my, mz};
+        long ntab = 0;
+        for (int d = 0; d < 3; ++d) ntab += 10L * nx[d];
+        ntab += mx;
+        std::vector<T> ht(ntab);
+        long off[3][10], offcb;
+        long o = 0;
+        for (int d = 0; d < 3; ++d)
+            for (int q2 = 0; q2 < 10; ++q2) {
+                off[d][q2] = o;
+                const std::vector<double>& src = q2 < 8 ? H.coef[d][q2] : (q2 == 8 ? H.wp[d] : H.wm[d]);
+                for (int i = 0; i < nx[d]; ++i) ht[o + i] = T(src[i]);
+                o += nx[d];
+            }
+        offcb = o;
+        for (int i = 0; i < mx; ++i) ht[o + i] = T(H.cbx[i]);
+        DASHA_CK(cudaMalloc(&tab, sizeof(T) * ntab));
+        DASHA_CK(cudaMemcpy(tab, ht.data(), sizeof(T) * ntab, cudaMemcpyHostToDevice));
+        const T* t = tab;
+        g.mx = mx; g.my = my; g.mz = mz; g.sy = mx; g.sz = (long)mx * my;
+        const T** c1[3][4] = {{&g.a1x, &g.b1x, &g.c1x, &g.d1x}, {&g.a1y, &g.b1y, &g.c1y, &g.d1y}, {&g.a1z, &g.b1z, &g.c1z, &g.d1z}};
+        const T** c2[3][4] = {{&g.a2x, &g.b2x, &g.c2x, &g.d2x}, {&g.a2y, &g.b2y, &g.c2y, &g.d2y}, {&g.a2z, &g.b2z, &g.c2z, &g.d2z}};
+        const T** w2[3][2] = {{&g.wpx, &g.wmx}, {&g.wpy, &g.wmy}, {&g.wpz, &g.wmz}};
+        for (int d = 0; d < 3; ++d) {
+            for (int q2 = 0; q2 < 4; ++q2) { *c1[d][q2] = t + off[d][q2]; *c2[d][q2] = t + off[d][4 + q2]; }
+            *w2[d][0] = t + off[d][8]; *w2[d][1] = t + off[d][9];
+        }
+        g.cbx = t + offcb;
+        g.cr = cr;
+        g.eta = T(p.eta); g.di = T(p.di); g.gamma = T(p.gamma); g.mu = T(p.mu); g.drho = T(p.drho); g.dp = T(p.dp);
+        g.hall = p.hall; g.viscos = p.viscos && p.mu != 0.0; g.diffu = p.diffu && (p.drho != 0.0 || p.dp != 0.0);
+
+        // FP64 tables: coords(3), spacing(3), weights(3), equilibrium profiles (16 x mz)
+        long nd = 0;
+        for (int d = 0; d < 3; ++d) nd += 3L * nx[d];
+        nd += 16L * mz;
+        std::vector<double> hd(nd, 0.0);
+        long od[3][3];
+        o = 0;
+        for (int d = 0; d < 3; ++d)
+            for (int q2 = 0; q2 < 3; ++q2) {
+                od[d][q2] = o;
+                const std::vector<double>& src = q2 == 0 ? H.coord[d] : (q2 == 1 ? H.spacing[d] : H.weight[d]);
+                for (int i = 0; i < nx[d]; ++i) hd[o + i] = src[i];
+                o += nx[d];
+            }
+        long oeq = o;
+        DASHA_CK(cudaMalloc(&dtab, sizeof(double) * nd));
+        DASHA_CK(cudaMemcpy(dtab, hd.data(), sizeof(double) * nd, cudaMemcpyHostToDevice));
+        xc = dtab + od[0][0]; yc = dtab + od[1][0]; zc = dtab + od[2][0];
+        dxs = dtab + od[0][1]; dys = dtab + od[1][1]; dzs = dtab + od[2][1];
+        wx = dtab + od[0][2]; wy = dtab + od[1][2]; wz = dtab + od[2][2];
+        double* eqp = dtab + oeq;
+        g.rho0 = eqp; g.bx0 = eqp + mz; g.by0 = eqp + 2 * mz; g.bz0 = eqp + 3 * mz; g.p0 = eqp + 4 * mz;
+        g.dzp0 = eqp + 5 * mz; g.d2rho0 = eqp + 6 * mz; g.d2p0 = eqp + 7 * mz;
+        g.rsx = eqp + 8 * mz; g.rsy = eqp + 9 * mz; g.rsz = eqp + 10 * mz;
+        g.j0x = eqp + 11 * mz; g.j0y = eqp + 12 * mz; g.j0z = eqp + 13 * mz;
+        zcoord = H.coord[2];
+        for (int q2 = 0; q2 < 8; ++q2) coefz[q2] = H.coef[2][q2];
+
+        nred = 2L * my * mz + my + 6L * mz + 64;
+        DASHA_CK(cudaMalloc(&red, sizeof(double) * (nred + 16)));
+        DASHA_CK(cudaMalloc(&flag, sizeof(int)));
+        DASHA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
+        DASHA_CK(cudaMallocHost(&hpin, sizeof(double) * 16));
+
+        blk = dim3(std::min(128, ((mx + 31) / 32) * 32));
+        grd = dim3((mx + blk.x - 1) / blk.x, my, mz);
+        k_init_cr<T><<<grd, blk, 0, st>>>(mx, my, mz, xc, yc, zc, cr);
+        DASHA_CK(cudaGetLastError());
+        DASHA_CK(cudaStreamSynchronize(st));
+        return Status::ok();
+    }
+
+    // 4th-order z-derivative of a profile at interior rows (zero on the wall rows)
+    std::vector<double> zderiv(const std::vector<double>& f, int order) const {
+        std::vector<double> out(mz, 0.0);
+        int base = order == 1 ? 0 : 4;
+        for (int k = 2; k <= mz - 3; ++k)
+            out[k] = coefz[base][k] * (f[k + 1] - f[k]) + coefz[base + 1][k] * (f[k] - f[k - 1]) +
+                     coefz[base + 2][k] * (f[k + 2] - f[k]) + coefz[base + 3][k] * (f[k] - f[k - 2]);
+        return out;
+    }
+
+    Status upload_eq() {
+        std::vector<double> h(16L * mz, 0.0);
+        for (int k = 0; k < mz; ++k) {
+            h[k] = rho0h[k]; h[mz + k] = b0h[0][k]; h[2 * mz + k] = b0h[1][k]; h[3 * mz + k] = b0h[2][k];
+            h[4 * mz + k] = p0h[k];
+        }
+        std::vector<double> dzp0 = zderiv(p0h, 1), d2r = zderiv(rho0h, 2), d2p = zderiv(p0h, 2);
+        std::vector<double> jx(mz, 0.0), jy(mz, 0.0), jz(mz, 0.0);
+        if (P.j0_mode == 1) {
+            if (j0_given) { jx = j0h[0]; jy = j0h[1]; jz = j0h[2]; }
+            else {   // J0 = curl B0(z) = (-dBy0/dz, dBx0/dz, 0)
+                std::vector<double> dbx = zderiv(b0h[0], 1), dby = zderiv(b0h[1], 1);
+                for (int k = 0; k < mz; ++k) { jx[k] = -dby[k]; jy[k] = dbx[k]; }
+            }
+        }
+        for (int k = 0; k < mz; ++k) {
+            h[5 * mz + k] = dzp0[k]; h[6 * mz + k] = d2r[k]; h[7 * mz + k] = d2p[k];
+            // xresd: momentum RHS of the pure equilibrium (initia t3dsdsc.f:816-834); the flux
+            // divergence and J1 vanish there, leaving J0 x B0 (zero in LITERAL mode)
+            double rx = 0., ry = 0., rz = 0.;
+            if (P.j0_mode == 1 && k >= 2 && k <= mz - 3) {
+                double b1 = b0h[0][k], b2 = b0h[1][k], b3 = b0h[2][k];
+                rx = jy[k] * b3 - jz[k] * b2;
+                ry = jz[k] * b1 - jx[k] * b3;
+                rz = jx[k] * b2 - jy[k] * b1;
+            }
+            h[8 * mz + k] = rx; h[9 * mz + k] = ry; h[10 * mz + k] = rz;
+            h[11 * mz + k] = jx[k]; h[12 * mz + k] = jy[k]; h[13 * mz + k] = jz[k];
+        }
+        DASHA_CK(cudaMemcpyAsync((void*)g.rho0, h.data(), sizeof(double) * 16 * mz, cudaMemcpyHostToDevice, st));
+        DASHA_CK(cudaStreamSynchronize(st));
+        return Status::ok();
+    }
+
+    Status set_equilibrium(const double* rho0, const double* b0, const double* p0, const double*) override {
+        rho0h.assign(rho0, rho0 + mz);
+        for (int m = 0; m < 3; ++m) b0h[m].assign(b0 + m * mz, b0 + (m + 1) * mz);
+        p0h.assign(p0, p0 + mz);
+        return upload_eq();
+    }
+    Status set_j0(const double* j0) override {
+        for (int m = 0; m < 3; ++m) j0h[m].assign(j0 + m * mz, j0 + (m + 1) * mz);
+        j0_given = true;
+        return upload_eq();
+    }
+
+    // ---- host array transfer through a FP64 staging buffer, one field at a time ----
+    Status transfer_in(const double* host, long ld1, long ld2, T* const* dst, int nf, bool sub_eq) {
+        size_t plane = (size_t)ld1 * ld2 * (mz + 4);
+        double* stage = nullptr;
+        DASHA_CK(cudaMalloc(&stage, sizeof(double) * plane));
+        Status s = Status::ok();
+        for (int m = 0; m < nf && s.code == 0; ++m) {
+            cudaError_t e = cudaMemcpyAsync(stage, host + plane * m, sizeof(double) * plane, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+            k_import_one(stage, ld1, ld2, m, dst[m], sub_eq);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+        }
+        cudaError_t e = cudaStreamSynchronize(st);
+        cudaFree(stage);
+        if (s.code == 0 && e != cudaSuccess) s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e));
+        return s;
+    }
+    void k_import_one(const double* stage, long ld1, long ld2, int m, T* dst, bool sub_eq);
+    void k_export_one(const T* src, long ld1, long ld2, int m, double* stage, bool add_eq);
+
+    Status transfer_out(double* host, long ld1, long ld2, T* const* src, int nf, bool add_eq) {
+        size_t plane = (size_t)ld1 * ld2 * (mz + 4);
+        double* stage = nullptr;
+        DASHA_CK(cudaMalloc(&stage, sizeof(double) * plane));
+        Status s = Status::ok();
+        for (int m = 0; m < nf && s.code == 0; ++m) {
+            // keep the caller's halo entries: start from the host field
+            cudaError_t e = cudaMemcpyAsync(stage, host + plane * m, sizeof(double) * plane, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+            k_export_one(src[m], ld1, ld2, m, stage, add_eq);
+            e = cudaMemcpyAsync(host + plane * m, stage, sizeof(double) * plane, cudaMemcpyDeviceToHost, st);
+            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+            e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+        }
+        cudaFree(stage);
+        return s;
+    }
+
+    Status set_state(const double* x, long ld1, long ld2) override {
+        Status s = transfer_in(x, ld1, ld2, X, 8, true);
+        if (s.code) return s;
+        if (KAHAN) for (int m = 0; m < 8; ++m) DASHA_CK(cudaMemsetAsync(C[m], 0, sizeof(T) * N, st));
+        DASHA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
+        DASHA_CK(cudaStreamSynchronize(st));
+        return Status::ok();
+    }
+    Status get_state(double* x, long ld1, long ld2) override { return transfer_out(x, ld1, ld2, X, 8, true); }
+
+    // ---- the RHS chain (right, t3dsdsc.f:1297-1673) ----
+    template <int NFLD>
+    void smooth(T* const* in, T* const* out, T* const* acc, unsigned kinds) {
+        FS<T, NFLD> a{}, b{}, c{};
+        for (int q = 0; q < NFLD; ++q) { a.f[q] = in[q]; b.f[q] = out[q]; c.f[q] = acc ? acc[q] : out[q]; }
+        const char* tg = NFLD == 8 ? "k_smooth8" : (acc ? "k_smooth3_acc" : "k_smooth3");
+        DASHA_LAUNCH(tg, (double)N * sizeof(T) * (2 * NFLD + (acc ? NFLD : 0)),
+                     k_smooth<T, NFLD><<<grd, blk, 0, st>>>(g, a, b, c, kinds, acc ? 1 : 0));
+    }
+    static F8<T> f8(T* const* p) { F8<T> r; for (int m = 0; m < 8; ++m) r.f[m] = p[m]; return r; }
+    static F3<T> f3(T* const* p) { F3<T> r; for (int m = 0; m < 3; ++m) r.f[m] = p[m]; return r; }
+
+    // smoothed current of state xs into cur[0] (current, t3dsdsc.f:2452-2500)
+    void launch_current(T* const* xs) {
+        T* bb[3] = {xs[4], xs[5], xs[6]};
+        DASHA_LAUNCH("k_curl", 6.0 * N * sizeof(T), k_curl<T><<<grd, blk, 0, st>>>(g, f3(bb), f3(cur[0])));
+        for (int pass = 0; pass < 4; ++pass) smooth<3>(cur[pass & 1], cur[(pass + 1) & 1], nullptr, 0u);
+        if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(cur[0])));
+    }
+
+    // xdif of state xs into K
+    void launch_rhs(T* const* xs, bool smooth_xdif) {
+        launch_current(xs);
+        DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(cur[0]), f3(E[0])));
+        for (int pass = 0; pass < 4; ++pass) smooth<3>(E[pass & 1], E[(pass + 1) & 1], nullptr, 0u);
+        if (P.hall) {
+            DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(cur[0]), f3(Hh[0])));
+            const unsigned k18 = 1u | (1u << 2) | (1u << 4);
+            for (int pass = 0; pass < 4; ++pass) smooth<3>(Hh[pass & 1], Hh[(pass + 1) & 1], nullptr, k18);
+            smooth<3>(Hh[0], E[0], E[0], k18);   // 5th pass accumulated into E
+        }
+        DASHA_LAUNCH("k_rhs", 22.0 * N * sizeof(T), k_rhs<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(cur[0]), f3(E[0]), f8(K)));
+        if (smooth_xdif) {   // avrg: 2 passes, B with the x-profile coefficient
+            T* tmp[8] = {cur[1][0], cur[1][1], cur[1][2], E[1][0], E[1][1], E[1][2], Hh[1][0], Hh[1][1]};
+            const unsigned kB = (2u << 8) | (2u << 10) | (2u << 12);
+            smooth<8>(K, tmp, nullptr, kB);
+            smooth<8>(tmp, K, nullptr, kB);
+        }
+    }
+
+    Status stepon(double time, double dt, int nstep) override {
+        (void)time;
+        long nb = (N + 255) / 256;
+        F8<T> cz{};
+        if (KAHAN) cz = f8(C);
+        else for (int m = 0; m < 8; ++m) cz.f[m] = nullptr;
+        T* Sx[8];
+        for (int m = 0; m < 8; ++m) Sx[m] = S[m];
+        // stage 1..4: base = X, stage state in S, accumulator in A
+        launch_rhs(X, true);
+        DASHA_LAUNCH("k_rk_s1", 32.0 * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 1, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
+        launch_rhs(Sx, true);
+        DASHA_LAUNCH("k_rk_s2", 40.0 * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 2, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
+        launch_rhs(Sx, true);
+        DASHA_LAUNCH("k_rk_s3", 40.0 * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 3, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
+        launch_rhs(Sx, true);
+        DASHA_LAUNCH("k_rk_s4", (KAHAN ? 48.0 : 24.0) * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 4, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
+        for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
+        int every = P.filter_every > 0 ? P.filter_every : 1;
+        if (nstep % every == 0) {   // avrgtt on the perturbation (t3dsdsc.f:1135-1165)
+            T* tmp[8] = {cur[1][0], cur[1][1], cur[1][2], E[1][0], E[1][1], E[1][2], Hh[1][0], Hh[1][1]};
+            const unsigned kB = (2u << 8) | (2u << 10) | (2u << 12);
+            smooth<8>(X, tmp, nullptr, kB);
+            smooth<8>(tmp, X, nullptr, kB);
+        }
+        if (nstep % 10 == 0) {      // diagn blow-up guard (t3dsdsc.f:1174-1182, 1232)
+            Status s = launch_diag(true);
+            if (s.code) return s;
+        }
+        DASHA_CK(cudaGetLastError());
+        return Status::ok();
+    }
+
+    Status launch_diag(bool guard_only) {
+        launch_current(X);
+        double* rows = red;
+        double* fl = red + 2L * my * mz;
+        double* jext = fl + my;
+        double* out = red + nred;
+        (void)guard_only;
+        dim3 g2(1, my, mz);
+        DASHA_LAUNCH("k_diag_rows", 8.0 * N * sizeof(T), k_diag_rows<T><<<g2, 128, 0, st>>>(g, f8(X), wx, wy, wz, P.gamma, rows));
+        k_diag_flux<T><<<my, 128, 0, st>>>(g, f8(X), wx, fl);
+        k_diag_jext<T><<<mz, 128, 0, st>>>(g, f3(cur[0]), my / 2, jext);
+        k_diag_final<<<1, 256, 0, st>>>(rows, (long)my * mz, fl, my, jext, mz, out, flag);
+        DASHA_CK(cudaGetLastError());
+        return Status::ok();
+    }
+
+    Status diagnostics(double* outh) override {
+        Status s = launch_diag(false);
+        if (s.code) return s;
+        DASHA_CK(cudaMemcpyAsync(hpin, red + nred, sizeof(double) * DASHA_NDIAG, cudaMemcpyDeviceToHost, st));
+        DASHA_CK(cudaStreamSynchronize(st));
+        for (int q = 0; q < DASHA_NDIAG; ++q) outh[q] = hpin[q];
+        return Status::ok();
+    }
+
+    Status setdt(double* dt, int* blowup) override {
+        dim3 g2(1, my, mz);
+        DASHA_LAUNCH("k_cfl", 8.0 * N * sizeof(T), k_cfl<T><<<g2, 128, 0, st>>>(g, f8(X), xc, yc, zc, dxs, dys, dzs, P.cfl, P.eta + P.mu, P.rcr, P.gamma, red));
+        k_reduce_min<<<1, 256, 0, st>>>(red, (long)my * mz, red + nred + 12);
+        DASHA_CK(cudaGetLastError());
+        DASHA_CK(cudaMemcpyAsync(hpin + 12, red + nred + 12, sizeof(double), cudaMemcpyDeviceToHost, st));
+        int fl = 0;
+        DASHA_CK(cudaMemcpyAsync(hpin + 13, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+        DASHA_CK(cudaStreamSynchronize(st));
+        std::memcpy(&fl, hpin + 13, sizeof(int));
+        *dt = hpin[12];
+        *blowup = fl;
+        return Status::ok();
+    }
+
+    Status current(double* curh, long ld1, long ld2) override {
+        launch_current(X);
+        DASHA_CK(cudaGetLastError());
+        return transfer_out(curh, ld1, ld2, cur[0], 3, false);
+    }
+
+    Status rhs(double t, double* xdif, long ld1, long ld2) override {
+        launch_rhs(X, t != 0.0);
+        DASHA_CK(cudaGetLastError());
+        return transfer_out(xdif, ld1, ld2, K, 8, false);
+    }
+
+    Status adjoint_flux_grad(int, const double*, int, double*, double*) override {
+        return Status::err(DASHA_E_UNSUPPORTED, "adjoint not available in this build");
+    }
+};
+
+template <class T>
+__global__ void k_import_field(int mx, int my, int mz, const double* src, long ld1, long ld2, double eq_scale,
+                               const double* eqprof, T* dst) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mx) return;
+    int j = blockIdx.y, k = blockIdx.z;
+    double v = src[(i + 2) + ld1 * (j + ld2 * (long)(k + 2))];
+    if (eqprof) v -= eq_scale * eqprof[k];
+    dst[(long)i + (long)mx * (j + (long)my * k)] = T(v);
+}
+template <class T>
+__global__ void k_export_field(int mx, int my, int mz, const T* src, const double* eqprof, double* dst, long ld1,
+                               long ld2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= mx) return;
+    int j = blockIdx.y, k = blockIdx.z;
+    double v = (double)src[(long)i + (long)mx * (j + (long)my * k)];
+    if (eqprof) v += eqprof[k];
+    dst[(i + 2) + ld1 * (j + ld2 * (long)(k + 2))] = v;
+}
+
+template <class T>
+inline const double* eq_profile(const Geo<T>& g, int m) {
+    switch (m) {
+        case 0: return g.rho0;
+        case 4: return g.bx0;
+        case 5: return g.by0;
+        case 6: return g.bz0;
+        case 7: return g.p0;
+        default: return nullptr;
+    }
+}
+
+template <class T>
+void Engine<T>::k_import_one(const double* stage, long ld1, long ld2, int m, T* dst, bool sub_eq) {
+    const double* prof = sub_eq ? eq_profile(g, m) : nullptr;
+    k_import_field<T><<<grd, blk, 0, st>>>(mx, my, mz, stage, ld1, ld2, 1.0, prof, dst);
+}
+template <class T>
+void Engine<T>::k_export_one(const T* src, long ld1, long ld2, int m, double* stage, bool add_eq) {
+    const double* prof = add_eq ? eq_profile(g, m) : nullptr;
+    k_export_field<T><<<grd, blk, 0, st>>>(mx, my, mz, src, prof, stage, ld1, ld2);
+}
+
+}  // namespace dasha

@@ -1,0 +1,613 @@
+// mhd_kernels.cuh -- sm_100a kernels of the RK4 Hall-MHD step (reference: t3dsdsc.f).
+//
+// Storage: structure-of-arrays, one array per field, node (i,j,k) at i + mx*(j + my*k),
+// no ghost nodes.  x and y are periodic (index wrap); z rows 0,1,mz-2,mz-1 are the wall
+// rows of the reference (outer row 0, next row one half of its inner neighbour).
+// Every field is stored as the perturbation from the FP64 z-profile equilibrium
+// (rho0, B0, p0; momentum has no equilibrium part), in type T (double or float).
+//
+// Each kernel is launched on a 3-D grid: blockIdx.x covers x in chunks of blockDim.x,
+// blockIdx.y = j, blockIdx.z = k, so a warp reads consecutive x (coalesced).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dasha {
+
+constexpr int NF = 8;
+
+template <class T>
+struct Geo {
+    int mx, my, mz;
+    long sy, sz;
+    // 4th-order first / second derivative coefficients (t3dsdsc.f:336-504), zero where the
+    // reference leaves them undefined (z rows outside 2..mz-3)
+    const T *a1x, *b1x, *c1x, *d1x, *a1y, *b1y, *c1y, *d1y, *a1z, *b1z, *c1z, *d1z;
+    const T *a2x, *b2x, *c2x, *d2x, *a2y, *b2y, *c2y, *d2y, *a2z, *b2z, *c2z, *d2z;
+    // difc weights: difc = (f+ - f0)*wp - (f0 - f-)*wm  (t3dsdsc.f:5618-5619)
+    const T *wpx, *wmx, *wpy, *wmy, *wpz, *wmz;
+    const T *cbx;    // (1/32)(1 - tanh((x+3)/8)), smoothing coefficient of B (t3dsdsc.f:5636-5642)
+    const T *cr;     // 1/32 + 3/32 * (1 + tanh((r-3)/3))/2 per node (t3dsdsc.f:5659-5661)
+    // equilibrium z-profiles (FP64)
+    const double *rho0, *bx0, *by0, *bz0, *p0;
+    const double *dzp0;               // Dz p0 (interior rows)
+    const double *d2rho0, *d2p0;      // D2z rho0, D2z p0 (interior rows)
+    const double *rsx, *rsy, *rsz;    // xresd profiles (interior rows)
+    const double *j0x, *j0y, *j0z;    // J0 profiles for j0_mode FULL (null otherwise)
+    T eta, di, gamma, mu, drho, dp;
+    int hall, viscos, diffu;
+};
+
+template <class T>
+struct F8 { T* f[NF]; };
+template <class T>
+struct F3 { T* f[3]; };
+
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
+template <class T>
+__device__ __forceinline__ T d1fc(T fm2, T fm, T f0, T fp, T fp2, T a, T b, T c, T d) {
+    return a * (fp - f0) + b * (f0 - fm) + c * (fp2 - f0) + d * (f0 - fm2);
+}
+
+// Stencil helper: neighbour offsets of node (i,j,k) in a periodic-x/y, bounded-z array.
+template <class T>
+struct Nbr {
+    long c;              // centre
+    long xm2, xm1, xp1, xp2, ym2, ym1, yp1, yp2;   // absolute indices
+    int i, j, k;
+    __device__ __forceinline__ Nbr(const Geo<T>& g, int i_, int j_, int k_) : i(i_), j(j_), k(k_) {
+        long row = (long)j * g.sy + (long)k * g.sz;
+        c = row + i;
+        xm2 = row + wrapi(i - 2, g.mx); xm1 = row + wrapi(i - 1, g.mx);
+        xp1 = row + wrapi(i + 1, g.mx); xp2 = row + wrapi(i + 2, g.mx);
+        long col = (long)i + (long)k * g.sz;
+        ym2 = col + (long)wrapi(j - 2, g.my) * g.sy; ym1 = col + (long)wrapi(j - 1, g.my) * g.sy;
+        yp1 = col + (long)wrapi(j + 1, g.my) * g.sy; yp2 = col + (long)wrapi(j + 2, g.my) * g.sy;
+    }
+    __device__ __forceinline__ T Dx(const Geo<T>& g, const T* f) const {
+        return d1fc(f[xm2], f[xm1], f[c], f[xp1], f[xp2], g.a1x[i], g.b1x[i], g.c1x[i], g.d1x[i]);
+    }
+    __device__ __forceinline__ T Dy(const Geo<T>& g, const T* f) const {
+        return d1fc(f[ym2], f[ym1], f[c], f[yp1], f[yp2], g.a1y[j], g.b1y[j], g.c1y[j], g.d1y[j]);
+    }
+    __device__ __forceinline__ T Dz(const Geo<T>& g, const T* f) const {
+        return d1fc(f[c - 2 * g.sz], f[c - g.sz], f[c], f[c + g.sz], f[c + 2 * g.sz],
+                    g.a1z[k], g.b1z[k], g.c1z[k], g.d1z[k]);
+    }
+    __device__ __forceinline__ T D2x(const Geo<T>& g, const T* f) const {
+        return d1fc(f[xm2], f[xm1], f[c], f[xp1], f[xp2], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i]);
+    }
+    __device__ __forceinline__ T D2y(const Geo<T>& g, const T* f) const {
+        return d1fc(f[ym2], f[ym1], f[c], f[yp1], f[yp2], g.a2y[j], g.b2y[j], g.c2y[j], g.d2y[j]);
+    }
+    __device__ __forceinline__ T D2z(const Geo<T>& g, const T* f) const {
+        return d1fc(f[c - 2 * g.sz], f[c - g.sz], f[c], f[c + g.sz], f[c + 2 * g.sz],
+                    g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
+    }
+    // one Jacobi smoothing stencil: difc_x + difc_y + difc_z (t3dsdsc.f:5643-5648)
+    __device__ __forceinline__ T difc3(const Geo<T>& g, const T* f) const {
+        T f0 = f[c];
+        T tx = (f[xp1] - f0) * g.wpx[i] - (f0 - f[xm1]) * g.wmx[i];
+        T ty = (f[yp1] - f0) * g.wpy[j] - (f0 - f[ym1]) * g.wmy[j];
+        T tz = (f[c + g.sz] - f0) * g.wpz[k] - (f0 - f[c - g.sz]) * g.wmz[k];
+        return tx + ty + tz;
+    }
+};
+
+// Row rule of the z walls: which interior row a wall row copies from, and the factor.
+__device__ __forceinline__ int wall_src(int k, int mz, bool& zero, bool& half) {
+    zero = (k == 0 || k == mz - 1);
+    half = (k == 1 || k == mz - 2);
+    if (k == 1) return 2;
+    if (k == mz - 2) return mz - 3;
+    return k;
+}
+
+// ---------------------------------------------------------------------------------------
+// J1 = curl(B - B0) on interior rows + wall rows (current t3dsdsc.f:2468-2491, bndryc).
+template <class T>
+__global__ void k_curl(Geo<T> g, F3<T> b, F3<T> j) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int jj = blockIdx.y, k = blockIdx.z;
+    bool zero, half;
+    int ks = wall_src(k, g.mz, zero, half);
+    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+    if (zero) { j.f[0][c] = T(0); j.f[1][c] = T(0); j.f[2][c] = T(0); return; }
+    Nbr<T> n(g, i, jj, ks);
+    T cx = n.Dy(g, b.f[2]) - n.Dz(g, b.f[1]);
+    T cy = n.Dz(g, b.f[0]) - n.Dx(g, b.f[2]);
+    T cz = n.Dx(g, b.f[1]) - n.Dy(g, b.f[0]);
+    if (half) { cx = T(0.5) * cx; cy = T(0.5) * cy; cz = T(0.5) * cz; }
+    j.f[0][c] = cx; j.f[1][c] = cy; j.f[2][c] = cz;
+}
+
+// ---------------------------------------------------------------------------------------
+// One smoothing pass over NFLD fields with the wall rows re-applied (avrg/avrgE/avrgc/avrgh
+// + bndry*).  kind per field: 0 radial coefficient cr, 1 constant 1/8, 2 x-profile cbx.
+// If acc is given: out = acc + smoothed (the Hall term added into E, t3dsdsc.f:1426-1432).
+template <class T, int NFLD>
+struct FS { T* f[NFLD]; };
+
+template <class T, int NFLD>
+__global__ void k_smooth(Geo<T> g, FS<T, NFLD> in, FS<T, NFLD> out, FS<T, NFLD> acc, unsigned kinds,
+                         int use_acc) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int jj = blockIdx.y, k = blockIdx.z;
+    bool zero, half;
+    int ks = wall_src(k, g.mz, zero, half);
+    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+    Nbr<T> n(g, i, jj, ks);
+#pragma unroll
+    for (int q = 0; q < NFLD; ++q) {
+        T val = T(0);
+        if (!zero) {
+            unsigned kind = (kinds >> (2 * q)) & 3u;
+            T coef = kind == 0 ? g.cr[n.c] : (kind == 1 ? T(0.125) : g.cbx[i]);
+            val = in.f[q][n.c] + coef * n.difc3(g, in.f[q]);
+            if (half) val = T(0.5) * val;
+        }
+        if (use_acc) val = acc.f[q][c] + val;
+        out.f[q][c] = val;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// E = -v x B + eta*J at every node (t3dsdsc.f:1367-1372).
+template <class T>
+__global__ void k_efield(Geo<T> g, F8<T> x, F3<T> cur, F3<T> e) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int jj = blockIdx.y, k = blockIdx.z;
+    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+    T r = T(g.rho0[k]) + x.f[0][c];
+    T m1 = x.f[1][c], m2 = x.f[2][c], m3 = x.f[3][c];
+    T b1 = T(g.bx0[k]) + x.f[4][c], b2 = T(g.by0[k]) + x.f[5][c], b3 = T(g.bz0[k]) + x.f[6][c];
+    e.f[0][c] = (-m2 * b3 + m3 * b2) / r + g.eta * cur.f[0][c];
+    e.f[1][c] = (-m3 * b1 + m1 * b3) / r + g.eta * cur.f[1][c];
+    e.f[2][c] = (-m1 * b2 + m2 * b1) / r + g.eta * cur.f[2][c];
+}
+
+// ---------------------------------------------------------------------------------------
+// Hall term xdh = di*(J x B - grad p)/rho on interior rows + wall rows (t3dsdsc.f:1404-1423).
+template <class T>
+__global__ void k_hall(Geo<T> g, F8<T> x, F3<T> cur, F3<T> h) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int jj = blockIdx.y, k = blockIdx.z;
+    bool zero, half;
+    int ks = wall_src(k, g.mz, zero, half);
+    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+    if (zero) { h.f[0][c] = T(0); h.f[1][c] = T(0); h.f[2][c] = T(0); return; }
+    Nbr<T> n(g, i, jj, ks);
+    long q = n.c;
+    T r = T(g.rho0[ks]) + x.f[0][q];
+    T b1 = T(g.bx0[ks]) + x.f[4][q], b2 = T(g.by0[ks]) + x.f[5][q], b3 = T(g.bz0[ks]) + x.f[6][q];
+    T j1 = cur.f[0][q], j2 = cur.f[1][q], j3 = cur.f[2][q];
+    const T* p = x.f[7];
+    T px = n.Dx(g, p), py = n.Dy(g, p), pz = n.Dz(g, p) + T(g.dzp0[ks]);
+    T h1 = g.di * (j2 * b3 - j3 * b2 - px) / r;
+    T h2 = g.di * (j3 * b1 - j1 * b3 - py) / r;
+    T h3 = g.di * (j1 * b2 - j2 * b1 - pz) / r;
+    if (half) { h1 = T(0.5) * h1; h2 = T(0.5) * h2; h3 = T(0.5) * h3; }
+    h.f[0][c] = h1; h.f[1][c] = h2; h.f[2][c] = h3;
+}
+
+// ---------------------------------------------------------------------------------------
+// Right-hand side xdif on interior rows + wall rows (right t3dsdsc.f:1334-1566, bndry).
+template <class T>
+__device__ __forceinline__ void rhs_point(const Geo<T>& g, const F8<T>& x, const F3<T>& cur,
+                                          const F3<T>& e, int i, int jj, int k, T out[NF]) {
+    Nbr<T> n(g, i, jj, k);
+    const T* R = x.f[0];
+    const T* M1 = x.f[1];
+    const T* M2 = x.f[2];
+    const T* M3 = x.f[3];
+    const T* P = x.f[7];
+    const T r0 = T(g.rho0[k]);
+    // density at the x / y neighbours share the centre's row profile; z neighbours do not
+    auto rx = [&](long q) { return r0 + R[q]; };
+    auto rz = [&](long q, int kk) { return T(g.rho0[kk]) + R[q]; };
+    // continuity: -div(rho v)
+    T dxf = n.Dx(g, M1), dyg = n.Dy(g, M2), dzh = n.Dz(g, M3);
+    out[0] = -dxf - dyg - dzh;
+    // momentum fluxes m=2..4 (flux, t3dsdsc.f:2317-2347) evaluated at the stencil points
+    const long sz = g.sz;
+    long zi[5] = {n.c - 2 * sz, n.c - sz, n.c, n.c + sz, n.c + 2 * sz};
+    long xi[5] = {n.xm2, n.xm1, n.c, n.xp1, n.xp2};
+    long yi[5] = {n.ym2, n.ym1, n.c, n.yp1, n.yp2};
+    T fx[3][5], fy[3][5], fz[3][5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        long q = xi[s];
+        T r = rx(q), a = M1[q], dp = P[q];
+        fx[0][s] = a * a / r + dp;
+        fx[1][s] = a * M2[q] / r;
+        fx[2][s] = a * M3[q] / r;
+        q = yi[s];
+        r = rx(q);
+        T bq = M2[q];
+        fy[0][s] = M1[q] * bq / r;
+        fy[1][s] = bq * bq / r + P[q];
+        fy[2][s] = M3[q] * bq / r;
+        q = zi[s];
+        r = rz(q, k - 2 + s);
+        T cq = M3[q];
+        fz[0][s] = M1[q] * cq / r;
+        fz[1][s] = M2[q] * cq / r;
+        fz[2][s] = cq * cq / r + P[q];
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        T ddx = d1fc(fx[m][0], fx[m][1], fx[m][2], fx[m][3], fx[m][4], g.a1x[i], g.b1x[i], g.c1x[i], g.d1x[i]);
+        T ddy = d1fc(fy[m][0], fy[m][1], fy[m][2], fy[m][3], fy[m][4], g.a1y[jj], g.b1y[jj], g.c1y[jj], g.d1y[jj]);
+        T ddz = d1fc(fz[m][0], fz[m][1], fz[m][2], fz[m][3], fz[m][4], g.a1z[k], g.b1z[k], g.c1z[k], g.d1z[k]);
+        out[1 + m] = -ddx - ddy - ddz;
+    }
+    // J x B - xresd (t3dsdsc.f:1355-1360)
+    long c = n.c;
+    T rc = r0 + R[c];
+    T b1 = T(g.bx0[k]) + x.f[4][c], b2 = T(g.by0[k]) + x.f[5][c], b3 = T(g.bz0[k]) + x.f[6][c];
+    T j1 = cur.f[0][c], j2 = cur.f[1][c], j3 = cur.f[2][c];
+    out[1] = out[1] - T(g.rsx[k]) + j2 * b3 - j3 * b2;
+    out[2] = out[2] - T(g.rsy[k]) + j3 * b1 - j1 * b3;
+    out[3] = out[3] - T(g.rsz[k]) + j1 * b2 - j2 * b1;
+    // induction: dB/dt = -curl E (t3dsdsc.f:1438-1452)
+    out[4] = -n.Dy(g, e.f[2]) + n.Dz(g, e.f[1]);
+    out[5] = -n.Dz(g, e.f[0]) + n.Dx(g, e.f[2]);
+    out[6] = -n.Dx(g, e.f[1]) + n.Dy(g, e.f[0]);
+    // pressure (t3dsdsc.f:1550-1566): velocities at the stencil points
+    T vx[5], vy[5], vz[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        vx[s] = M1[xi[s]] / rx(xi[s]);
+        vy[s] = M2[yi[s]] / rx(yi[s]);
+        vz[s] = M3[zi[s]] / rz(zi[s], k - 2 + s);
+    }
+    T v1 = M1[c] / rc, v2 = M2[c] / rc, v3 = M3[c] / rc;
+    T px = n.Dx(g, P), py = n.Dy(g, P), pz = n.Dz(g, P) + T(g.dzp0[k]);
+    T divv = -d1fc(vx[0], vx[1], vx[2], vx[3], vx[4], g.a1x[i], g.b1x[i], g.c1x[i], g.d1x[i])
+             - d1fc(vy[0], vy[1], vy[2], vy[3], vy[4], g.a1y[jj], g.b1y[jj], g.c1y[jj], g.d1y[jj])
+             - d1fc(vz[0], vz[1], vz[2], vz[3], vz[4], g.a1z[k], g.b1z[k], g.c1z[k], g.d1z[k]);
+    T pc = T(g.p0[k]) + P[c];
+    out[7] = -px * v1 - py * v2 - pz * v3 + divv * g.gamma * pc
+             + (g.gamma - T(1)) * g.eta * (j1 * j1 + j2 * j2 + j3 * j3);
+    if (g.viscos) {   // t3dsdsc.f:1612-1634, 5-point second derivatives of v
+        // v at the x/y stencil points of the other components
+        T ux[5], uy[5], uz[5];
+        T af, ag, ah;
+        // af = lap(vx)
+#pragma unroll
+        for (int s = 0; s < 5; ++s) { uy[s] = M1[yi[s]] / rx(yi[s]); uz[s] = M1[zi[s]] / rz(zi[s], k - 2 + s); }
+        af = d1fc(vx[0], vx[1], vx[2], vx[3], vx[4], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i])
+           + d1fc(uy[0], uy[1], uy[2], uy[3], uy[4], g.a2y[jj], g.b2y[jj], g.c2y[jj], g.d2y[jj])
+           + d1fc(uz[0], uz[1], uz[2], uz[3], uz[4], g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
+#pragma unroll
+        for (int s = 0; s < 5; ++s) { ux[s] = M2[xi[s]] / rx(xi[s]); uz[s] = M2[zi[s]] / rz(zi[s], k - 2 + s); }
+        ag = d1fc(ux[0], ux[1], ux[2], ux[3], ux[4], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i])
+           + d1fc(vy[0], vy[1], vy[2], vy[3], vy[4], g.a2y[jj], g.b2y[jj], g.c2y[jj], g.d2y[jj])
+           + d1fc(uz[0], uz[1], uz[2], uz[3], uz[4], g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
+#pragma unroll
+        for (int s = 0; s < 5; ++s) { ux[s] = M3[xi[s]] / rx(xi[s]); uy[s] = M3[yi[s]] / rx(yi[s]); }
+        ah = d1fc(ux[0], ux[1], ux[2], ux[3], ux[4], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i])
+           + d1fc(uy[0], uy[1], uy[2], uy[3], uy[4], g.a2y[jj], g.b2y[jj], g.c2y[jj], g.d2y[jj])
+           + d1fc(vz[0], vz[1], vz[2], vz[3], vz[4], g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
+        out[1] = out[1] + g.mu * af;
+        out[2] = out[2] + g.mu * ag;
+        out[3] = out[3] + g.mu * ah;
+        out[7] = out[7] + g.mu * (v1 * af + v2 * ag + v3 * ah);
+    }
+    if (g.diffu) {    // t3dsdsc.f:1642-1661
+        T lr = n.D2x(g, R) + n.D2y(g, R) + (n.D2z(g, R) + T(g.d2rho0[k]));
+        T lp = n.D2x(g, P) + n.D2y(g, P) + (n.D2z(g, P) + T(g.d2p0[k]));
+        out[0] = out[0] + g.drho * lr;
+        out[7] = out[7] + g.dp * lp;
+    }
+}
+
+template <class T>
+__global__ void k_rhs(Geo<T> g, F8<T> x, F3<T> cur, F3<T> e, F8<T> xdif) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int jj = blockIdx.y, k = blockIdx.z;
+    bool zero, half;
+    int ks = wall_src(k, g.mz, zero, half);
+    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+    T out[NF];
+    if (zero) {
+#pragma unroll
+        for (int m = 0; m < NF; ++m) out[m] = T(0);
+    } else {
+        rhs_point(g, x, cur, e, i, jj, ks, out);
+        if (half) {
+#pragma unroll
+            for (int m = 0; m < NF; ++m) out[m] = T(0.5) * out[m];
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < NF; ++m) xdif.f[m][c] = out[m];
+}
+
+// ---------------------------------------------------------------------------------------
+// J0 added to the smoothed J1 (j0_mode FULL).
+template <class T>
+__global__ void k_add_j0(Geo<T> g, F3<T> cur) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int jj = blockIdx.y, k = blockIdx.z;
+    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+    cur.f[0][c] += T(g.j0x[k]);
+    cur.f[1][c] += T(g.j0y[k]);
+    cur.f[2][c] += T(g.j0z[k]);
+}
+
+// ---------------------------------------------------------------------------------------
+// RK4 stage updates (stepon t3dsdsc.f:1090-1132).
+//  Plain form (FP64, the reference's registers xfold=base, xm=acc, x):
+//   s1: acc = base + k*dt/6, x = base + k*dt/2;   s2: acc += k*dt/3, x = base + k*dt/2
+//   s3: acc += k*dt/3,   x = base + k*dt;         s4: x = acc + k*dt/6
+//  Compensated form (FP32): acc holds the increment only and the base update of stage 4
+//   is a Kahan sum with the per-node compensation comp.
+template <class T, bool KAHAN>
+__global__ void k_rk(long n, int stage, double dt, F8<T> x, F8<T> base, F8<T> acc, F8<T> comp, F8<T> k) {
+    long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    const T tdt = T(dt);
+#pragma unroll
+    for (int m = 0; m < NF; ++m) {
+        T kv = k.f[m][c];
+        if (!KAHAN) {
+            T b = base.f[m][c];
+            if (stage == 1) { acc.f[m][c] = b + kv * tdt / T(6.); x.f[m][c] = b + kv * tdt / T(2.); }
+            else if (stage == 2) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt / T(2.); }
+            else if (stage == 3) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt; }
+            else { x.f[m][c] = acc.f[m][c] + kv * tdt / T(6.); }
+        } else {
+            T b = base.f[m][c];
+            if (stage == 1) { acc.f[m][c] = kv * tdt / T(6.); x.f[m][c] = b + kv * tdt / T(2.); }
+            else if (stage == 2) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt / T(2.); }
+            else if (stage == 3) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt; }
+            else {
+                T inc = acc.f[m][c] + kv * tdt / T(6.);
+                T y = inc - comp.f[m][c];
+                T t = b + y;
+                comp.f[m][c] = (t - b) - y;
+                x.f[m][c] = t;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// FP64 reductions
+__device__ __forceinline__ double warp_min(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// CFL time step (setdt t3dsdsc.f:4709-4736) over the reference's region: k 0..mz-3,
+// j 0..my-2, i 0..mx-3 (t3dsdsc.f:4709-4711).  One block per (j,k) row pair chunk; writes
+// one partial minimum per block.
+template <class T>
+__global__ void k_cfl(Geo<T> g, F8<T> x, const double* xc, const double* yc, const double* zc,
+                      const double* dxs, const double* dys, const double* dzs, double cfl, double visc,
+                      double rcr, double gamma, double* partial) {
+    int jj = blockIdx.y, k = blockIdx.z;
+    double best = 100.;
+    if (k <= g.mz - 3 && jj <= g.my - 2) {
+        const double r0 = g.rho0[k], bx0 = g.bx0[k], by0 = g.by0[k], bz0 = g.bz0[k], p0 = g.p0[k];
+        for (int i = threadIdx.x; i <= g.mx - 3; i += blockDim.x) {
+            double rr = sqrt(xc[i] * xc[i] + yc[jj] * yc[jj] + zc[k] * zc[k]);
+            if (!(rr >= rcr)) continue;
+            long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+            double rho = r0 + (double)x.f[0][c];
+            double vx = (double)x.f[1][c] / rho, vy = (double)x.f[2][c] / rho, vz = (double)x.f[3][c] / rho;
+            double b1 = bx0 + (double)x.f[4][c], b2 = by0 + (double)x.f[5][c], b3 = bz0 + (double)x.f[6][c];
+            double va2 = (b1 * b1 + b2 * b2 + b3 * b3) / rho;
+            double cs2 = gamma * (p0 + (double)x.f[7][c]) / rho;
+            double vf = sqrt(fabs(va2 + cs2));
+            double dx = dxs[i], dy = dys[jj], dz = dzs[k];
+            double dtx = fabs(dx) / ((fabs(vx) + vf) / cfl + visc / dx / 2.);
+            double dty = fabs(dy) / ((fabs(vy) + vf) / cfl + visc / dy / 2.);
+            double dtz = fabs(dz) / ((fabs(vz) + vf) / cfl + visc / dz / 2.);
+            double d = fmin(fmin(dtx, dty), dtz);
+            // NaN must win so that a corrupted state is detected
+            if (d != d) best = d; else if (best == best) best = fmin(best, d);
+        }
+    }
+    __shared__ double sh[32];
+    // NaN-propagating warp min
+    double v = best;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double w = __shfl_down_sync(0xffffffffu, v, o);
+        v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? sh[lane] : 100.;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w = __shfl_down_sync(0xffffffffu, v, o);
+            v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
+        }
+        if (lane == 0) partial[(long)blockIdx.z * gridDim.y + blockIdx.y] = v;
+    }
+}
+
+// final reduction of partials by one block, fixed order
+__global__ void k_reduce_min(const double* partial, long n, double* out) {
+    double v = 100.;
+    for (long q = threadIdx.x; q < n; q += blockDim.x) {
+        double w = partial[q];
+        v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
+    }
+    __shared__ double sh[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        double w = __shfl_down_sync(0xffffffffu, v, o);
+        v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
+    }
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? sh[lane] : 100.;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double w = __shfl_down_sync(0xffffffffu, v, o);
+            v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
+        }
+        if (lane == 0) *out = v;
+    }
+}
+
+// Diagnostics partial sums per (j,k) row: mass, energy (trapezoid weights), and the
+// per-row extrema of J on the mid-y plane; partial layout [row][5]: mass, energy, jmax/jmin
+// handled separately.
+template <class T>
+__global__ void k_diag_rows(Geo<T> g, F8<T> x, const double* wx, const double* wy, const double* wz,
+                            double gamma, double* part) {
+    int jj = blockIdx.y, k = blockIdx.z;
+    const double r0 = g.rho0[k], bx0 = g.bx0[k], by0 = g.by0[k], bz0 = g.bz0[k], p0 = g.p0[k];
+    double sm = 0., se = 0.;
+    for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
+        long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+        double rho = r0 + (double)x.f[0][c];
+        double m1 = x.f[1][c], m2 = x.f[2][c], m3 = x.f[3][c];
+        double b1 = bx0 + (double)x.f[4][c], b2 = by0 + (double)x.f[5][c], b3 = bz0 + (double)x.f[6][c];
+        double p = p0 + (double)x.f[7][c];
+        double vol = wx[i];
+        sm += rho * vol;
+        se += (0.5 * (m1 * m1 + m2 * m2 + m3 * m3) / rho + p / (gamma - 1.) + 0.5 * (b1 * b1 + b2 * b2 + b3 * b3)) * vol;
+    }
+    __shared__ double s1[32], s2[32];
+    sm = warp_sum(sm); se = warp_sum(se);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { s1[wid] = sm; s2[wid] = se; }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        sm = lane < nw ? s1[lane] : 0.;
+        se = lane < nw ? s2[lane] : 0.;
+        sm = warp_sum(sm); se = warp_sum(se);
+        if (lane == 0) {
+            long row = (long)k * gridDim.y + jj;
+            part[2 * row] = sm * wy[jj] * wz[k];
+            part[2 * row + 1] = se * wy[jj] * wz[k];
+        }
+    }
+}
+
+// Reconnected flux partials per y row (one block per j): sum_x sqrt(Bz(z=0)^2+eps^2)*wx.
+template <class T>
+__global__ void k_diag_flux(Geo<T> g, F8<T> x, const double* wx, double* part) {
+    int jj = blockIdx.x;
+    double s = 0.;
+    for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
+        double bz;
+        if (g.mz % 2) {
+            int kc = (g.mz - 1) / 2;
+            bz = g.bz0[kc] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)kc * g.sz];
+        } else {
+            int ka = g.mz / 2 - 1, kb = g.mz / 2;
+            double za = g.bz0[ka] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)ka * g.sz];
+            double zb = g.bz0[kb] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)kb * g.sz];
+            bz = 0.5 * (za + zb);
+        }
+        s += sqrt(bz * bz + 1e-20) * wx[i];
+    }
+    __shared__ double sh[32];
+    s = warp_sum(s);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = s;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        s = lane < nw ? sh[lane] : 0.;
+        s = warp_sum(s);
+        if (lane == 0) part[jj] = s;
+    }
+}
+
+// J extrema on the mid-y plane (diagn t3dsdsc.f:1199-1214): one block per k row.
+template <class T>
+__global__ void k_diag_jext(Geo<T> g, F3<T> cur, int jm, double* part) {
+    int k = blockIdx.x;
+    double mx[3] = {-1e300, -1e300, -1e300}, mn[3] = {1e300, 1e300, 1e300};
+    for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
+        long c = (long)i + (long)jm * g.sy + (long)k * g.sz;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            double v = cur.f[m][c];
+            mx[m] = fmax(mx[m], v);
+            mn[m] = fmin(mn[m], v);
+        }
+    }
+    __shared__ double sh[6][32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        double a = warp_max(mx[m]), b = warp_min(mn[m]);
+        if (lane == 0) { sh[2 * m][wid] = a; sh[2 * m + 1][wid] = b; }
+    }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            double a = lane < nw ? sh[2 * m][lane] : -1e300;
+            double b = lane < nw ? sh[2 * m + 1][lane] : 1e300;
+            a = warp_max(a); b = warp_min(b);
+            if (lane == 0) { part[6 * k + 2 * m] = a; part[6 * k + 2 * m + 1] = b; }
+        }
+    }
+}
+
+// Final diagnostics reduction (one block, fixed order) -> out[9]; also raises the blow-up
+// flag when max Jy >= 1e7 (t3dsdsc.f:1232).
+__global__ void k_diag_final(const double* rows, long nrows, const double* fl, int my, const double* jext, int mz,
+                             double* out, int* blowup) {
+    __shared__ double sh[2][32];
+    double sm = 0., se = 0.;
+    for (long q = threadIdx.x; q < nrows; q += blockDim.x) { sm += rows[2 * q]; se += rows[2 * q + 1]; }
+    sm = warp_sum(sm); se = warp_sum(se);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { sh[0][wid] = sm; sh[1][wid] = se; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        double a = 0., b = 0.;
+        for (int w = 0; w < nw; ++w) { a += sh[0][w]; b += sh[1][w]; }
+        double f = 0.;
+        for (int j = 0; j < my; ++j) f += fl[j];
+        double e[6] = {-1e300, 1e300, -1e300, 1e300, -1e300, 1e300};
+        for (int k = 0; k < mz; ++k)
+            for (int m = 0; m < 3; ++m) {
+                e[2 * m] = fmax(e[2 * m], jext[6 * k + 2 * m]);
+                e[2 * m + 1] = fmin(e[2 * m + 1], jext[6 * k + 2 * m + 1]);
+            }
+        out[0] = a; out[1] = b; out[2] = f / my;
+        for (int q = 0; q < 6; ++q) out[3 + q] = e[q];
+        if (blowup && (fabs(e[2]) >= 1e7 || e[2] != e[2])) *blowup = 1;
+    }
+}
+
+}  // namespace dasha

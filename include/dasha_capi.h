@@ -1,0 +1,144 @@
+/*
+ * dasha_capi.h -- C-ABI of libdasha.so, the B200 (sm_100a) RK4 Hall-MHD step.
+ *
+ * The reference program (t3dsdsc.f) advances its state with two argument-less Fortran
+ * subroutines called from its main loop:
+ *     call setdt     (t3dsdsc.f:139,  body t3dsdsc.f:4694-4810)
+ *     call stepon    (t3dsdsc.f:171,  body t3dsdsc.f:1063-1185)
+ * and reads the current density through COMMON /var11/ cur after `call current`
+ * (t3dsdsc.f:2452-2500).  All data moves through COMMON blocks (mhd01.for:55-66,
+ * mhd02.for:1-6).  This header replaces those bodies: the state lives on the GPU inside an
+ * opaque context, and the Fortran loop calls the functions below through an ISO_C_BINDING
+ * interface (INTEGRATION.md shows the module).
+ *
+ * Conventions
+ *  - Every function returns 0 (DASHA_OK) or a DASHA_E_* code; no exception or exit() crosses
+ *    the ABI.  The text of the last error of a context is given by dasha_last_error().
+ *  - Host pointers are borrowed for the duration of a call only; copies finish before return.
+ *  - One host thread per context.  Kernels run in order on the context's own CUDA stream.
+ *  - Host state arrays use the reference's layout x(mxpr,my,mzpr,8) at a 1x1 process grid:
+ *    Fortran order, x fastest, a 2-node halo in x and z (mxpr = mx+4, mzpr = mz+4), none in
+ *    y.  ld1 (>= mx+4) and ld2 (>= my) are the first two leading dimensions; the third is
+ *    always mz+4.  Physical node (i,j,k), 0-based, is element
+ *        (i+2) + ld1*( j + ld2*( (k+2) + (mz+4)*m ) ),   m = 0..7 = rho, rho*v(3), B(3), p.
+ *    Halo entries are ignored on input and left untouched on output.
+ *  - x and y are periodic (true wrap); z is bounded by walls whose two outer node rows
+ *    follow the reference's fixed rows (t3dsdsc.f:1821-1857).
+ */
+#ifndef DASHA_CAPI_H
+#define DASHA_CAPI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dasha_ctx dasha_ctx;
+
+enum {
+    DASHA_OK = 0,
+    DASHA_E_INVALID = 1,      /* bad argument (null pointer, size, leading dimension) */
+    DASHA_E_UNSUPPORTED = 2,  /* an option the build does not implement */
+    DASHA_E_CUDA = 3,         /* a CUDA runtime error; the context should be destroyed */
+    DASHA_E_NOMEM = 4,        /* the grid does not fit in device memory */
+    DASHA_E_DT_COLLAPSE = 5,  /* dt < 0.1*dt0 or not finite: the guard of t3dsdsc.f:142-154 */
+    DASHA_E_BLOWUP = 6,       /* max Jy on the mid-y plane >= 1e7: the guard of t3dsdsc.f:1232 */
+    DASHA_E_STATE = 7,        /* call out of order (no equilibrium or state set yet) */
+    DASHA_E_NOSCRATCH = 8     /* a size beyond a fixed scratch limit */
+};
+
+/* Grid: node coordinates (FP64, host, borrowed).  Replaces gridpntnew2 (t3dsdsc.f:4380-4690)
+ * and the local slices of input (t3dsdsc.f:296-313).  periodic must be {1,1,0}. */
+typedef struct {
+    int mx, my, mz;
+    const double *x, *y, *z;
+    int periodic[3];
+} dasha_grid_c;
+
+/* Run-time constants and flags, mhd03.for:1-83 and COMMON /cst/ (mhd01.for:55).
+ *  gamma, cfl                      mhd03.for:60,71
+ *  eta (etan = eta0), mu (fmu0), drho (frho0), dp (fpr0)   foreta/formu t3dsdsc.f:6489-6532
+ *  di: Hall coefficient cht, uniform (replaces the radial profile of t3dsdsc.f:1398)
+ *  rcr: inner-sphere mask radius (mhd03.for:26); only rcr <= 0 (no mask) is supported
+ *  hall, viscos, diffu, total_e: mhd03.for:18-23 (total_e must be 1)
+ *  j0_mode: 0 = LITERAL (J = curl(B-B0), the reference's equations), 1 = FULL (J0 added)
+ *  filter_every: cadence of the post-step filter avrgtt (reference: every step = 1)
+ *  precision: 0 = FP64 state and arithmetic; 1 = FP32 perturbation + Kahan-compensated RK4 */
+typedef struct {
+    double gamma, eta, di, mu, drho, dp, cfl, rcr;
+    int hall, viscos, diffu, total_e, j0_mode;
+    int filter_every;
+    int precision;
+} dasha_params_c;
+
+#define DASHA_NDIAG 9
+
+/* Create a context on the current CUDA device: copies the grid, builds the stencil
+ * coefficients (input, t3dsdsc.f:336-606) and allocates all device buffers. */
+int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_ctx** out);
+
+/* Equilibrium as FP64 1-D z-profiles, length mz each: rho0, b0 = [bx0|by0|bz0] (3*mz), p0.
+ * Replaces the 3-D COMMON arrays rhoi, bxi, byi, bzi, pri (t3dsdsc.f:805-813) and computes
+ * the residual xresd of the pure equilibrium (t3dsdsc.f:816-834). */
+int dasha_set_equilibrium(dasha_ctx* ctx, const double* rho0, const double* b0, const double* p0);
+
+/* J0 = curl B0 as FP64 z-profiles [j0x|j0y|j0z] (3*mz), used when j0_mode = FULL.  Without
+ * this call FULL mode takes J0 from the z-derivative of b0 with the 4th-order stencil. */
+int dasha_set_equilibrium_current(dasha_ctx* ctx, const double* j0);
+
+/* Upload / download the total state x(mxpr,my,mzpr,8) (COMMON /var21/ x, mhd02.for:4). */
+int dasha_set_state(dasha_ctx* ctx, const double* x_f, long ld1, long ld2);
+int dasha_get_state(dasha_ctx* ctx, double* x_f, long ld1, long ld2);
+
+/* CFL time step of the current state (setdt, t3dsdsc.f:4694-4763): synchronises, returns dt.
+ * Also reports a latched blow-up (DASHA_E_BLOWUP) and dt collapse (DASHA_E_DT_COLLAPSE,
+ * dt < 0.1*dt0 with dt0 the first dt of the context, t3dsdsc.f:142). */
+int dasha_setdt(dasha_ctx* ctx, double time, double* dt_out);
+
+/* One RK4 step (stepon, t3dsdsc.f:1063-1185), enqueued asynchronously.  nstep is the step
+ * counter before the step: the post-step filter runs when nstep % filter_every == 0 and the
+ * blow-up guard (diagn) when nstep % 10 == 0. */
+int dasha_stepon(dasha_ctx* ctx, double time, double dt, int nstep);
+
+/* Smoothed current density cur(mxpr,my,mzpr,3) of the current state (current,
+ * t3dsdsc.f:2452-2500), same layout rules as the state. */
+int dasha_current(dasha_ctx* ctx, double* cur_f, long ld1, long ld2);
+
+/* One right-hand side xdif(mxpr,my,mzpr,8) = dx/dt of the current state at stage time t
+ * (right, t3dsdsc.f:1297-1673); the xdif smoothing avrg runs only when t != 0. */
+int dasha_rhs(dasha_ctx* ctx, double t, double* xdif_f, long ld1, long ld2);
+
+/* FP64 diagnostics of the current state, out[DASHA_NDIAG]:
+ *  [0] mass  sum(rho dV)      [1] energy  sum((rho v^2/2 + p/(gamma-1) + B^2/2) dV)
+ *  [2] reconnected flux  (1/my) sum_y sum_x sqrt(Bz(z=0)^2 + 1e-20) dx
+ *  [3..8] Jx max, Jx min, Jy max, Jy min, Jz max, Jz min on the mid-y plane (diagn,
+ *  t3dsdsc.f:1189-1235). */
+int dasha_diagnostics(dasha_ctx* ctx, double* out);
+
+/* Gradient of the final reconnected flux (out[2] of dasha_diagnostics) after nsteps RK4
+ * steps with the recorded dt sequence dt_seq[nsteps], starting from the current state, with
+ * respect to eta (*dPhi_deta) and to a psi perturbation on the (x,z) nodes (dPhi_dpsi[mx*mz],
+ * x fastest), where the perturbation enters the initial B as dBx = -Dz psi, dBz = Dx psi.
+ * snaps: number of stored step snapshots for checkpointing (>= 1).  FP64 contexts only.
+ * The state of the context is left unchanged. */
+int dasha_adjoint_flux_grad(dasha_ctx* ctx, int nsteps, const double* dt_seq, int snaps,
+                            double* dPhi_deta, double* dPhi_dpsi);
+
+/* Measurement helpers (no counterpart in the reference).
+ * dasha_timer(ctx, 0, NULL) records a start event on the context stream;
+ * dasha_timer(ctx, 1, &ms) records a stop event, waits for it and returns the elapsed ms.
+ * dasha_profile(ctx, 1) brackets every later kernel launch with CUDA events on the context
+ * stream (this slows launches down; use it for breakdowns, not for headline numbers);
+ * dasha_profile_read(ctx, n, names, ms, launches, bytes) waits, then fills up to n rows:
+ * names (32 chars each), total ms, launch count and the algorithmic bytes of one launch per
+ * kernel kind, returns the number of rows in *n, and clears the record. */
+int dasha_timer(dasha_ctx* ctx, int op, double* ms);
+int dasha_profile(dasha_ctx* ctx, int enable);
+int dasha_profile_read(dasha_ctx* ctx, int* n, char* names, double* ms, long* launches, double* bytes);
+
+const char* dasha_last_error(dasha_ctx* ctx);
+void dasha_destroy(dasha_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
