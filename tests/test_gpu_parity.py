@@ -183,7 +183,9 @@ def test_blowup_guard():
     cfg = SMALL
     d = capi.gem_context(cfg, 0)
     X = d.get_state()
-    X[4, 10, cfg.my // 2, 7] += 1e8          # huge B spike makes |Jy| >= 1e7 on the mid-y plane
+    # a B spike on the mid-y plane; the filter and the 4 smoothing passes of J damp a single
+    # spike by ~1e-3, so it must be large for max Jy to reach the 1e7 guard
+    X[4, 10, cfg.my // 2, 7] += 1e13
     d.set_state(X)
     dt = 1e-12
     d.stepon(0.0, dt, 0)                     # nstep % 10 == 0 runs the guard
