@@ -58,6 +58,7 @@ SIGNATURES = {
     "dasha_timer": ([_P, C.c_int, _D], C.c_int),
     "dasha_profile": ([_P, C.c_int], C.c_int),
     "dasha_profile_read": ([_P, C.POINTER(C.c_int), C.c_char_p, _D, C.POINTER(C.c_long), _D], C.c_int),
+    "dasha_current_noalloc": ([C.POINTER(GridC), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "dasha_last_error": ([_P], C.c_char_p),
     "dasha_destroy": ([_P], None),
 }
@@ -225,6 +226,15 @@ class Dasha:
             time += dt
             dts.append(dt)
         return time, np.array(dts)
+
+
+def current_noalloc(x, y, z, db_ptr: int, cur_ptr: int, stream: int = 0) -> int:
+    """dasha_current_noalloc on caller device arrays (raw device addresses); returns the status."""
+    lib = load()
+    x, y, z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
+    g = GridC(x.size, y.size, z.size, _dp(x), _dp(y), _dp(z), (C.c_int * 3)(1, 1, 0))
+    return lib.dasha_current_noalloc(C.byref(g), C.c_void_p(db_ptr), C.c_void_p(cur_ptr),
+                                     C.c_void_p(stream) if stream else None)
 
 
 def gem_context(cfg: harris.RunConfig, precision: int = 0, seed_v: int = harris.SEED_V, **over) -> Dasha:

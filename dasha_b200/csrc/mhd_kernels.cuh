@@ -452,7 +452,7 @@ __global__ void k_cfl(Geo<T> g, F8<T> x, const double* xc, const double* yc, con
 }
 
 // final reduction of partials by one block, fixed order
-__global__ void k_reduce_min(const double* partial, long n, double* out) {
+static __global__ void k_reduce_min(const double* partial, long n, double* out) {
     double v = 100.;
     for (long q = threadIdx.x; q < n; q += blockDim.x) {
         double w = partial[q];
@@ -583,7 +583,7 @@ __global__ void k_diag_jext(Geo<T> g, F3<T> cur, int jm, double* part) {
 
 // Final diagnostics reduction (one block, fixed order) -> out[9]; also raises the blow-up
 // flag when max Jy >= 1e7 (t3dsdsc.f:1232).
-__global__ void k_diag_final(const double* rows, long nrows, const double* fl, int my, const double* jext, int mz,
+static __global__ void k_diag_final(const double* rows, long nrows, const double* fl, int my, const double* jext, int mz,
                              double* out, int* blowup) {
     __shared__ double sh[2][32];
     double sm = 0., se = 0.;

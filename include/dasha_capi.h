@@ -135,6 +135,23 @@ int dasha_timer(dasha_ctx* ctx, int op, double* ms);
 int dasha_profile(dasha_ctx* ctx, int enable);
 int dasha_profile_read(dasha_ctx* ctx, int* n, char* names, double* ms, long* launches, double* bytes);
 
+/* Smoothed current density without any device allocation.  No counterpart in the reference:
+ * for callers that cannot call cudaMalloc (their device memory is owned by a pool or a
+ * budget, or the allocator must not be called at that point).  Computes what dasha_current
+ * computes for j0_mode LITERAL, J = S^4(curl(B - B0)) with the wall rows, from caller device
+ * arrays: db_dev = B - B0 and cur_dev = J, each 3 fields of mx*my*mz FP64 values, node
+ * (i,j,k) at i + mx*(j + my*k), field stride mx*my*mz.  Work is enqueued on `stream` (a
+ * cudaStream_t, NULL for the default stream).  The ping-pong buffer and the stencil tables
+ * live in one static device array of DASHA_NOALLOC_SCRATCH_DOUBLES doubles (about 26 MB) that
+ * every GPU loading the library holds until exit; grids above DASHA_NOALLOC_MAX_CELLS nodes
+ * or DASHA_NOALLOC_MAX_AXIS nodes per axis return DASHA_E_NOSCRATCH.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Calls share the array: calls that overlap on the GPU race. */
+#define DASHA_NOALLOC_MAX_CELLS (1L << 20)
+#define DASHA_NOALLOC_MAX_AXIS 4096
+#define DASHA_NOALLOC_SCRATCH_DOUBLES (3L * DASHA_NOALLOC_MAX_CELLS + 3L * 7 * DASHA_NOALLOC_MAX_AXIS)
+int dasha_current_noalloc(const dasha_grid_c* grid, const double* db_dev, double* cur_dev, void* stream);
+
 const char* dasha_last_error(dasha_ctx* ctx);
 void dasha_destroy(dasha_ctx* ctx);
 
