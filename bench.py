@@ -48,6 +48,16 @@ def pin_device(local_rank: int, world: int):
     os.environ["CUDA_VISIBLE_DEVICES"] = devs[local_rank]
 
 
+def max_over_ranks(value: float, dist) -> float:
+    """Max of a per-rank time over all ranks (the replicas' step time is the slowest rank's)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -195,11 +205,7 @@ def run_dasha(args, rank, world):
         n += 1
     ms = d.timer_stop()
     ck = clocks.stop()
-    if dist:
-        import torch
-        tt = torch.tensor([ms], dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dist)
     cells = cfg.cells
     value = world * cells * args.steps / (ms / 1e3)
 
@@ -246,11 +252,7 @@ def run_dasha(args, rank, world):
     if rc:
         raise capi.DashaError(rc, "get_state")
     e2e_s = time.perf_counter() - t0
-    if dist:
-        import torch
-        tt = torch.tensor([e2e_s], dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     state_bytes = 8 * cells * 8
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
            "h2d_bytes_per_step": state_bytes / args.steps,

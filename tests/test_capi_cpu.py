@@ -1,0 +1,85 @@
+"""The C-ABI library without a GPU: it loads, exports every function include/dasha_capi.h
+declares, rejects bad arguments before touching the device, and the product has no CPU
+fallback.  Also cross-checks the library's stencil-weight solver (coef.h) against the
+oracle's closed forms of the reference (t3dsdsc.f:336-504)."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from dasha_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "dasha_capi.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(dasha_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = capi.load()
+    names = declared_functions()
+    assert len(names) >= 15
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in capi.SIGNATURES, n
+
+
+def test_missing_library_fails_loudly(tmp_path):
+    saved = capi._lib
+    capi._lib = None
+    try:
+        with pytest.raises(RuntimeError):
+            capi.load(str(tmp_path / "nope.so"))
+    finally:
+        capi._lib = saved
+
+
+def test_argument_checks_need_no_device():
+    lib = capi.load()
+    h = ctypes.c_void_p()
+    assert lib.dasha_create(None, None, ctypes.byref(h)) == capi.E_INVALID
+    x = np.arange(4.0)
+    g = capi.GridC(4, 8, 8, capi._dp(x), capi._dp(x), capi._dp(x), (ctypes.c_int * 3)(1, 1, 0))
+    p = capi.ParamsC(gamma=5 / 3, cfl=0.4, total_e=1)
+    assert lib.dasha_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == capi.E_INVALID   # mx < 5
+    y = np.arange(8.0)
+    g = capi.GridC(8, 8, 8, capi._dp(y), capi._dp(y), capi._dp(y), (ctypes.c_int * 3)(0, 1, 0))
+    assert lib.dasha_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == capi.E_UNSUPPORTED
+    dt = ctypes.c_double()
+    assert lib.dasha_setdt(None, 0.0, ctypes.byref(dt)) == capi.E_INVALID
+    assert lib.dasha_stepon(None, 0.0, 0.1, 0) == capi.E_INVALID
+    assert lib.dasha_diagnostics(None, None) == capi.E_INVALID
+    # the scratch-free entry point rejects oversize grids before any device call
+    big = np.arange(2048.0)
+    gb = capi.GridC(2048, 1024, 8, capi._dp(big), capi._dp(big), capi._dp(big), (ctypes.c_int * 3)(1, 1, 0))
+    assert lib.dasha_current_noalloc(ctypes.byref(gb), ctypes.c_void_p(1), ctypes.c_void_p(1), None) == capi.E_NOSCRATCH
+
+
+def test_library_stencil_weights_match_reference_closed_forms(tmp_path):
+    """coef.h solves the 4x4 exactness system; the oracle uses the reference's closed forms."""
+    from oracle.oracle import Oracle
+    src = tmp_path / "w.cpp"
+    src.write_text('#include "coef.h"\n#include <cstdio>\nint main(int c, char** v){double h[4];'
+                   'for(int i=0;i<4;++i) std::sscanf(v[1+i], "%lf", &h[i]);'
+                   'double w1[4], w2[4]; dasha::stencil_weights(h[0],h[1],h[2],h[3],1,w1);'
+                   'dasha::stencil_weights(h[0],h[1],h[2],h[3],2,w2);'
+                   'for(int i=0;i<4;++i) std::printf("%.17g %.17g\\n", w1[i], w2[i]); return 0;}')
+    exe = tmp_path / "w"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "dasha_b200", "csrc"), str(src), "-o", str(exe)],
+                   check=True)
+    rng = np.random.default_rng(11)
+    z = np.concatenate([[0.0], np.cumsum(rng.uniform(0.3, 1.7, 19))])
+    o = Oracle(np.arange(8.0), np.arange(8.0), z)
+    co = o.coefficients(2)
+    for k in range(2, z.size - 2):
+        hs = [z[k + 1] - z[k], z[k] - z[k - 1], z[k + 2] - z[k], z[k] - z[k - 2]]
+        out = subprocess.run([str(exe)] + ["%.17g" % v for v in hs], capture_output=True, text=True, check=True).stdout
+        w = np.array([[float(t) for t in line.split()] for line in out.strip().splitlines()])
+        np.testing.assert_allclose(w[:, 0], co[0:4, k], rtol=1e-10, atol=1e-12)
+        np.testing.assert_allclose(w[:, 1], co[4:8, k], rtol=1e-9, atol=1e-11)

@@ -1,0 +1,150 @@
+"""Known-answer tests of the CPU oracle, derived from the reference's own formulas (the
+reference ships no tests or golden vectors; parity is unpinned, so these pin the restatement
+to the mathematics it states)."""
+import numpy as np
+import pytest
+
+from dasha_b200 import harris
+
+
+def _oracle(x, y, z, **kw):
+    from oracle.oracle import Oracle
+    return Oracle(x, y, z, **kw)
+
+
+def _rand_grid(n, rng, L=10.0):
+    h = rng.uniform(0.5, 1.5, n)
+    c = np.concatenate([[0.0], np.cumsum(h[:-1])])
+    return c * (L / (c[-1] + h[-1]))
+
+
+def test_first_and_second_derivative_exact_to_degree_4():
+    """t3dsdsc.f:336-504: 5-point weights exact for polynomials of degree <= 4 (z: stretched,
+    non-uniform; evaluated at the interior rows)."""
+    rng = np.random.default_rng(3)
+    x = np.linspace(-4, 4, 16, endpoint=False)
+    y = np.linspace(-2, 2, 8, endpoint=False)
+    z = _rand_grid(24, rng) - 5.0
+    o = _oracle(x, y, z)
+    co = o.coefficients(2)
+    for k in range(2, z.size - 2):
+        zz = z[k - 2:k + 3]
+        for deg in range(0, 5):
+            f = (zz - z[k]) ** deg
+            f0 = f[2]
+            d1 = co[0, k] * (f[3] - f0) + co[1, k] * (f0 - f[1]) + co[2, k] * (f[4] - f0) + co[3, k] * (f0 - f[0])
+            d2 = co[4, k] * (f[3] - f0) + co[5, k] * (f0 - f[1]) + co[6, k] * (f[4] - f0) + co[7, k] * (f0 - f[0])
+            assert abs(d1 - (1.0 if deg == 1 else 0.0)) < 1e-9, (k, deg, d1)
+            assert abs(d2 - (2.0 if deg == 2 else 0.0)) < 1e-8, (k, deg, d2)
+
+
+def test_uniform_coefficients_are_classic_4th_order():
+    x = np.arange(16) * 0.5
+    o = _oracle(x, np.arange(8) * 1.0, np.arange(12) * 0.25)
+    a1, b1, c1, d1 = o.coefficients(0)[:4, 5]
+    h = 0.5
+    # (8(f+ - f-) - (f++ - f--)) / 12h in the a,b,c,d form
+    np.testing.assert_allclose([a1, b1, c1, d1], [8 / (12 * h), 8 / (12 * h), -1 / (12 * h), -1 / (12 * h)], rtol=1e-12)
+
+
+def test_difc_uniform_is_second_difference():
+    """t3dsdsc.f:5618-5620: difc = f+ - 2 f0 + f- on a uniform grid."""
+    x = np.arange(16) * 0.5
+    y = np.arange(8) * 0.5
+    z = np.arange(12) * 0.5
+    o = _oracle(x, y, z)
+    rng = np.random.default_rng(0)
+    f = rng.standard_normal((12, 8, 16))
+    g = o.smooth_pass(f, 1)      # f + (1/8) * (difc_x + difc_y + difc_z) on interior rows
+    lap = (np.roll(f, 1, 2) + np.roll(f, -1, 2) + np.roll(f, 1, 1) + np.roll(f, -1, 1) - 4 * f)
+    lap[1:-1] += f[2:] + f[:-2] - 2 * f[1:-1]
+    exp = f + 0.125 * lap
+    np.testing.assert_allclose(g[2:-2], exp[2:-2], rtol=0, atol=1e-13)
+    np.testing.assert_array_equal(g[:2], f[:2])
+
+
+def test_equilibrium_is_steady():
+    """x = eq: J1 = 0, v = 0, p - p0 = 0, so every RHS term vanishes (LITERAL equations)."""
+    cfg = harris.RunConfig("eq", 16, 8, 24, True, 0.005, 0.5, 1)
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
+    o = _oracle(x, y, z)
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    o.set_equilibrium(rho0, b0, p0)
+    X = harris.gem_state(x, y, z, noise_amp=0.0)
+    X[4] = b0[0][:, None, None]
+    X[6] = 0.0
+    o.set_state(X)
+    np.testing.assert_array_equal(o.rhs(0.5), 0.0)
+    assert np.abs(o.residual()).max() == 0.0
+
+
+def test_full_j0_residual_is_j0_cross_b0():
+    cfg = harris.RunConfig("eq", 16, 8, 24, True, 0.005, 0.5, 1, j0_mode=1)
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
+    o = _oracle(x, y, z, j0_mode=1)
+    rho0, b0, p0, j0 = harris.harris_profiles(z)
+    o.set_equilibrium(rho0, b0, p0, j0)
+    r = o.residual()
+    kk = slice(2, z.size - 2)
+    np.testing.assert_allclose(r[2, kk], (-j0[1] * b0[0])[kk, None, None] * np.ones((1, 8, 16)), rtol=1e-14)
+    np.testing.assert_array_equal(r[0, kk], 0.0)
+
+
+def test_gem_mirror_symmetry():
+    """Noise-free GEM state on a z-symmetric grid: rho, Bz, p even in z; vz, Bx, By odd."""
+    cfg = harris.RunConfig("sym", 16, 8, 20, True, 0.005, 0.5, 3)
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
+    o = _oracle(x, y, z, eta=cfg.eta, di=cfg.di)
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    o.set_equilibrium(rho0, b0, p0)
+    o.set_state(harris.gem_state(x, y, z, noise_amp=0.0))
+    o.run(3)
+    X = o.get_state()
+    F = X[:, ::-1]
+    for m, sign in [(0, 1), (1, 1), (2, 1), (3, -1), (4, -1), (5, -1), (6, 1), (7, 1)]:
+        scale = max(np.abs(X[m]).max(), 1e-30)
+        assert np.abs(X[m] - sign * F[m]).max() / scale < 1e-10, m
+
+
+def test_mass_nearly_conserved_and_dt_positive():
+    cfg = harris.RunConfig("m", 16, 8, 24, False, 0.005, 0.5, 4)
+    from oracle.oracle import gem_oracle
+    o = gem_oracle(cfg)
+    m0 = o.diagnostics()[0]
+    _, dts = o.run(4)
+    assert np.all(dts > 0)
+    assert abs(o.diagnostics()[0] - m0) / m0 < 1e-4
+
+
+def test_setdt_uniform_state_matches_formula():
+    """setdt T:4709-4736 for a uniform state at rest: dt = dx / (c_f/cfl + eta/(2 dx))."""
+    x = np.arange(16) * 0.5
+    y = np.arange(8) * 0.5
+    z = np.arange(12) * 0.25
+    o = _oracle(x, y, z, eta=0.01, cfl=0.4)
+    mz = z.size
+    o.set_equilibrium(np.ones(mz), np.zeros(3 * mz), 0.5 * np.ones(mz))
+    X = np.zeros((8, mz, 8, 16))
+    X[0] = 1.0
+    X[4] = 0.5
+    X[7] = 0.5
+    o.set_state(X)
+    cf = np.sqrt(0.25 + 5.0 / 3.0 * 0.5)
+    dz = 0.25
+    exp = dz / (cf / 0.4 + 0.01 / dz / 2.0)
+    assert abs(o.setdt() - exp) < 1e-15
+
+
+def test_two_fp64_builds_agree_closely():
+    """The spread of two FP64 builds (FMA contraction off / on) after a few steps sets the scale
+    of the GPU FP64 parity tolerance."""
+    from oracle.oracle import gem_oracle
+    cfg = harris.RunConfig("spread", 32, 16, 32, False, 0.005, 0.5, 5)
+    a = gem_oracle(cfg)
+    b = gem_oracle(cfg, variant="_fma")
+    _, dts = a.run(5)
+    b.run(5, dts=dts)
+    A, B = a.get_state(), b.get_state()
+    scale = np.abs(A).reshape(8, -1).max(axis=1)
+    spread = (np.abs(A - B).reshape(8, -1).max(axis=1) / scale).max()
+    assert spread < 1e-11, spread
