@@ -37,7 +37,8 @@ class ParamsC(C.Structure):
     _fields_ = [("gamma", C.c_double), ("eta", C.c_double), ("di", C.c_double), ("mu", C.c_double),
                 ("drho", C.c_double), ("dp", C.c_double), ("cfl", C.c_double), ("rcr", C.c_double),
                 ("hall", C.c_int), ("viscos", C.c_int), ("diffu", C.c_int), ("total_e", C.c_int),
-                ("j0_mode", C.c_int), ("filter_every", C.c_int), ("precision", C.c_int)]
+                ("j0_mode", C.c_int), ("filter_every", C.c_int), ("precision", C.c_int),
+                ("dt_whistler", C.c_int)]
 
 
 # every symbol include/dasha_capi.h declares, with its argument types
@@ -89,7 +90,7 @@ def _dp(a: np.ndarray):
 def make_params(cfg: harris.RunConfig, precision: int = 0, **over) -> ParamsC:
     p = ParamsC(gamma=cfg.gamma, eta=cfg.eta, di=cfg.di, mu=0.0, drho=0.0, dp=0.0, cfl=cfg.cfl, rcr=0.0,
                 hall=cfg.hall, viscos=1, diffu=1, total_e=1, j0_mode=cfg.j0_mode,
-                filter_every=cfg.filter_every, precision=precision)
+                filter_every=cfg.filter_every, precision=precision, dt_whistler=cfg.dt_whistler)
     for k, v in over.items():
         setattr(p, k, v)
     return p

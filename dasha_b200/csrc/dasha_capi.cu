@@ -87,6 +87,7 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
     *out = nullptr;
     if (!grid || !params || !grid->x || !grid->y || !grid->z) return DASHA_E_INVALID;
     if (grid->mx < 5 || grid->my < 5 || grid->mz < 7) return DASHA_E_INVALID;
+    if (grid->mx % 32 != 0) return DASHA_E_UNSUPPORTED;   // the z-marching tiles are 32 nodes wide in x
     if (!(grid->periodic[0] == 1 && grid->periodic[1] == 1 && grid->periodic[2] == 0)) return DASHA_E_UNSUPPORTED;
     const dasha_params_c& p = *params;
     if (p.precision != 0 && p.precision != 1) return DASHA_E_INVALID;

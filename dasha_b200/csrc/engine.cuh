@@ -3,6 +3,7 @@
 #pragma once
 #include "dasha_capi.h"
 #include "mhd_kernels.cuh"
+#include "zm_kernels.cuh"
 #include <cuda_runtime.h>
 #include <string>
 #include <vector>
@@ -140,7 +141,7 @@ public:
 
     Status init(int mx_, int my_, int mz_, const dasha_params_c& p, cudaStream_t st_, const HostTables& H) {
         mx = mx_; my = my_; mz = mz_; N = (long)mx * my * mz; P = p; st = st_;
-        int nfield = 8 * 4 + (KAHAN ? 8 : 0) + 18 + 1;
+        int nfield = 8 * 4 + (KAHAN ? 8 : 0) + 18;
         size_t fbytes = ((size_t)N * sizeof(T) + 255) & ~(size_t)255;
         size_t freeb = 0, totb = 0;
         DASHA_CK(cudaMemGetInfo(&freeb, &totb));
@@ -159,21 +160,21 @@ public:
         for (int b = 0; b < 2; ++b) for (int m = 0; m < 3; ++m) cur[b][m] = take();
         for (int b = 0; b < 2; ++b) for (int m = 0; m < 3; ++m) E[b][m] = take();
         for (int b = 0; b < 2; ++b) for (int m = 0; m < 3; ++m) Hh[b][m] = take();
-        cr = take();
         DASHA_CK(cudaMemsetAsync(pool, 0, fbytes * nfield, st));
 
         // T tables: per axis 8 coefficients + wp + wm, plus cbx
         int nx[3] = {mx, my, mz};
         long ntab = 0;
-        for (int d = 0; d < 3; ++d) ntab += 10L * nx[d];
+        for (int d = 0; d < 3; ++d) ntab += 11L * nx[d];
         ntab += mx;
         std::vector<T> ht(ntab);
-        long off[3][10], offcb;
+        long off[3][11], offcb;
         long o = 0;
         for (int d = 0; d < 3; ++d)
-            for (int q2 = 0; q2 < 10; ++q2) {
+            for (int q2 = 0; q2 < 11; ++q2) {
                 off[d][q2] = o;
-                const std::vector<double>& src = q2 < 8 ? H.coef[d][q2] : (q2 == 8 ? H.wp[d] : H.wm[d]);
+                const std::vector<double>& src =
+                    q2 < 8 ? H.coef[d][q2] : (q2 == 8 ? H.wp[d] : (q2 == 9 ? H.wm[d] : H.coord[d]));
                 for (int i = 0; i < nx[d]; ++i) ht[o + i] = T(src[i]);
                 o += nx[d];
             }
@@ -191,7 +192,8 @@ public:
             *w2[d][0] = t + off[d][8]; *w2[d][1] = t + off[d][9];
         }
         g.cbx = t + offcb;
-        g.cr = cr;
+        g.cr = nullptr;
+        g.xc = t + off[0][10]; g.yc = t + off[1][10]; g.zc = t + off[2][10];
         g.eta = T(p.eta); g.di = T(p.di); g.gamma = T(p.gamma); g.mu = T(p.mu); g.drho = T(p.drho); g.dp = T(p.dp);
         g.hall = p.hall; g.viscos = p.viscos && p.mu != 0.0; g.diffu = p.diffu && (p.drho != 0.0 || p.dp != 0.0);
 
@@ -231,8 +233,7 @@ public:
 
         blk = dim3(std::min(128, ((mx + 31) / 32) * 32));
         grd = dim3((mx + blk.x - 1) / blk.x, my, mz);
-        k_init_cr<T><<<grd, blk, 0, st>>>(mx, my, mz, xc, yc, zc, cr);
-        DASHA_CK(cudaGetLastError());
+        DASHA_CK(zs_attr());
         DASHA_CK(cudaStreamSynchronize(st));
         return Status::ok();
     }
@@ -355,58 +356,171 @@ public:
     static F8<T> f8(T* const* p) { F8<T> r; for (int m = 0; m < 8; ++m) r.f[m] = p[m]; return r; }
     static F3<T> f3(T* const* p) { F3<T> r; for (int m = 0; m < 3; ++m) r.f[m] = p[m]; return r; }
 
-    // smoothed current of state xs into cur[0] (current, t3dsdsc.f:2452-2500)
+    // ---- z-marching launches ----
+    static constexpr int TX = 32, TY = 8;
+    int zchunk(int gxy, int minlen) const {
+        int nch = (4 * 148 * 8 + gxy - 1) / gxy;
+        nch = std::max(1, std::min(nch, mz / minlen));
+        return (mz + nch - 1) / nch;
+    }
+    // k_zpass tiling: 32 x 16 columns per CTA (256 threads, 2 rows each), 4 planes in flight
+    static constexpr int ZTX = 32, ZTYH = 8, ZRY = sizeof(T) == 4 ? 2 : 1, ZD = 4;
+    template <int NF>
+    using ZPc = ZP<T, NF, ZTX, ZTYH, ZRY, ZD>;
+    // one smoothing pass of NF fields: src -> epi
+    template <int NF, unsigned KINDS, class Epi>
+    void zp(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
+        dim3 gg(mx / ZTX, (my + ZPc<NF>::TY - 1) / ZPc<NF>::TY, 1);
+        int ch = zchunk(gg.x * gg.y, 16);
+        gg.z = (mz + ch - 1) / ch;
+        DASHA_LAUNCH(tag, bytes, (k_zpass<T, NF, KINDS, ZTX, ZTYH, ZRY, ZD, Epi>
+                                  <<<gg, ZTX * ZTYH, ZPc<NF>::smem(), st>>>(g, src, epi, ch)));
+    }
+    template <int NF, unsigned KINDS, class Epi>
+    static cudaError_t zp_attr1() {
+        return cudaFuncSetAttribute(k_zpass<T, NF, KINDS, ZTX, ZTYH, ZRY, ZD, Epi>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZPc<NF>::smem());
+    }
+    cudaError_t zs_attr() {
+        cudaError_t e;
+        if ((e = zp_attr1<3, 0u, EpiStore<T, 3>>())) return e;
+        if ((e = zp_attr1<3, KIND_H, EpiStore<T, 3>>())) return e;
+        if ((e = zp_attr1<3, KIND_H, EpiAcc<T, 3>>())) return e;
+        if ((e = zp_attr1<4, 0u, EpiStore<T, 4>>())) return e;
+        if ((e = zp_attr1<4, KIND_B4, EpiStore<T, 4>>())) return e;
+        if ((e = zp_attr1<4, 0u, EpiRK<T, 4, KAHAN>>())) return e;
+        if ((e = zp_attr1<4, KIND_B4, EpiRK<T, 4, KAHAN>>())) return e;
+        if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ZS2<T, 5, ZTX, 8>::smem(true))))
+            return e;
+        return cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpInduction<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ZS2<T, 3, ZTX, 8>::smem(false));
+    }
+    static constexpr int HMINB = sizeof(T) == 4 ? 2 : 1;   // CTAs per SM asked of the register allocator
+    static SrcFields<T, 3> src3(T* const* p) { SrcFields<T, 3> s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
+    static SrcFields<T, 8> src8(T* const* p) { SrcFields<T, 8> s; for (int q = 0; q < 8; ++q) s.f[q] = p[q]; return s; }
+    static EpiStore<T, 3> st3(T* const* p) { EpiStore<T, 3> s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
+    static EpiStore<T, 8> st8(T* const* p) { EpiStore<T, 8> s; for (int q = 0; q < 8; ++q) s.f[q] = p[q]; return s; }
+    static constexpr unsigned KIND_H = 1u | (1u << 2) | (1u << 4);                 // 1/8 for 3 fields
+    static constexpr unsigned KIND_X = (2u << 8) | (2u << 10) | (2u << 12);         // B with the x profile
+    static constexpr unsigned KIND_B4 = 2u | (2u << 2) | (2u << 4);                 // fields 4..7: B1 B2 B3 p
+
+    // one avrg/avrgtt pass over the 8 state-like fields, as two 4-field launches (rho, m) and
+    // (B, p); mk(lo) builds the epilogue of fields lo..lo+3
+    template <class MkEpi>
+    void pass8(const char* tag, double bytes_per_cell, T* const* in, MkEpi mk) {
+        SrcFields<T, 4> a, b;
+        for (int q = 0; q < 4; ++q) { a.f[q] = in[q]; b.f[q] = in[4 + q]; }
+        zp<4, 0u>(tag, 0.5 * bytes_per_cell * N * sizeof(T), a, mk(0));
+        zp<4, KIND_B4>(tag, 0.5 * bytes_per_cell * N * sizeof(T), b, mk(4));
+    }
+    static EpiStore<T, 4> st4(T* const* p, int lo) { EpiStore<T, 4> s; for (int q = 0; q < 4; ++q) s.f[q] = p[lo + q]; return s; }
+
+    T** curF = nullptr;   // smoothed current after launch_current
+    T** Ef = nullptr;     // total E after launch_rhs_raw
+
+    // n smoothing passes of 3 fields, ping-pong between a and b starting from a; returns the
+    // buffer holding the result
+    template <unsigned KINDS>
+    T** passes3(const char* tag, T** a, T** b, int n) {
+        for (int p = 0; p < n; ++p) {
+            T** in = (p & 1) ? b : a;
+            T** out = (p & 1) ? a : b;
+            zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+        }
+        return (n & 1) ? b : a;
+    }
+
+    // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
     void launch_current(T* const* xs) {
         T* bb[3] = {xs[4], xs[5], xs[6]};
         DASHA_LAUNCH("k_curl", 6.0 * N * sizeof(T), k_curl<T><<<grd, blk, 0, st>>>(g, f3(bb), f3(cur[0])));
-        for (int pass = 0; pass < 4; ++pass) smooth<3>(cur[pass & 1], cur[(pass + 1) & 1], nullptr, 0u);
-        if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(cur[0])));
+        curF = passes3<0u>("k_zpass_J", cur[0], cur[1], 4);
+        if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(curF)));
     }
 
-    // xdif of state xs into K
-    void launch_rhs(T* const* xs, bool smooth_xdif) {
+    // E_total and the raw RHS of state xs into K (wall rows applied)
+    void launch_rhs_raw(T* const* xs) {
         launch_current(xs);
-        DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(cur[0]), f3(E[0])));
-        for (int pass = 0; pass < 4; ++pass) smooth<3>(E[pass & 1], E[(pass + 1) & 1], nullptr, 0u);
+        T** cother = curF == cur[0] ? cur[1] : cur[0];
+        (void)cother;
+        // E0 = -v x B + eta J at every node, then avrgE's 4 passes (t3dsdsc.f:1367-1389)
+        DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
+        Ef = passes3<0u>("k_zpass_E", E[0], E[1], 4);
         if (P.hall) {
-            DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(cur[0]), f3(Hh[0])));
-            const unsigned k18 = 1u | (1u << 2) | (1u << 4);
-            for (int pass = 0; pass < 4; ++pass) smooth<3>(Hh[pass & 1], Hh[(pass + 1) & 1], nullptr, k18);
-            smooth<3>(Hh[0], E[0], E[0], k18);   // 5th pass accumulated into E
+            DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(Hh[0])));
+            T** h = passes3<KIND_H>("k_zpass_H", Hh[0], Hh[1], 4);
+            EpiAcc<T, 3> ea;
+            for (int q = 0; q < 3; ++q) { ea.f[q] = Ef[q]; ea.a[q] = Ef[q]; }
+            zp<3, KIND_H>("k_zpass_H5acc", 9.0 * N * sizeof(T), src3(h), ea);   // 5th pass added into E
         }
-        DASHA_LAUNCH("k_rhs", 22.0 * N * sizeof(T), k_rhs<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(cur[0]), f3(E[0]), f8(K)));
-        if (smooth_xdif) {   // avrg: 2 passes, B with the x-profile coefficient
-            T* tmp[8] = {cur[1][0], cur[1][1], cur[1][2], E[1][0], E[1][1], E[1][2], Hh[1][0], Hh[1][1]};
-            const unsigned kB = (2u << 8) | (2u << 10) | (2u << 12);
-            smooth<8>(K, tmp, nullptr, kB);
-            smooth<8>(tmp, K, nullptr, kB);
+        // right-hand side: hydro part (xdif 0..3, 7) and induction (xdif 4..6)
+        dim3 gg(mx / ZTX, (my + 7) / 8, 1);
+        int ch = zchunk(gg.x * gg.y, 32);
+        gg.z = (mz + ch - 1) / ch;
+        SrcFields<T, 5> sh;
+        sh.f[0] = xs[0]; sh.f[1] = xs[1]; sh.f[2] = xs[2]; sh.f[3] = xs[3]; sh.f[4] = xs[7];
+        OpHydro<T> oh;
+        oh.out[0] = K[0]; oh.out[1] = K[1]; oh.out[2] = K[2]; oh.out[3] = K[3]; oh.out[4] = K[7];
+        oh.j1 = curF[0]; oh.j2 = curF[1]; oh.j3 = curF[2]; oh.b1 = xs[4]; oh.b2 = xs[5]; oh.b3 = xs[6];
+        DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
+                     (k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>><<<gg, ZTX * 8, ZS2<T, 5, ZTX, 8>::smem(true), st>>>(g, sh, oh, ch)));
+        OpInduction<T> oi;
+        oi.out[0] = K[4]; oi.out[1] = K[5]; oi.out[2] = K[6];
+        DASHA_LAUNCH("k_rhs_induction", 6.0 * N * sizeof(T),
+                     (k_zst2<T, 3, ZTX, 8, 2, OpInduction<T>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(Ef), oi, ch)));
+    }
+    // 8 scratch fields that are free once the RHS is written
+    void tmp8(T** t) {
+        T* s[8] = {cur[0][0], cur[0][1], cur[0][2], cur[1][0], cur[1][1], cur[1][2], Hh[0][0], Hh[0][1]};
+        for (int m = 0; m < 8; ++m) t[m] = s[m];
+    }
+
+    // xdif of state xs into `out` (dasha_rhs): the RHS and, when smoothing, 2 avrg passes
+    void launch_rhs(T* const* xs, bool smooth_xdif, T** out) {
+        launch_rhs_raw(xs);
+        if (smooth_xdif) {
+            T* t[8];
+            tmp8(t);
+            pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpass_X", 16.0, t, [&](int lo) { return st4(out, lo); });
+        } else {
+            for (int m = 0; m < 8; ++m) out[m] = K[m];
         }
     }
 
     Status stepon(double time, double dt, int nstep) override {
         (void)time;
-        long nb = (N + 255) / 256;
-        F8<T> cz{};
-        if (KAHAN) cz = f8(C);
-        else for (int m = 0; m < 8; ++m) cz.f[m] = nullptr;
-        T* Sx[8];
-        for (int m = 0; m < 8; ++m) Sx[m] = S[m];
-        // stage 1..4: base = X, stage state in S, accumulator in A
-        launch_rhs(X, true);
-        DASHA_LAUNCH("k_rk_s1", 32.0 * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 1, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
-        launch_rhs(Sx, true);
-        DASHA_LAUNCH("k_rk_s2", 40.0 * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 2, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
-        launch_rhs(Sx, true);
-        DASHA_LAUNCH("k_rk_s3", 40.0 * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 3, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
-        launch_rhs(Sx, true);
-        DASHA_LAUNCH("k_rk_s4", (KAHAN ? 48.0 : 24.0) * N * sizeof(T), k_rk<T, KAHAN><<<nb, 256, 0, st>>>(N, 4, dt, f8(Sx), f8(X), f8(A), cz, f8(K)));
+        // stages 1..4: base = X, stage state in S, accumulator in A; the second xdif
+        // smoothing pass ends in the RK stage update
+        for (int stage = 1; stage <= 4; ++stage) {
+            launch_rhs_raw(stage == 1 ? X : S);
+            T* t[8];
+            tmp8(t);
+            pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
+            auto mkrk = [&](int lo) {
+                EpiRK<T, 4, KAHAN> er;
+                for (int m = 0; m < 4; ++m) {
+                    er.x[m] = S[lo + m]; er.base[m] = X[lo + m]; er.acc[m] = A[lo + m];
+                    er.comp[m] = KAHAN ? C[lo + m] : nullptr;
+                }
+                er.stage = stage;
+                er.dt = dt;
+                return er;
+            };
+            static const char* names[4] = {"k_zpass_X_rk1", "k_zpass_X_rk2", "k_zpass_X_rk3", "k_zpass_X_rk4"};
+            static const double rkb[4] = {8 + 24, 8 + 32, 8 + 32, 0};
+            double b = stage < 4 ? rkb[stage - 1] : (KAHAN ? 8 + 40 : 8 + 24);
+            pass8(names[stage - 1], b, t, mkrk);
+        }
         for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
         int every = P.filter_every > 0 ? P.filter_every : 1;
         if (nstep % every == 0) {   // avrgtt on the perturbation (t3dsdsc.f:1135-1165)
-            T* tmp[8] = {cur[1][0], cur[1][1], cur[1][2], E[1][0], E[1][1], E[1][2], Hh[1][0], Hh[1][1]};
-            const unsigned kB = (2u << 8) | (2u << 10) | (2u << 12);
-            smooth<8>(X, tmp, nullptr, kB);
-            smooth<8>(tmp, X, nullptr, kB);
+            T* t[8];
+            tmp8(t);
+            pass8("k_zpass_F", 16.0, X, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpass_F", 16.0, t, [&](int lo) { return st4(S, lo); });
+            for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
         }
         if (nstep % 10 == 0) {      // diagn blow-up guard (t3dsdsc.f:1174-1182, 1232)
             Status s = launch_diag(true);
@@ -426,7 +540,7 @@ public:
         dim3 g2(1, my, mz);
         DASHA_LAUNCH("k_diag_rows", 8.0 * N * sizeof(T), k_diag_rows<T><<<g2, 128, 0, st>>>(g, f8(X), wx, wy, wz, P.gamma, rows));
         k_diag_flux<T><<<my, 128, 0, st>>>(g, f8(X), wx, fl);
-        k_diag_jext<T><<<mz, 128, 0, st>>>(g, f3(cur[0]), my / 2, jext);
+        k_diag_jext<T><<<mz, 128, 0, st>>>(g, f3(curF), my / 2, jext);
         k_diag_final<<<1, 256, 0, st>>>(rows, (long)my * mz, fl, my, jext, mz, out, flag);
         DASHA_CK(cudaGetLastError());
         return Status::ok();
@@ -443,7 +557,8 @@ public:
 
     Status setdt(double* dt, int* blowup) override {
         dim3 g2(1, my, mz);
-        DASHA_LAUNCH("k_cfl", 8.0 * N * sizeof(T), k_cfl<T><<<g2, 128, 0, st>>>(g, f8(X), xc, yc, zc, dxs, dys, dzs, P.cfl, P.eta + P.mu, P.rcr, P.gamma, red));
+        DASHA_LAUNCH("k_cfl", 8.0 * N * sizeof(T), k_cfl<T><<<g2, 128, 0, st>>>(g, f8(X), xc, yc, zc, dxs, dys, dzs, P.cfl, P.eta + P.mu, P.rcr, P.gamma,
+                                                     (P.dt_whistler && P.hall) ? P.di * 3.141592653589793 : 0.0, red));
         k_reduce_min<<<1, 256, 0, st>>>(red, (long)my * mz, red + nred + 12);
         DASHA_CK(cudaGetLastError());
         DASHA_CK(cudaMemcpyAsync(hpin + 12, red + nred + 12, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -459,13 +574,15 @@ public:
     Status current(double* curh, long ld1, long ld2) override {
         launch_current(X);
         DASHA_CK(cudaGetLastError());
-        return transfer_out(curh, ld1, ld2, cur[0], 3, false);
+        return transfer_out(curh, ld1, ld2, curF, 3, false);
     }
 
     Status rhs(double t, double* xdif, long ld1, long ld2) override {
-        launch_rhs(X, t != 0.0);
+        T* out[8];
+        for (int m = 0; m < 8; ++m) out[m] = S[m];
+        launch_rhs(X, t != 0.0, out);
         DASHA_CK(cudaGetLastError());
-        return transfer_out(xdif, ld1, ld2, K, 8, false);
+        return transfer_out(xdif, ld1, ld2, out, 8, false);
     }
 
     Status adjoint_flux_grad(int, const double*, int, double*, double*) override {

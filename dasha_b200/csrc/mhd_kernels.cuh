@@ -27,7 +27,8 @@ struct Geo {
     // difc weights: difc = (f+ - f0)*wp - (f0 - f-)*wm  (t3dsdsc.f:5618-5619)
     const T *wpx, *wmx, *wpy, *wmy, *wpz, *wmz;
     const T *cbx;    // (1/32)(1 - tanh((x+3)/8)), smoothing coefficient of B (t3dsdsc.f:5636-5642)
-    const T *cr;     // 1/32 + 3/32 * (1 + tanh((r-3)/3))/2 per node (t3dsdsc.f:5659-5661)
+    const T *cr;     // 1/32 + 3/32 * (1 + tanh((r-3)/3))/2 per node (t3dsdsc.f:5659-5661), optional
+    const T *xc, *yc, *zc;   // node coordinates (radial coefficient evaluated on the fly)
     // equilibrium z-profiles (FP64)
     const double *rho0, *bx0, *by0, *bz0, *p0;
     const double *dzp0;               // Dz p0 (interior rows)
@@ -404,7 +405,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 template <class T>
 __global__ void k_cfl(Geo<T> g, F8<T> x, const double* xc, const double* yc, const double* zc,
                       const double* dxs, const double* dys, const double* dzs, double cfl, double visc,
-                      double rcr, double gamma, double* partial) {
+                      double rcr, double gamma, double whistler, double* partial) {
     int jj = blockIdx.y, k = blockIdx.z;
     double best = 100.;
     if (k <= g.mz - 3 && jj <= g.my - 2) {
@@ -420,9 +421,14 @@ __global__ void k_cfl(Geo<T> g, F8<T> x, const double* xc, const double* yc, con
             double cs2 = gamma * (p0 + (double)x.f[7][c]) / rho;
             double vf = sqrt(fabs(va2 + cs2));
             double dx = dxs[i], dy = dys[jj], dz = dzs[k];
-            double dtx = fabs(dx) / ((fabs(vx) + vf) / cfl + visc / dx / 2.);
-            double dty = fabs(dy) / ((fabs(vy) + vf) / cfl + visc / dy / 2.);
-            double dtz = fabs(dz) / ((fabs(vz) + vf) / cfl + visc / dz / 2.);
+            double vpx = fabs(vx) + vf, vpy = fabs(vy) + vf, vpz = fabs(vz) + vf;
+            if (whistler != 0.0) {   // di*pi*|B|/rho per unit length (dt_whistler option)
+                double w = whistler * sqrt(b1 * b1 + b2 * b2 + b3 * b3) / rho;
+                vpx += w / fabs(dx); vpy += w / fabs(dy); vpz += w / fabs(dz);
+            }
+            double dtx = fabs(dx) / (vpx / cfl + visc / dx / 2.);
+            double dty = fabs(dy) / (vpy / cfl + visc / dy / 2.);
+            double dtz = fabs(dz) / (vpz / cfl + visc / dz / 2.);
             double d = fmin(fmin(dtx, dty), dtz);
             // NaN must win so that a corrupted state is detected
             if (d != d) best = d; else if (best == best) best = fmin(best, d);

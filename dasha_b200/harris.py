@@ -124,6 +124,7 @@ class RunConfig:
     cfl: float = 0.4
     hall: int = 1
     j0_mode: int = 0
+    dt_whistler: int = 0
 
     @property
     def cells(self) -> int:
@@ -134,9 +135,10 @@ class RunConfig:
 CONFIGS = {
     "c0": RunConfig("c0-64x32x64-uniform", 64, 32, 64, False, 0.005, 0.5, 200),
     "c1": RunConfig("c1-256x128x256-sinh", 256, 128, 256, True, 0.003, 0.5, 1000, filter_every=10),
-    "c2": RunConfig("c2-512x256x512-sinh", 512, 256, 512, True, 0.003, 1.0, 1000),
+    # di = 1 on these fine grids: the explicit Hall term needs the whistler term in the CFL
+    "c2": RunConfig("c2-512x256x512-sinh", 512, 256, 512, True, 0.003, 1.0, 1000, dt_whistler=1),
     "c3": RunConfig("c3-128x64x128-uniform", 128, 64, 128, False, 0.005, 0.5, 500),
-    "c4": RunConfig("c4-1024x512x1024-sinh", 1024, 512, 1024, True, 0.002, 1.0, 200),
+    "c4": RunConfig("c4-1024x512x1024-sinh", 1024, 512, 1024, True, 0.002, 1.0, 200, dt_whistler=1),
 }
 
 

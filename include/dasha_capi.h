@@ -62,12 +62,16 @@ typedef struct {
  *  hall, viscos, diffu, total_e: mhd03.for:18-23 (total_e must be 1)
  *  j0_mode: 0 = LITERAL (J = curl(B-B0), the reference's equations), 1 = FULL (J0 added)
  *  filter_every: cadence of the post-step filter avrgtt (reference: every step = 1)
- *  precision: 0 = FP64 state and arithmetic; 1 = FP32 perturbation + Kahan-compensated RK4 */
+ *  precision: 0 = FP64 state and arithmetic; 1 = FP32 perturbation + Kahan-compensated RK4
+ *  dt_whistler: 0 = the reference's CFL (fast speed only, t3dsdsc.f:4719-4733); 1 = also add
+ *    the grid-scale whistler speed di*pi*|B|/(rho*h) to each direction's signal speed (the
+ *    explicit Hall term is unstable at fine grids without it; no counterpart in the reference) */
 typedef struct {
     double gamma, eta, di, mu, drho, dp, cfl, rcr;
     int hall, viscos, diffu, total_e, j0_mode;
     int filter_every;
     int precision;
+    int dt_whistler;
 } dasha_params_c;
 
 #define DASHA_NDIAG 9

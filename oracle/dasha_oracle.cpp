@@ -42,6 +42,7 @@ typedef struct {
     int hall, viscos, diffu, total_e, j0_mode;
     int filter_every;
     int precision;
+    int dt_whistler;
 } oracle_params;
 
 }
@@ -460,6 +461,11 @@ struct Oracle {
                     double vpy = std::fabs(vy) + std::sqrt(std::fabs(va2 + cs2));
                     double vpz = std::fabs(vz) + std::sqrt(std::fabs(va2 + cs2));
                     double dxi = xext[3][i] - xc[i], dyj = yext[3][j] - yc[j], dzk = zc[k + 1] - zc[k];
+                    if (P.dt_whistler && P.hall) {   /* build option: grid-scale whistler speed */
+                        double bm = std::sqrt(x[4][c] * x[4][c] + x[5][c] * x[5][c] + x[6][c] * x[6][c]);
+                        double w = P.di * 3.141592653589793 * bm / x[0][c];
+                        vpx += w / std::fabs(dxi); vpy += w / std::fabs(dyj); vpz += w / std::fabs(dzk);
+                    }
                     double dtx = std::fabs(dxi) / (vpx / cfl + (eta + fmu) / dxi / 2.);
                     double dty = std::fabs(dyj) / (vpy / cfl + (eta + fmu) / dyj / 2.);
                     double dtz = std::fabs(dzk) / (vpz / cfl + (eta + fmu) / dzk / 2.);

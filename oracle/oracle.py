@@ -15,7 +15,8 @@ class OracleParams(C.Structure):
     _fields_ = [("gamma", C.c_double), ("eta", C.c_double), ("di", C.c_double), ("mu", C.c_double),
                 ("drho", C.c_double), ("dp", C.c_double), ("cfl", C.c_double), ("rcr", C.c_double),
                 ("hall", C.c_int), ("viscos", C.c_int), ("diffu", C.c_int), ("total_e", C.c_int),
-                ("j0_mode", C.c_int), ("filter_every", C.c_int), ("precision", C.c_int)]
+                ("j0_mode", C.c_int), ("filter_every", C.c_int), ("precision", C.c_int),
+                ("dt_whistler", C.c_int)]
 
 
 _libs = {}
@@ -60,7 +61,8 @@ class Oracle:
     """CPU restatement of one run; state is the compact total x(mx,my,mz,8) = numpy (8,mz,my,mx)."""
 
     def __init__(self, x, y, z, gamma=5.0 / 3.0, eta=0.005, di=0.5, cfl=0.4, hall=1, j0_mode=0,
-                 filter_every=1, mu=0.0, drho=0.0, dp=0.0, viscos=1, diffu=1, threads=0, variant=""):
+                 filter_every=1, mu=0.0, drho=0.0, dp=0.0, viscos=1, diffu=1, threads=0, variant="",
+                 dt_whistler=0):
         self.lib = load(variant)
         if threads:
             self.lib.oracle_set_threads(threads)
@@ -68,7 +70,7 @@ class Oracle:
         self.mx, self.my, self.mz = self.x.size, self.y.size, self.z.size
         p = OracleParams(gamma=gamma, eta=eta, di=di, mu=mu, drho=drho, dp=dp, cfl=cfl, rcr=0.0, hall=hall,
                          viscos=viscos, diffu=diffu, total_e=1, j0_mode=j0_mode, filter_every=filter_every,
-                         precision=0)
+                         precision=0, dt_whistler=dt_whistler)
         self.h = self.lib.oracle_create(self.mx, self.my, self.mz, _dp(self.x), _dp(self.y), _dp(self.z),
                                         C.byref(p))
         if not self.h:
@@ -79,7 +81,7 @@ class Oracle:
         from dasha_b200 import harris
         x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
         return cls(x, y, z, gamma=cfg.gamma, eta=cfg.eta, di=cfg.di, cfl=cfg.cfl, hall=cfg.hall,
-                   j0_mode=cfg.j0_mode, filter_every=cfg.filter_every, **kw)
+                   j0_mode=cfg.j0_mode, filter_every=cfg.filter_every, dt_whistler=cfg.dt_whistler, **kw)
 
     def close(self):
         if self.h:

@@ -86,6 +86,15 @@ def test_setdt_parity(cfg):
     assert abs(d.setdt() - o.setdt()) <= 1e-14 * o.setdt()
 
 
+def test_setdt_parity_whistler_option():
+    import dataclasses
+    cfg = dataclasses.replace(SMALL_S, dt_whistler=1)
+    o, d = pair(cfg)
+    plain = capi.gem_context(SMALL_S, 0).setdt()
+    assert abs(d.setdt() - o.setdt()) <= 1e-14 * o.setdt()
+    assert d.setdt() < 0.5 * plain
+
+
 @pytest.mark.parametrize("cfg", [SMALL, SMALL_S], ids=lambda c: c.name)
 def test_steps_parity(cfg):
     o, d = pair(cfg)
