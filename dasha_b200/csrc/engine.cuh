@@ -119,6 +119,7 @@ public:
     T* tab = nullptr;            // 1-D tables in T
     double* dtab = nullptr;      // 1-D tables in FP64
     double* red = nullptr;       // reduction scratch
+    double* cfltab = nullptr;    // CFL rate tables: ich[mx+my+mz], vv[..], ih[..]
     int* flag = nullptr;         // blow-up flag
     double* hpin = nullptr;      // pinned host scratch
     Geo<T> g{};
@@ -135,6 +136,7 @@ public:
         if (tab) cudaFree(tab);
         if (dtab) cudaFree(dtab);
         if (red) cudaFree(red);
+        if (cfltab) cudaFree(cfltab);
         if (flag) cudaFree(flag);
         if (hpin) cudaFreeHost(hpin);
     }
@@ -225,6 +227,20 @@ public:
         zcoord = H.coord[2];
         for (int q2 = 0; q2 < 8; ++q2) coefz[q2] = H.coef[2][q2];
 
+        {   // CFL rate tables (setdt): 1/(cfl |h|), (eta+mu)/(2 h^2), 1/|h| per axis
+            long nt = (long)mx + my + mz;
+            std::vector<double> ct(3 * nt);
+            long o2 = 0;
+            for (int d = 0; d < 3; ++d)
+                for (int i2 = 0; i2 < nx[d]; ++i2, ++o2) {
+                    double h = H.spacing[d][i2];
+                    ct[o2] = 1.0 / (p.cfl * std::fabs(h));
+                    ct[nt + o2] = (p.eta + p.mu) / h / 2.0 / h;
+                    ct[2 * nt + o2] = 1.0 / std::fabs(h);
+                }
+            DASHA_CK(cudaMalloc(&cfltab, sizeof(double) * 3 * nt));
+            DASHA_CK(cudaMemcpy(cfltab, ct.data(), sizeof(double) * 3 * nt, cudaMemcpyHostToDevice));
+        }
         nred = 2L * my * mz + my + 6L * mz + 64;
         DASHA_CK(cudaMalloc(&red, sizeof(double) * (nred + 16)));
         DASHA_CK(cudaMalloc(&flag, sizeof(int)));
@@ -393,7 +409,13 @@ public:
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
             return e;
-        return cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpInduction<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if ((e = cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, 1>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ZS2<T, 3, ZTX, 8>::smem(false))))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_zst2<T, 1, ZTX, 8, 2, OpHall<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ZS2<T, 1, ZTX, 8>::smem(false))))
+            return e;
+        return cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, -1>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ZS2<T, 3, ZTX, 8>::smem(false));
     }
     static constexpr int HMINB = sizeof(T) == 4 ? 2 : 1;   // CTAs per SM asked of the register allocator
@@ -434,7 +456,13 @@ public:
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
     void launch_current(T* const* xs) {
         T* bb[3] = {xs[4], xs[5], xs[6]};
-        DASHA_LAUNCH("k_curl", 6.0 * N * sizeof(T), k_curl<T><<<grd, blk, 0, st>>>(g, f3(bb), f3(cur[0])));
+        dim3 gg(mx / ZTX, (my + 7) / 8, 1);
+        int ch = zchunk(gg.x * gg.y, 32);
+        gg.z = (mz + ch - 1) / ch;
+        OpCurl<T, 1> oc;
+        for (int q = 0; q < 3; ++q) oc.out[q] = cur[0][q];
+        DASHA_LAUNCH("k_curl", 6.0 * N * sizeof(T),
+                     (k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, 1>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(bb), oc, ch)));
         curF = passes3<0u>("k_zpass_J", cur[0], cur[1], 4);
         if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(curF)));
     }
@@ -448,6 +476,7 @@ public:
         DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
         Ef = passes3<0u>("k_zpass_E", E[0], E[1], 4);
         if (P.hall) {
+            // plain kernel: faster here than the ring framework (one stencil field, seven pointwise)
             DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(Hh[0])));
             T** h = passes3<KIND_H>("k_zpass_H", Hh[0], Hh[1], 4);
             EpiAcc<T, 3> ea;
@@ -465,10 +494,10 @@ public:
         oh.j1 = curF[0]; oh.j2 = curF[1]; oh.j3 = curF[2]; oh.b1 = xs[4]; oh.b2 = xs[5]; oh.b3 = xs[6];
         DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
                      (k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>><<<gg, ZTX * 8, ZS2<T, 5, ZTX, 8>::smem(true), st>>>(g, sh, oh, ch)));
-        OpInduction<T> oi;
+        OpCurl<T, -1> oi;
         oi.out[0] = K[4]; oi.out[1] = K[5]; oi.out[2] = K[6];
         DASHA_LAUNCH("k_rhs_induction", 6.0 * N * sizeof(T),
-                     (k_zst2<T, 3, ZTX, 8, 2, OpInduction<T>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(Ef), oi, ch)));
+                     (k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, -1>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(Ef), oi, ch)));
     }
     // 8 scratch fields that are free once the RHS is written
     void tmp8(T** t) {
@@ -557,9 +586,11 @@ public:
 
     Status setdt(double* dt, int* blowup) override {
         dim3 g2(1, my, mz);
-        DASHA_LAUNCH("k_cfl", 8.0 * N * sizeof(T), k_cfl<T><<<g2, 128, 0, st>>>(g, f8(X), xc, yc, zc, dxs, dys, dzs, P.cfl, P.eta + P.mu, P.rcr, P.gamma,
-                                                     (P.dt_whistler && P.hall) ? P.di * 3.141592653589793 : 0.0, red));
-        k_reduce_min<<<1, 256, 0, st>>>(red, (long)my * mz, red + nred + 12);
+        const long nt = (long)mx + my + mz;
+        DASHA_LAUNCH("k_cfl", 8.0 * N * sizeof(T),
+                     k_cfl_rate<T><<<g2, 128, 0, st>>>(g, f8(X), cfltab, cfltab + nt, cfltab + 2 * nt, P.gamma,
+                                                       (P.dt_whistler && P.hall) ? P.di * 3.141592653589793 : 0.0, red));
+        k_reduce_rate<<<1, 256, 0, st>>>(red, (long)my * mz, red + nred + 12);
         DASHA_CK(cudaGetLastError());
         DASHA_CK(cudaMemcpyAsync(hpin + 12, red + nred + 12, sizeof(double), cudaMemcpyDeviceToHost, st));
         int fl = 0;

@@ -457,6 +457,80 @@ __global__ void k_cfl(Geo<T> g, F8<T> x, const double* xc, const double* yc, con
     }
 }
 
+// CFL in rate form: the reference's per-direction step h / (vp/cfl + visc/(2h)) is the
+// inverse of the rate vp * (1/(cfl h)) + visc/(2 h^2), so dt = min(100, 1 / max rate) over
+// the region k 0..mz-3, j 0..my-2, i 0..mx-3 (t3dsdsc.f:4709-4736).  Tables per axis:
+// ich = 1/(cfl |h|), vv = visc/(2 h^2), ih = 1/|h| (whistler term).  One block per (j,k)
+// row; NaN wins so that a corrupted state is reported.
+__device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a != a ? a : b) : fmax(a, b); }
+
+template <class T>
+__global__ void k_cfl_rate(Geo<T> g, F8<T> x, const double* ich, const double* vv, const double* ih, double gamma,
+                           double whistler, double* partial) {
+    int jj = blockIdx.y, k = blockIdx.z;
+    double best = 0.0;
+    const int nx = g.mx;
+    const double* ichx = ich;
+    const double* ichy = ich + nx;
+    const double* ichz = ich + nx + g.my;
+    const double* vvx = vv;
+    const double* vvy = vv + nx;
+    const double* vvz = vv + nx + g.my;
+    const double* ihx = ih;
+    const double* ihy = ih + nx;
+    const double* ihz = ih + nx + g.my;
+    if (k <= g.mz - 3 && jj <= g.my - 2) {
+        const double r0 = g.rho0[k], bx0 = g.bx0[k], by0 = g.by0[k], bz0 = g.bz0[k], p0 = g.p0[k];
+        const double cy = ichy[jj], vy_ = vvy[jj], cz = ichz[k], vz_ = vvz[k], hy = ihy[jj], hz = ihz[k];
+        for (int i = threadIdx.x; i <= g.mx - 3; i += blockDim.x) {
+            long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
+            double rinv = 1.0 / (r0 + (double)x.f[0][c]);
+            double vx = (double)x.f[1][c] * rinv, vy = (double)x.f[2][c] * rinv, vz = (double)x.f[3][c] * rinv;
+            double b1 = bx0 + (double)x.f[4][c], b2 = by0 + (double)x.f[5][c], b3 = bz0 + (double)x.f[6][c];
+            double bb = b1 * b1 + b2 * b2 + b3 * b3;
+            double vf = sqrt(fabs((bb + gamma * (p0 + (double)x.f[7][c])) * rinv));
+            double w = whistler != 0.0 ? whistler * sqrt(bb) * rinv : 0.0;
+            double rx = (fabs(vx) + vf + w * ihx[i]) * ichx[i] + vvx[i];
+            double ry = (fabs(vy) + vf + w * hy) * cy + vy_;
+            double rz = (fabs(vz) + vf + w * hz) * cz + vz_;
+            best = nanmax(best, nanmax(rx, nanmax(ry, rz)));
+        }
+    }
+    __shared__ double sh[32];
+    double v = best;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        if (lane == 0) partial[(long)blockIdx.z * gridDim.y + blockIdx.y] = v;
+    }
+}
+
+// dt = min(100, 1 / max rate) from the row partials, one block, fixed order
+static __global__ void k_reduce_rate(const double* partial, long n, double* out) {
+    double v = 0.0;
+    for (long q = threadIdx.x; q < n; q += blockDim.x) v = nanmax(v, partial[q]);
+    __shared__ double sh[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        v = lane < nw ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        if (lane == 0) *out = (v != v) ? v : fmin(100.0, 1.0 / v);
+    }
+}
+
 // final reduction of partials by one block, fixed order
 static __global__ void k_reduce_min(const double* partial, long n, double* out) {
     double v = 100.;

@@ -814,9 +814,10 @@ __global__ void __launch_bounds__(TX* TYH, MINB) k_zst2(Geo<T> g, SrcFields<T, N
     cp_async_wait<0>();
 }
 
-// dB/dt = -curl E (t3dsdsc.f:1435-1452); ring fields E1 E2 E3
-template <class T>
-struct OpInduction {
+// SIGN * curl of the 3 ring fields, wall rows applied: SIGN = +1 is J1 = curl(B - B0)
+// (current t3dsdsc.f:2476-2491 with bndryc), SIGN = -1 is dB/dt = -curl E (t3dsdsc.f:1435-1452)
+template <class T, int SIGN>
+struct OpCurl {
     static constexpr bool RINV = false;
     T* out[3];
     struct Col { T ax, bx, cx, dx, ay, by, cy, dy; };
@@ -835,9 +836,60 @@ struct OpInduction {
         auto DY = [&](int f) { return d1fc(v.Y(f, 0), v.Y(f, 1), v.Y(f, 2), v.Y(f, 3), v.Y(f, 4), k.ay, k.by, k.cy, k.dy); };
         auto DZ = [&](int f) { return d1fc(v.Zz(f, 0), v.Zz(f, 1), v.Zz(f, 2), v.Zz(f, 3), v.Zz(f, 4), p.az, p.bz, p.cz, p.dz); };
         T o[3];
-        o[0] = -DY(2) + DZ(1);
-        o[1] = -DZ(0) + DX(2);
-        o[2] = -DX(1) + DY(0);
+        if (SIGN > 0) {
+            o[0] = DY(2) - DZ(1);
+            o[1] = DZ(0) - DX(2);
+            o[2] = DX(1) - DY(0);
+        } else {
+            o[0] = -DY(2) + DZ(1);
+            o[1] = -DZ(0) + DX(2);
+            o[2] = -DX(1) + DY(0);
+        }
+        const long base = (long)i + (long)j * g.sy;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) out[m][base + (long)c * g.sz] = o[m];
+        if (c == 2 || c == g.mz - 3) {
+            const int kh = c == 2 ? 1 : g.mz - 2, kz = c == 2 ? 0 : g.mz - 1;
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                out[m][base + (long)kh * g.sz] = T(0.5) * o[m];
+                out[m][base + (long)kz * g.sz] = T(0);
+            }
+        }
+    }
+};
+
+// Hall term xdh = di (J x B - grad p) / rho with the wall rows (t3dsdsc.f:1404-1423, bndryh);
+// ring field dp, the rest pointwise
+template <class T>
+struct OpHall {
+    static constexpr bool RINV = false;
+    T* out[3];
+    const T *r, *b1, *b2, *b3, *j1, *j2, *j3;
+    struct Col { T ax, bx, cx, dx, ay, by, cy, dy; };
+    struct Pre { T az, bz, cz, dz, r, b1, b2, b3, j1, j2, j3, dzp0; };
+    __device__ __forceinline__ void column(const Geo<T>& g, int i, int j, Col& c) const {
+        c.ax = g.a1x[i]; c.bx = g.b1x[i]; c.cx = g.c1x[i]; c.dx = g.d1x[i];
+        c.ay = g.a1y[j]; c.by = g.b1y[j]; c.cy = g.c1y[j]; c.dy = g.d1y[j];
+    }
+    __device__ __forceinline__ void pre(const Geo<T>& g, int i, int j, int c, Pre& p) const {
+        const long ci = (long)i + (long)j * g.sy + (long)c * g.sz;
+        p.az = g.a1z[c]; p.bz = g.b1z[c]; p.cz = g.c1z[c]; p.dz = g.d1z[c];
+        p.r = T(g.rho0[c]) + r[ci];
+        p.b1 = T(g.bx0[c]) + b1[ci]; p.b2 = T(g.by0[c]) + b2[ci]; p.b3 = T(g.bz0[c]) + b3[ci];
+        p.j1 = j1[ci]; p.j2 = j2[ci]; p.j3 = j3[ci];
+        p.dzp0 = T(g.dzp0[c]);
+    }
+    template <class V>
+    __device__ __forceinline__ void compute(const Geo<T>& g, const V& v, int i, int j, int c, const Col& k,
+                                            const Pre& p) const {
+        const T px = d1fc(v.X(0, 0), v.X(0, 1), v.X(0, 2), v.X(0, 3), v.X(0, 4), k.ax, k.bx, k.cx, k.dx);
+        const T py = d1fc(v.Y(0, 0), v.Y(0, 1), v.Y(0, 2), v.Y(0, 3), v.Y(0, 4), k.ay, k.by, k.cy, k.dy);
+        const T pz = d1fc(v.Zz(0, 0), v.Zz(0, 1), v.Zz(0, 2), v.Zz(0, 3), v.Zz(0, 4), p.az, p.bz, p.cz, p.dz) + p.dzp0;
+        T o[3];
+        o[0] = g.di * (p.j2 * p.b3 - p.j3 * p.b2 - px) / p.r;
+        o[1] = g.di * (p.j3 * p.b1 - p.j1 * p.b3 - py) / p.r;
+        o[2] = g.di * (p.j1 * p.b2 - p.j2 * p.b1 - pz) / p.r;
         const long base = (long)i + (long)j * g.sy;
 #pragma unroll
         for (int m = 0; m < 3; ++m) out[m][base + (long)c * g.sz] = o[m];
