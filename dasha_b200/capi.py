@@ -56,6 +56,7 @@ SIGNATURES = {
     "dasha_rhs": ([_P, C.c_double, _D, C.c_long, C.c_long], C.c_int),
     "dasha_diagnostics": ([_P, _D], C.c_int),
     "dasha_adjoint_flux_grad": ([_P, C.c_int, _D, C.c_int, _D, _D], C.c_int),
+    "dasha_adjoint_rhs": ([_P, _D, _D, C.c_long, C.c_long], C.c_int),
     "dasha_timer": ([_P, C.c_int, _D], C.c_int),
     "dasha_profile": ([_P, C.c_int], C.c_int),
     "dasha_profile_read": ([_P, C.POINTER(C.c_int), C.c_char_p, _D, C.POINTER(C.c_long), _D], C.c_int),
@@ -191,6 +192,13 @@ class Dasha:
         self._check(self.lib.dasha_adjoint_flux_grad(self.h, int(dt_seq.size), _dp(dt_seq), int(snaps),
                                                      _dp(deta), _dp(dpsi)))
         return float(deta[0]), dpsi
+
+    def adjoint_rhs(self, W: np.ndarray) -> np.ndarray:
+        """G'(x)^T W for the current state x, W and the result compact (8, mz, my, mx)."""
+        Hw = harris.to_halo(np.ascontiguousarray(W, np.float64))
+        Ho = harris.to_halo(np.zeros((8, self.mz, self.my, self.mx)))
+        self._check(self.lib.dasha_adjoint_rhs(self.h, _dp(Hw), _dp(Ho), Hw.shape[3], Hw.shape[2]))
+        return harris.from_halo(Ho, self.mx, self.my, self.mz)
 
     # -- measurement --
     def timer_start(self):

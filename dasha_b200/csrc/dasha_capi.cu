@@ -277,6 +277,14 @@ int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int 
     return from_status(c, c->eng->adjoint_flux_grad(nsteps, dt_seq, snaps, dPhi_deta, dPhi_dpsi));
 }
 
+int dasha_adjoint_rhs(dasha_ctx* c, const double* w_f, double* out_f, long ld1, long ld2) {
+    CAPI_GUARD(c);
+    if (int rc = check_ld(c, w_f, ld1, ld2)) return rc;
+    if (int rc = check_ld(c, out_f, ld1, ld2)) return rc;
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return from_status(c, c->eng->adjoint_rhs(w_f, out_f, ld1, ld2));
+}
+
 int dasha_timer(dasha_ctx* c, int op, double* ms) {
     CAPI_GUARD(c);
     EngineBase* e = c->eng;

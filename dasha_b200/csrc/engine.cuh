@@ -4,7 +4,9 @@
 #include "dasha_capi.h"
 #include "mhd_kernels.cuh"
 #include "zm_kernels.cuh"
+#include "adjoint.cuh"
 #include <cuda_runtime.h>
+#include <type_traits>
 #include <string>
 #include <vector>
 #include <cmath>
@@ -76,6 +78,7 @@ struct EngineBase {
     virtual Status rhs(double t, double* xdif, long ld1, long ld2) = 0;
     virtual Status diagnostics(double* out) = 0;
     virtual Status adjoint_flux_grad(int nsteps, const double* dt_seq, int snaps, double* deta, double* dpsi) = 0;
+    virtual Status adjoint_rhs(const double* w, double* out, long ld1, long ld2) = 0;
 };
 
 EngineBase* make_engine_f64(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const HostTables& H,
@@ -616,8 +619,267 @@ public:
         return transfer_out(xdif, ld1, ld2, out, 8, false);
     }
 
-    Status adjoint_flux_grad(int, const double*, int, double*, double*) override {
-        return Status::err(DASHA_E_UNSUPPORTED, "adjoint not available in this build");
+    // ======================= discrete adjoint (FP64 contexts) =======================
+    // scratch of one adjoint call (cudaMalloc'd per call, freed at the end)
+    struct AdjBufs {
+        std::vector<void*> mem;
+        double* take(size_t n) {
+            void* p = nullptr;
+            if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+            mem.push_back(p);
+            return (double*)p;
+        }
+        ~AdjBufs() { for (void* p : mem) cudaFree(p); }
+    };
+    struct V8 { T* f[8]; };
+
+    void k8(T** d, T* const* s2) { for (int m = 0; m < 8; ++m) d[m] = s2[m]; }
+    void copy8(T* const* dst, T* const* src) {
+        for (int m = 0; m < 8; ++m) cudaMemcpyAsync(dst[m], src[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+    }
+    void zero8(T* const* f, int nf = 8) { for (int m = 0; m < nf; ++m) cudaMemsetAsync(f[m], 0, sizeof(T) * N, st); }
+    void axpby8(T* const* y, double b, T* const* x, double a) {
+        if constexpr (std::is_same<T, double>::value) {
+            long nb = (N + 255) / 256;
+            F8<double> Y, Xv;
+            for (int m = 0; m < 8; ++m) { Y.f[m] = y[m]; Xv.f[m] = x[m]; }
+            k_axpby8<<<nb, 256, 0, st>>>(N, Y, b, Xv, a);
+        }
+    }
+
+    // the forward step in explicit buffers: stage states S1..S3, result Xo (filtered if
+    // filt); same kernels and arithmetic as stepon
+    void fwd_step(T* const* Xb, double dt, bool filt, T* const* S1, T* const* S2, T* const* S3, T* const* Xo, T* const* Acc) {
+        T* const* outs[4] = {S1, S2, S3, Xo};
+        T* const* ins[4] = {Xb, S1, S2, S3};
+        for (int stage = 1; stage <= 4; ++stage) {
+            launch_rhs_raw(ins[stage - 1]);
+            T* t[8];
+            tmp8(t);
+            pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
+            T* const* xo = outs[stage - 1];
+            auto mkrk = [&](int lo) {
+                EpiRK<T, 4, KAHAN> er;
+                for (int m = 0; m < 4; ++m) { er.x[m] = xo[lo + m]; er.base[m] = Xb[lo + m]; er.acc[m] = Acc[lo + m]; er.comp[m] = nullptr; }
+                er.stage = stage;
+                er.dt = dt;
+                return er;
+            };
+            pass8("k_zpass_X", 24.0, t, mkrk);
+        }
+        if (filt) {
+            T* t[8];
+            tmp8(t);
+            pass8("k_zpass_F", 16.0, Xo, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpass_F", 16.0, t, [&](int lo) { return st4(Xo, lo); });
+        }
+    }
+
+    // transposed smoothing passes: n passes of nf (3 or 8) fields, kinds per field, in place
+    // on `a` using `b` as the other buffer; returns the buffer holding the result
+    T** adj_passes(T** a, T** b, int nf, int n, unsigned kinds3, bool fold_after) {
+        if constexpr (std::is_same<T, double>::value) {
+            dim3 gf((mx + blk.x - 1) / blk.x, my, 1);
+            for (int p = 0; p < n; ++p) {
+                F8<double> fa{};
+                for (int m = 0; m < nf; ++m) fa.f[m] = a[m];
+                k_adj_fold_rows<<<gf, blk, 0, st>>>(g, fa, nf);
+                if (nf == 3) {
+                    FS<double, 3> in, out;
+                    for (int m = 0; m < 3; ++m) { in.f[m] = a[m]; out.f[m] = b[m]; }
+                    k_adj_pass<3><<<grd, blk, 0, st>>>(g, in, out, kinds3);
+                } else {
+                    FS<double, 4> in, out;
+                    for (int m = 0; m < 4; ++m) { in.f[m] = a[m]; out.f[m] = b[m]; }
+                    k_adj_pass<4><<<grd, blk, 0, st>>>(g, in, out, 0u);
+                    for (int m = 0; m < 4; ++m) { in.f[m] = a[4 + m]; out.f[m] = b[4 + m]; }
+                    k_adj_pass<4><<<grd, blk, 0, st>>>(g, in, out, KIND_B4);
+                }
+                std::swap(a, b);
+            }
+            if (fold_after) {
+                F8<double> fa{};
+                for (int m = 0; m < nf; ++m) fa.f[m] = a[m];
+                k_adj_fold_rows<<<dim3((mx + blk.x - 1) / blk.x, my, 1), blk, 0, st>>>(g, fa, nf);
+            }
+        }
+        return a;
+    }
+
+    // sigma = G'(S)^T kappa, G = avrg(right(.)); eta partials summed into *eta_acc (device)
+    struct AdjScratch {
+        T *a8[8], *b8[8], *sb[8], *wq[8];
+        T *e0[3], *e1[3], *et[3], *h0[3], *h1[3], *jb[3], *jt[3], *ub[3];
+        double* etap;
+        long netap;
+        double* eta_acc;
+    };
+    void adj_rhs(T* const* Sx, T* const* kappa, T* const* sigma, AdjScratch& w) {
+        if constexpr (std::is_same<T, double>::value) {
+            launch_current(Sx);                       // curF = J of the stage state
+            for (int m = 0; m < 8; ++m) cudaMemcpyAsync(w.a8[m], kappa[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+            T** rb = adj_passes(w.a8, w.b8, 8, 2, 0u, true);       // adjoint of the raw RHS (rows folded)
+            // induction: o_B = -curl(E_total)  ->  Et_bar = -curl^T(o_B)
+            F3<double> ob3, et3;
+            for (int m = 0; m < 3; ++m) { ob3.f[m] = rb[4 + m]; et3.f[m] = w.et[m]; }
+            k_adj_curlT<<<grd, blk, 0, st>>>(g, ob3, et3, -1.0, 0);
+            // E chain: 4 transposed avrgE passes -> adjoint of E0 (all nodes)
+            for (int m = 0; m < 3; ++m) cudaMemcpyAsync(w.e0[m], w.et[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+            T** eb = adj_passes(w.e0, w.e1, 3, 4, 0u, false);
+            T** hb = nullptr;
+            if (P.hall) {   // Hall chain: 5 transposed avrgh passes, then the rows of k_hall folded
+                for (int m = 0; m < 3; ++m) cudaMemcpyAsync(w.h0[m], w.et[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+                hb = adj_passes(w.h0, w.h1, 3, 5, KIND_H, true);
+            }
+            zero8(w.sb);
+            AdjPtw ap;
+            for (int m = 0; m < 8; ++m) { ap.s.f[m] = Sx[m]; ap.sb.f[m] = w.sb[m]; ap.wq.f[m] = w.wq[m]; }
+            for (int m = 0; m < 3; ++m) {
+                ap.j.f[m] = curF[m]; ap.eb.f[m] = eb[m]; ap.hb.f[m] = hb ? hb[m] : w.et[m];
+                ap.jb.f[m] = w.jb[m]; ap.ub.f[m] = w.ub[m];
+            }
+            ap.ob[0] = rb[0]; ap.ob[1] = rb[1]; ap.ob[2] = rb[2]; ap.ob[3] = rb[3]; ap.ob[4] = rb[7];
+            ap.etapart = w.etap;
+            ap.hall = P.hall;
+            k_adj_pointwise<<<grd, blk, 0, st>>>(g, ap);
+            k_reduce_add<<<1, 256, 0, st>>>(w.etap, w.netap, w.eta_acc);
+            AdjGat ag;
+            for (int m = 0; m < 8; ++m) { ag.s.f[m] = Sx[m]; ag.sb.f[m] = w.sb[m]; ag.wq.f[m] = w.wq[m]; }
+            for (int m = 0; m < 3; ++m) ag.ub.f[m] = w.ub[m];
+            ag.ob[0] = rb[0]; ag.ob[1] = rb[1]; ag.ob[2] = rb[2]; ag.ob[3] = rb[3]; ag.ob[4] = rb[7];
+            k_adj_gather<<<grd, blk, 0, st>>>(g, ag);
+            // current chain: 4 transposed avrgc passes, the curl's rows folded, curl^T into B
+            T** jt = adj_passes(w.jb, w.jt, 3, 4, 0u, true);
+            F3<double> jw, bo;
+            for (int m = 0; m < 3; ++m) { jw.f[m] = jt[m]; bo.f[m] = w.sb[4 + m]; }
+            k_adj_curlT<<<grd, blk, 0, st>>>(g, jw, bo, 1.0, 1);
+            for (int m = 0; m < 8; ++m) cudaMemcpyAsync(sigma[m], w.sb[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+        }
+    }
+
+    bool adj_scratch(AdjBufs& B, AdjScratch& w) {
+        auto t8 = [&](T** a) { for (int m = 0; m < 8; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
+        auto t3 = [&](T** a) { for (int m = 0; m < 3; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
+        if (!t8(w.a8) || !t8(w.b8) || !t8(w.sb) || !t8(w.wq)) return false;
+        if (!t3(w.e0) || !t3(w.e1) || !t3(w.et) || !t3(w.h0) || !t3(w.h1) || !t3(w.jb) || !t3(w.jt) || !t3(w.ub)) return false;
+        w.netap = (long)grd.x * grd.y * grd.z;
+        if (!(w.etap = B.take(w.netap)) || !(w.eta_acc = B.take(4))) return false;
+        cudaMemsetAsync(w.eta_acc, 0, 4 * sizeof(double), st);
+        return true;
+    }
+
+    Status adjoint_rhs(const double* wh, double* outh, long ld1, long ld2) override {
+        if constexpr (!std::is_same<T, double>::value) {
+            (void)wh; (void)outh; (void)ld1; (void)ld2;
+            return Status::err(DASHA_E_UNSUPPORTED, "the adjoint runs on FP64 contexts only");
+        } else {
+            if (g.viscos || g.diffu) return Status::err(DASHA_E_UNSUPPORTED, "adjoint with viscous/diffusive terms");
+            AdjBufs B;
+            AdjScratch w;
+            T *kap[8], *sig[8];
+            if (!adj_scratch(B, w)) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
+            for (int m = 0; m < 8; ++m) {
+                if (!(kap[m] = (T*)B.take(N)) || !(sig[m] = (T*)B.take(N))) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
+            }
+            Status s2 = transfer_in(wh, ld1, ld2, kap, 8, false);
+            if (s2.code) return s2;
+            adj_rhs(X, kap, sig, w);
+            DASHA_CK(cudaGetLastError());
+            return transfer_out(outh, ld1, ld2, sig, 8, false);
+        }
+    }
+
+    Status adjoint_flux_grad(int nsteps, const double* dts, int snaps, double* deta, double* dpsi) override {
+        if constexpr (!std::is_same<T, double>::value) {
+            (void)nsteps; (void)dts; (void)snaps; (void)deta; (void)dpsi;
+            return Status::err(DASHA_E_UNSUPPORTED, "the adjoint runs on FP64 contexts only");
+        } else {
+            if (g.viscos || g.diffu) return Status::err(DASHA_E_UNSUPPORTED, "adjoint with viscous/diffusive terms");
+            const int every = P.filter_every > 0 ? P.filter_every : 1;
+            const int seg = std::max(1, (nsteps + snaps - 1) / std::max(1, snaps));
+            const int nseg = (nsteps + seg - 1) / seg;
+            AdjBufs B;
+            AdjScratch w;
+            if (!adj_scratch(B, w)) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
+            auto take8 = [&](T** a) { for (int m = 0; m < 8; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
+            std::vector<std::vector<T*>> snap(std::max(nseg, 1), std::vector<T*>(8));
+            std::vector<std::vector<T*>> sst(seg + 1, std::vector<T*>(8));
+            T *X0[8], *S1[8], *S2[8], *S3[8], *Xo[8], *Ac[8], *lam[8], *mu[8], *kap[8], *sig[8], *tot[8], *ta[8], *tb[8];
+            bool ok = take8(X0) && take8(S1) && take8(S2) && take8(S3) && take8(Xo) && take8(Ac) && take8(lam) && take8(mu) &&
+                      take8(kap) && take8(sig) && take8(tot) && take8(ta) && take8(tb);
+            for (auto& v : snap) ok = ok && take8(v.data());
+            for (auto& v : sst) ok = ok && take8(v.data());
+            if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
+            copy8(X0, X);
+            // forward sweep with segment snapshots
+            T *cur8[8], *nxt8[8];
+            copy8(ta, X0);
+            k8(cur8, ta);
+            k8(nxt8, tb);
+            for (int n = 0; n < nsteps; ++n) {
+                if (n % seg == 0) copy8(snap[n / seg].data(), cur8);
+                fwd_step(cur8, dts[n], n % every == 0, S1, S2, S3, nxt8, Ac);
+                std::swap_ranges(cur8, cur8 + 8, nxt8);
+            }
+            // seed: dPhi/dX_N
+            zero8(lam);
+            {
+                dim3 g2((mx + blk.x - 1) / blk.x, my, 1);
+                k_adj_flux_seed<<<g2, blk, 0, st>>>(g, cur8[6], wx, lam[6]);
+            }
+            // reverse sweep, one segment at a time
+            for (int sgi = nseg - 1; sgi >= 0; --sgi) {
+                const int n0 = sgi * seg, n1 = std::min(nsteps, n0 + seg);
+                copy8(sst[0].data(), snap[sgi].data());
+                for (int n = n0; n < n1 - 1; ++n)
+                    fwd_step(sst[n - n0].data(), dts[n], n % every == 0, S1, S2, S3, sst[n - n0 + 1].data(), Ac);
+                for (int n = n1 - 1; n >= n0; --n) {
+                    T* const* Xn = sst[n - n0].data();
+                    const double dt = dts[n];
+                    fwd_step(Xn, dt, false, S1, S2, S3, Xo, Ac);       // stage states of step n
+                    // mu = F^T lambda
+                    if (n % every == 0) {
+                        copy8(ta, lam);
+                        T** r = adj_passes(ta, tb, 8, 2, 0u, false);
+                        copy8(mu, r);
+                    } else {
+                        copy8(mu, lam);
+                    }
+                    copy8(tot, mu);                                    // lambda_X = mu + sum sigma
+                    copy8(kap, mu);
+                    axpby8(kap, dt / 6.0, mu, 0.0);                    // kappa4 = dt/6 mu
+                    adj_rhs(S3, kap, sig, w);                          // sigma3
+                    axpby8(tot, 1.0, sig, 1.0);
+                    axpby8(kap, 0.0, mu, dt / 3.0);                    // kappa3 = dt/3 mu + dt sigma3
+                    axpby8(kap, 1.0, sig, dt);
+                    adj_rhs(S2, kap, sig, w);                          // sigma2
+                    axpby8(tot, 1.0, sig, 1.0);
+                    axpby8(kap, 0.0, mu, dt / 3.0);                    // kappa2 = dt/3 mu + dt/2 sigma2
+                    axpby8(kap, 1.0, sig, dt / 2.0);
+                    adj_rhs(S1, kap, sig, w);                          // sigma1
+                    axpby8(tot, 1.0, sig, 1.0);
+                    axpby8(kap, 0.0, mu, dt / 6.0);                    // kappa1 = dt/6 mu + dt/2 sigma1
+                    axpby8(kap, 1.0, sig, dt / 2.0);
+                    adj_rhs(Xn, kap, sig, w);                          // sigma0
+                    axpby8(tot, 1.0, sig, 1.0);
+                    copy8(lam, tot);
+                }
+            }
+            // gradients: eta, and psi through dBx = -Dz psi, dBz = Dx psi
+            double* dpsi_d = B.take((size_t)mx * mz);
+            if (!dpsi_d) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
+            k_adj_psi<<<dim3((mx + blk.x - 1) / blk.x, mz, 1), blk, 0, st>>>(g, lam[4], lam[6], dpsi_d);
+            DASHA_CK(cudaGetLastError());
+            std::vector<double> hp((size_t)mx * mz);
+            DASHA_CK(cudaMemcpyAsync(hp.data(), dpsi_d, sizeof(double) * mx * mz, cudaMemcpyDeviceToHost, st));
+            double he = 0.0;
+            DASHA_CK(cudaMemcpyAsync(&he, w.eta_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+            copy8(X, X0);                                              // the context state is unchanged
+            DASHA_CK(cudaStreamSynchronize(st));
+            *deta = he;
+            std::memcpy(dpsi, hp.data(), sizeof(double) * mx * mz);
+            return Status::ok();
+        }
     }
 };
 

@@ -188,10 +188,14 @@ __global__ void k_hall(Geo<T> g, F8<T> x, F3<T> cur, F3<T> h) {
     T b1 = T(g.bx0[ks]) + x.f[4][q], b2 = T(g.by0[ks]) + x.f[5][q], b3 = T(g.bz0[ks]) + x.f[6][q];
     T j1 = cur.f[0][q], j2 = cur.f[1][q], j3 = cur.f[2][q];
     const T* p = x.f[7];
-    T px = n.Dx(g, p), py = n.Dy(g, p), pz = n.Dz(g, p) + T(g.dzp0[ks]);
+    // grad p = grad(p - p0) + dp0/dz ez.  Of -di dp0/dz / rho, the plane-uniform part
+    // -di dp0/dz / rho0 has an exactly zero discrete curl (the Hall passes keep it uniform in
+    // x and y) and is left out; the rest is di dp0/dz (rho - rho0) / (rho0 rho).  This keeps
+    // an O(1) field out of the FP32 sum that drives dB/dt.
+    T px = n.Dx(g, p), py = n.Dy(g, p), pz = n.Dz(g, p);
     T h1 = g.di * (j2 * b3 - j3 * b2 - px) / r;
     T h2 = g.di * (j3 * b1 - j1 * b3 - py) / r;
-    T h3 = g.di * (j1 * b2 - j2 * b1 - pz) / r;
+    T h3 = g.di * (j1 * b2 - j2 * b1 - pz + T(g.dzp0[ks]) * x.f[0][q] / T(g.rho0[ks])) / r;
     if (half) { h1 = T(0.5) * h1; h2 = T(0.5) * h2; h3 = T(0.5) * h3; }
     h.f[0][c] = h1; h.f[1][c] = h2; h.f[2][c] = h3;
 }

@@ -178,6 +178,49 @@ def gem_state_halo(x, y, z, seed_v: int = SEED_V, noise_amp: float = 1e-3, threa
     return H
 
 
+def stencil_weights(h_p1, h_m1, h_p2, h_m2, order=1):
+    """5-point weights a, b, c, d of a (f+ - f0) + b (f0 - f-) + c (f++ - f0) + d (f0 - f--),
+    exact for (x - x0)^n, n = 1..4 (the reference's non-uniform 4th-order stencils,
+    t3dsdsc.f:336-504)."""
+    A = np.array([[h_p1 ** n, -(-h_m1) ** n, h_p2 ** n, -(-h_m2) ** n] for n in range(1, 5)])
+    rhs = np.array([1.0 if n == order else 0.0 for n in range(1, 5)]) * (1.0 if order == 1 else 2.0)
+    return np.linalg.solve(A, rhs)
+
+
+def deriv_coefficients(c: np.ndarray, periodic: bool, L: float | None = None) -> np.ndarray:
+    """(4, n) first-derivative weights per node; zero on the two outer nodes of a bounded
+    axis (the reference leaves them undefined)."""
+    n = c.size
+    if periodic and L is None:
+        L = c[-1] - c[0] + (c[1] - c[0])
+    at = (lambda i: c[i % n] + (i // n) * L) if periodic else (lambda i: c[i])
+    out = np.zeros((4, n))
+    for i in range(n):
+        if periodic or 2 <= i <= n - 3:
+            x0 = at(i)
+            out[:, i] = stencil_weights(at(i + 1) - x0, x0 - at(i - 1), at(i + 2) - x0, x0 - at(i - 2))
+    return out
+
+
+def psi_to_dB(psi: np.ndarray, x: np.ndarray, z: np.ndarray):
+    """The psi perturbation map of dasha_adjoint_flux_grad: on the (x, z) nodes,
+    dBx = -Dz psi (interior z rows; 0 on the 4 wall rows), dBz = Dx psi (all rows), with the
+    4th-order stencils.  psi (mz, mx) -> (dBx, dBz), each (mz, mx), constant in y."""
+    cx = deriv_coefficients(x, True)
+    cz = deriv_coefficients(z, False)
+    mz, mx = psi.shape
+    dbz = np.zeros_like(psi)
+    for s_, (a, sh) in enumerate([(cx[0], 1), (cx[1], -1), (cx[2], 2), (cx[3], -2)]):
+        nb = np.roll(psi, -sh, axis=1)
+        dbz += a[None, :] * ((nb - psi) if sh > 0 else (psi - nb))
+    dbx = np.zeros_like(psi)
+    for k in range(2, mz - 2):
+        a, b, c, d = cz[:, k]
+        dz = a * (psi[k + 1] - psi[k]) + b * (psi[k] - psi[k - 1]) + c * (psi[k + 2] - psi[k]) + d * (psi[k] - psi[k - 2])
+        dbx[k] = -dz
+    return dbx, dbz
+
+
 def to_halo(X: np.ndarray, ld1: int | None = None, ld2: int | None = None) -> np.ndarray:
     """Compact (nf, mz, my, mx) -> reference layout x(ld1, ld2, mz+4, nf) as C-order
     (nf, mz+4, ld2, ld1), physical node (i,j,k) at [m, k+2, j, i+2]; halo filled with NaN."""

@@ -127,6 +127,11 @@ int dasha_diagnostics(dasha_ctx* ctx, double* out);
 int dasha_adjoint_flux_grad(dasha_ctx* ctx, int nsteps, const double* dt_seq, int snaps,
                             double* dPhi_deta, double* dPhi_dpsi);
 
+/* Verification hook of the adjoint (no counterpart in the reference): out = G'(x)^T w, the
+ * transposed Jacobian of one smoothed right-hand side G = avrg(right(.)) at the current state,
+ * applied to w; both in the state layout (8 fields).  FP64 contexts only. */
+int dasha_adjoint_rhs(dasha_ctx* ctx, const double* w_f, double* out_f, long ld1, long ld2);
+
 /* Measurement helpers (no counterpart in the reference).
  * dasha_timer(ctx, 0, NULL) records a start event on the context stream;
  * dasha_timer(ctx, 1, &ms) records a stop event, waits for it and returns the elapsed ms.
