@@ -37,41 +37,59 @@ static __global__ void k_adj_fold_rows(Geo<double> g, F8<double> f, int nf) {
     }
 }
 
-// smoothing coefficient of node (i,j,k) for a kind (0 radial, 1 1/8, 2 x-profile)
-__device__ __forceinline__ double adj_coef(const Geo<double>& g, int kind, int i, int j, int k) {
+// smoothing coefficient of node (i,j,k) for a kind (0 radial, from the precomputed field cr;
+// 1 constant 1/8; 2 x-profile)
+__device__ __forceinline__ double adj_coef(const Geo<double>& g, const double* cr, int kind, int i, int j, int k) {
     if (kind == 1) return 0.125;
     if (kind == 2) return g.cbx[i];
-    const double xx = g.xc[i], yy = g.yc[j], zz = g.zc[k];
-    return radial_coef(sqrt(xx * xx + yy * yy + zz * zz));
+    return cr[(long)i + (long)j * g.sy + (long)k * g.sz];
 }
 
-// transpose of one smoothing pass on rows-folded input ybar (interior rows only nonzero):
+// the radial coefficient at every node, once per adjoint call
+static __global__ void k_adj_cr(Geo<double> g, double* cr) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.mx) return;
+    int j = blockIdx.y, k = blockIdx.z;
+    const double xx = g.xc[i], yy = g.yc[j], zz = g.zc[k];
+    cr[(long)i + (long)j * g.sy + (long)k * g.sz] = radial_coef(sqrt(xx * xx + yy * yy + zz * zz));
+}
+
+// transpose of one smoothing pass.  The input ybar is the adjoint of the pass output with
+// its wall rows; folding them (y(1) = y(2)/2 -> ybar(2) += ybar(1)/2, same at the top; rows 0
+// and mz-1 constant) is done on the fly.  Then
 //   x = y (1 - c sum(wp+wm)) at interior n  +  sum over interior neighbours m of y(m) c(m) w(m->n)
 template <int NFLD>
-__global__ void k_adj_pass(Geo<double> g, FS<double, NFLD> in, FS<double, NFLD> out, unsigned kinds) {
+__global__ void k_adj_pass(Geo<double> g, const double* cr, FS<double, NFLD> in, FS<double, NFLD> out, unsigned kinds) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.mx) return;
     int j = blockIdx.y, k = blockIdx.z;
     const int im = wrapi(i - 1, g.mx), ip = wrapi(i + 1, g.mx), jm = wrapi(j - 1, g.my), jp = wrapi(j + 1, g.my);
     const bool intr = k >= 2 && k <= g.mz - 3;
     const bool zm = (k - 1) >= 2 && (k - 1) <= g.mz - 3, zp = (k + 1) >= 2 && (k + 1) <= g.mz - 3;
-    long c = (long)i + (long)j * g.sy + (long)k * g.sz;
+    const long c = (long)i + (long)j * g.sy + (long)k * g.sz;
+    // folded adjoint at node (ii, jj, kk) of an interior row
+    auto Y = [&](const double* y, long q, int kk) {
+        double v = y[q];
+        if (kk == 2) v += 0.5 * y[q - g.sz];
+        if (kk == g.mz - 3) v += 0.5 * y[q + g.sz];
+        return v;
+    };
 #pragma unroll
     for (int q = 0; q < NFLD; ++q) {
         const int kind = (kinds >> (2 * q)) & 3u;
         const double* y = in.f[q];
         double v = 0.0;
         if (intr) {
-            const double cn = adj_coef(g, kind, i, j, k);
-            v += y[c] * (1.0 - cn * (g.wpx[i] + g.wmx[i] + g.wpy[j] + g.wmy[j] + g.wpz[k] + g.wmz[k]));
+            const double cn = adj_coef(g, cr, kind, i, j, k);
+            v += Y(y, c, k) * (1.0 - cn * (g.wpx[i] + g.wmx[i] + g.wpy[j] + g.wmy[j] + g.wpz[k] + g.wmz[k]));
             // x neighbours (always interior): m = i-1 sees n as its plus neighbour
-            v += y[c - i + im] * adj_coef(g, kind, im, j, k) * g.wpx[im];
-            v += y[c - i + ip] * adj_coef(g, kind, ip, j, k) * g.wmx[ip];
-            v += y[c + (long)(jm - j) * g.sy] * adj_coef(g, kind, i, jm, k) * g.wpy[jm];
-            v += y[c + (long)(jp - j) * g.sy] * adj_coef(g, kind, i, jp, k) * g.wmy[jp];
+            v += Y(y, c - i + im, k) * adj_coef(g, cr, kind, im, j, k) * g.wpx[im];
+            v += Y(y, c - i + ip, k) * adj_coef(g, cr, kind, ip, j, k) * g.wmx[ip];
+            v += Y(y, c + (long)(jm - j) * g.sy, k) * adj_coef(g, cr, kind, i, jm, k) * g.wpy[jm];
+            v += Y(y, c + (long)(jp - j) * g.sy, k) * adj_coef(g, cr, kind, i, jp, k) * g.wmy[jp];
         }
-        if (zm) v += y[c - g.sz] * adj_coef(g, kind, i, j, k - 1) * g.wpz[k - 1];
-        if (zp) v += y[c + g.sz] * adj_coef(g, kind, i, j, k + 1) * g.wmz[k + 1];
+        if (zm) v += Y(y, c - g.sz, k - 1) * adj_coef(g, cr, kind, i, j, k - 1) * g.wpz[k - 1];
+        if (zp) v += Y(y, c + g.sz, k + 1) * adj_coef(g, cr, kind, i, j, k + 1) * g.wmz[k + 1];
         out.f[q][c] = v;
     }
 }

@@ -635,7 +635,8 @@ public:
 
     void k8(T** d, T* const* s2) { for (int m = 0; m < 8; ++m) d[m] = s2[m]; }
     void copy8(T* const* dst, T* const* src) {
-        for (int m = 0; m < 8; ++m) cudaMemcpyAsync(dst[m], src[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
+        DASHA_LAUNCH("a_copy8", 16.0 * N * sizeof(T),
+                     for (int m = 0; m < 8; ++m) cudaMemcpyAsync(dst[m], src[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st));
     }
     void zero8(T* const* f, int nf = 8) { for (int m = 0; m < nf; ++m) cudaMemsetAsync(f[m], 0, sizeof(T) * N, st); }
     void axpby8(T* const* y, double b, T* const* x, double a) {
@@ -643,7 +644,7 @@ public:
             long nb = (N + 255) / 256;
             F8<double> Y, Xv;
             for (int m = 0; m < 8; ++m) { Y.f[m] = y[m]; Xv.f[m] = x[m]; }
-            k_axpby8<<<nb, 256, 0, st>>>(N, Y, b, Xv, a);
+            DASHA_LAUNCH("a_axpby", 24.0 * N * 8, k_axpby8<<<nb, 256, 0, st>>>(N, Y, b, Xv, a));
         }
     }
 
@@ -680,20 +681,17 @@ public:
     T** adj_passes(T** a, T** b, int nf, int n, unsigned kinds3, bool fold_after) {
         if constexpr (std::is_same<T, double>::value) {
             dim3 gf((mx + blk.x - 1) / blk.x, my, 1);
-            for (int p = 0; p < n; ++p) {
-                F8<double> fa{};
-                for (int m = 0; m < nf; ++m) fa.f[m] = a[m];
-                k_adj_fold_rows<<<gf, blk, 0, st>>>(g, fa, nf);
+            for (int p = 0; p < n; ++p) {   // each transposed pass folds its input rows itself
                 if (nf == 3) {
                     FS<double, 3> in, out;
                     for (int m = 0; m < 3; ++m) { in.f[m] = a[m]; out.f[m] = b[m]; }
-                    k_adj_pass<3><<<grd, blk, 0, st>>>(g, in, out, kinds3);
+                    DASHA_LAUNCH("a_pass3", 6.0 * N * 8, k_adj_pass<3><<<grd, blk, 0, st>>>(g, adj_cr, in, out, kinds3));
                 } else {
                     FS<double, 4> in, out;
                     for (int m = 0; m < 4; ++m) { in.f[m] = a[m]; out.f[m] = b[m]; }
-                    k_adj_pass<4><<<grd, blk, 0, st>>>(g, in, out, 0u);
+                    DASHA_LAUNCH("a_pass4", 8.0 * N * 8, k_adj_pass<4><<<grd, blk, 0, st>>>(g, adj_cr, in, out, 0u));
                     for (int m = 0; m < 4; ++m) { in.f[m] = a[4 + m]; out.f[m] = b[4 + m]; }
-                    k_adj_pass<4><<<grd, blk, 0, st>>>(g, in, out, KIND_B4);
+                    DASHA_LAUNCH("a_pass4", 8.0 * N * 8, k_adj_pass<4><<<grd, blk, 0, st>>>(g, adj_cr, in, out, KIND_B4));
                 }
                 std::swap(a, b);
             }
@@ -722,7 +720,7 @@ public:
             // induction: o_B = -curl(E_total)  ->  Et_bar = -curl^T(o_B)
             F3<double> ob3, et3;
             for (int m = 0; m < 3; ++m) { ob3.f[m] = rb[4 + m]; et3.f[m] = w.et[m]; }
-            k_adj_curlT<<<grd, blk, 0, st>>>(g, ob3, et3, -1.0, 0);
+            DASHA_LAUNCH("a_curlT", 6.0 * N * 8, k_adj_curlT<<<grd, blk, 0, st>>>(g, ob3, et3, -1.0, 0));
             // E chain: 4 transposed avrgE passes -> adjoint of E0 (all nodes)
             for (int m = 0; m < 3; ++m) cudaMemcpyAsync(w.e0[m], w.et[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
             T** eb = adj_passes(w.e0, w.e1, 3, 4, 0u, false);
@@ -741,23 +739,28 @@ public:
             ap.ob[0] = rb[0]; ap.ob[1] = rb[1]; ap.ob[2] = rb[2]; ap.ob[3] = rb[3]; ap.ob[4] = rb[7];
             ap.etapart = w.etap;
             ap.hall = P.hall;
-            k_adj_pointwise<<<grd, blk, 0, st>>>(g, ap);
-            k_reduce_add<<<1, 256, 0, st>>>(w.etap, w.netap, w.eta_acc);
+            DASHA_LAUNCH("a_pointwise", 30.0 * N * 8, k_adj_pointwise<<<grd, blk, 0, st>>>(g, ap));
+            DASHA_LAUNCH("a_reduce", 0.0, k_reduce_add<<<1, 256, 0, st>>>(w.etap, w.netap, w.eta_acc));
             AdjGat ag;
             for (int m = 0; m < 8; ++m) { ag.s.f[m] = Sx[m]; ag.sb.f[m] = w.sb[m]; ag.wq.f[m] = w.wq[m]; }
             for (int m = 0; m < 3; ++m) ag.ub.f[m] = w.ub[m];
             ag.ob[0] = rb[0]; ag.ob[1] = rb[1]; ag.ob[2] = rb[2]; ag.ob[3] = rb[3]; ag.ob[4] = rb[7];
-            k_adj_gather<<<grd, blk, 0, st>>>(g, ag);
+            DASHA_LAUNCH("a_gather", 25.0 * N * 8, k_adj_gather<<<grd, blk, 0, st>>>(g, ag));
             // current chain: 4 transposed avrgc passes, the curl's rows folded, curl^T into B
             T** jt = adj_passes(w.jb, w.jt, 3, 4, 0u, true);
             F3<double> jw, bo;
             for (int m = 0; m < 3; ++m) { jw.f[m] = jt[m]; bo.f[m] = w.sb[4 + m]; }
-            k_adj_curlT<<<grd, blk, 0, st>>>(g, jw, bo, 1.0, 1);
+            DASHA_LAUNCH("a_curlT", 9.0 * N * 8, k_adj_curlT<<<grd, blk, 0, st>>>(g, jw, bo, 1.0, 1));
             for (int m = 0; m < 8; ++m) cudaMemcpyAsync(sigma[m], w.sb[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
         }
     }
 
+    double* adj_cr = nullptr;   // radial coefficient field of the current adjoint call
     bool adj_scratch(AdjBufs& B, AdjScratch& w) {
+        if constexpr (std::is_same<T, double>::value) {
+            if (!(adj_cr = B.take(N))) return false;
+            k_adj_cr<<<grd, blk, 0, st>>>(g, adj_cr);
+        }
         auto t8 = [&](T** a) { for (int m = 0; m < 8; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
         auto t3 = [&](T** a) { for (int m = 0; m < 3; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
         if (!t8(w.a8) || !t8(w.b8) || !t8(w.sb) || !t8(w.wq)) return false;
@@ -804,12 +807,25 @@ public:
             auto take8 = [&](T** a) { for (int m = 0; m < 8; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
             std::vector<std::vector<T*>> snap(std::max(nseg, 1), std::vector<T*>(8));
             std::vector<std::vector<T*>> sst(seg + 1, std::vector<T*>(8));
+            // stage states of every step of a segment, kept from the segment recompute when
+            // they fit (else each reverse step recomputes its own)
+            std::vector<std::vector<T*>> stg;
             T *X0[8], *S1[8], *S2[8], *S3[8], *Xo[8], *Ac[8], *lam[8], *mu[8], *kap[8], *sig[8], *tot[8], *ta[8], *tb[8];
             bool ok = take8(X0) && take8(S1) && take8(S2) && take8(S3) && take8(Xo) && take8(Ac) && take8(lam) && take8(mu) &&
                       take8(kap) && take8(sig) && take8(tot) && take8(ta) && take8(tb);
             for (auto& v : snap) ok = ok && take8(v.data());
             for (auto& v : sst) ok = ok && take8(v.data());
             if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
+            {
+                size_t freeb = 0, totb = 0;
+                cudaMemGetInfo(&freeb, &totb);
+                const double need = 24.0 * seg * N * sizeof(T);
+                if (need < 0.8 * (double)freeb) {
+                    stg.assign(3L * seg, std::vector<T*>(8));
+                    for (auto& v : stg) ok = ok && take8(v.data());
+                    if (!ok) { stg.clear(); ok = true; cudaGetLastError(); }
+                }
+            }
             copy8(X0, X);
             // forward sweep with segment snapshots
             T *cur8[8], *nxt8[8];
@@ -831,12 +847,19 @@ public:
             for (int sgi = nseg - 1; sgi >= 0; --sgi) {
                 const int n0 = sgi * seg, n1 = std::min(nsteps, n0 + seg);
                 copy8(sst[0].data(), snap[sgi].data());
-                for (int n = n0; n < n1 - 1; ++n)
-                    fwd_step(sst[n - n0].data(), dts[n], n % every == 0, S1, S2, S3, sst[n - n0 + 1].data(), Ac);
+                const bool keep = !stg.empty();
+                for (int n = n0; n < n1 - 1; ++n) {
+                    const int q = n - n0;
+                    fwd_step(sst[q].data(), dts[n], n % every == 0, keep ? stg[3 * q].data() : S1,
+                             keep ? stg[3 * q + 1].data() : S2, keep ? stg[3 * q + 2].data() : S3, sst[q + 1].data(), Ac);
+                }
                 for (int n = n1 - 1; n >= n0; --n) {
-                    T* const* Xn = sst[n - n0].data();
+                    const int q = n - n0;
+                    T* const* Xn = sst[q].data();
                     const double dt = dts[n];
-                    fwd_step(Xn, dt, false, S1, S2, S3, Xo, Ac);       // stage states of step n
+                    T *const *s1 = S1, *const *s2 = S2, *const *s3 = S3;
+                    if (keep && n < n1 - 1) { s1 = stg[3 * q].data(); s2 = stg[3 * q + 1].data(); s3 = stg[3 * q + 2].data(); }
+                    else fwd_step(Xn, dt, false, S1, S2, S3, Xo, Ac);  // stage states of step n
                     // mu = F^T lambda
                     if (n % every == 0) {
                         copy8(ta, lam);
@@ -848,15 +871,15 @@ public:
                     copy8(tot, mu);                                    // lambda_X = mu + sum sigma
                     copy8(kap, mu);
                     axpby8(kap, dt / 6.0, mu, 0.0);                    // kappa4 = dt/6 mu
-                    adj_rhs(S3, kap, sig, w);                          // sigma3
+                    adj_rhs(s3, kap, sig, w);                          // sigma3
                     axpby8(tot, 1.0, sig, 1.0);
                     axpby8(kap, 0.0, mu, dt / 3.0);                    // kappa3 = dt/3 mu + dt sigma3
                     axpby8(kap, 1.0, sig, dt);
-                    adj_rhs(S2, kap, sig, w);                          // sigma2
+                    adj_rhs(s2, kap, sig, w);                          // sigma2
                     axpby8(tot, 1.0, sig, 1.0);
                     axpby8(kap, 0.0, mu, dt / 3.0);                    // kappa2 = dt/3 mu + dt/2 sigma2
                     axpby8(kap, 1.0, sig, dt / 2.0);
-                    adj_rhs(S1, kap, sig, w);                          // sigma1
+                    adj_rhs(s1, kap, sig, w);                          // sigma1
                     axpby8(tot, 1.0, sig, 1.0);
                     axpby8(kap, 0.0, mu, dt / 6.0);                    // kappa1 = dt/6 mu + dt/2 sigma1
                     axpby8(kap, 1.0, sig, dt / 2.0);
