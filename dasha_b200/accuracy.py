@@ -40,8 +40,12 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--check", type=int, nargs="*", default=[100, 500, 1000])
     ap.add_argument("--out", default=None)
+    ap.add_argument("--hall", type=int, default=None)
     a = ap.parse_args(argv)
     cfg = harris.CONFIGS[a.config]
+    if a.hall is not None:
+        import dataclasses
+        cfg = dataclasses.replace(cfg, hall=a.hall)
     x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
     rho0, b0, p0, _ = harris.harris_profiles(z)
     eq = np.zeros((8, cfg.mz, 1, 1))

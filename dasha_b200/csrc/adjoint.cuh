@@ -74,22 +74,35 @@ __global__ void k_adj_pass(Geo<double> g, const double* cr, FS<double, NFLD> in,
         if (kk == g.mz - 3) v += 0.5 * y[q + g.sz];
         return v;
     };
+    // neighbour coefficients, loaded once per kind (the fields of one launch share at most two)
+    int lastkind = -1;
+    double cn = 0, cxm = 0, cxp = 0, cym = 0, cyp = 0, czm = 0, czp = 0;
 #pragma unroll
     for (int q = 0; q < NFLD; ++q) {
         const int kind = (kinds >> (2 * q)) & 3u;
+        if (kind != lastkind) {
+            lastkind = kind;
+            if (intr) {
+                cn = adj_coef(g, cr, kind, i, j, k) * (g.wpx[i] + g.wmx[i] + g.wpy[j] + g.wmy[j] + g.wpz[k] + g.wmz[k]);
+                cxm = adj_coef(g, cr, kind, im, j, k) * g.wpx[im];
+                cxp = adj_coef(g, cr, kind, ip, j, k) * g.wmx[ip];
+                cym = adj_coef(g, cr, kind, i, jm, k) * g.wpy[jm];
+                cyp = adj_coef(g, cr, kind, i, jp, k) * g.wmy[jp];
+            }
+            if (zm) czm = adj_coef(g, cr, kind, i, j, k - 1) * g.wpz[k - 1];
+            if (zp) czp = adj_coef(g, cr, kind, i, j, k + 1) * g.wmz[k + 1];
+        }
         const double* y = in.f[q];
         double v = 0.0;
         if (intr) {
-            const double cn = adj_coef(g, cr, kind, i, j, k);
-            v += Y(y, c, k) * (1.0 - cn * (g.wpx[i] + g.wmx[i] + g.wpy[j] + g.wmy[j] + g.wpz[k] + g.wmz[k]));
-            // x neighbours (always interior): m = i-1 sees n as its plus neighbour
-            v += Y(y, c - i + im, k) * adj_coef(g, cr, kind, im, j, k) * g.wpx[im];
-            v += Y(y, c - i + ip, k) * adj_coef(g, cr, kind, ip, j, k) * g.wmx[ip];
-            v += Y(y, c + (long)(jm - j) * g.sy, k) * adj_coef(g, cr, kind, i, jm, k) * g.wpy[jm];
-            v += Y(y, c + (long)(jp - j) * g.sy, k) * adj_coef(g, cr, kind, i, jp, k) * g.wmy[jp];
+            v += Y(y, c, k) * (1.0 - cn);
+            v += Y(y, c - i + im, k) * cxm;
+            v += Y(y, c - i + ip, k) * cxp;
+            v += Y(y, c + (long)(jm - j) * g.sy, k) * cym;
+            v += Y(y, c + (long)(jp - j) * g.sy, k) * cyp;
         }
-        if (zm) v += Y(y, c - g.sz, k - 1) * adj_coef(g, cr, kind, i, j, k - 1) * g.wpz[k - 1];
-        if (zp) v += Y(y, c + g.sz, k + 1) * adj_coef(g, cr, kind, i, j, k + 1) * g.wmz[k + 1];
+        if (zm) v += Y(y, c - g.sz, k - 1) * czm;
+        if (zp) v += Y(y, c + g.sz, k + 1) * czp;
         out.f[q][c] = v;
     }
 }

@@ -383,21 +383,24 @@ public:
         return (mz + nch - 1) / nch;
     }
     // k_zpass tiling: 32 x 16 columns per CTA (256 threads, 2 rows each), 4 planes in flight
-    static constexpr int ZTX = 32, ZTYH = 8, ZRY = sizeof(T) == 4 ? 2 : 1, ZD = 4;
+    static constexpr int ZTX = 32, ZTYH = 8, ZD = 4;
+    // rows per thread: 2 for the 4-field FP32 passes, 1 otherwise (smaller ring, more CTAs/SM)
     template <int NF>
-    using ZPc = ZP<T, NF, ZTX, ZTYH, ZRY, ZD>;
+    static constexpr int zry() { return (sizeof(T) == 4 && NF == 4) ? 2 : 1; }
+    template <int NF>
+    using ZPc = ZP<T, NF, ZTX, ZTYH, zry<NF>(), ZD>;
     // one smoothing pass of NF fields: src -> epi
     template <int NF, unsigned KINDS, class Epi>
     void zp(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
         dim3 gg(mx / ZTX, (my + ZPc<NF>::TY - 1) / ZPc<NF>::TY, 1);
         int ch = zchunk(gg.x * gg.y, 16);
         gg.z = (mz + ch - 1) / ch;
-        DASHA_LAUNCH(tag, bytes, (k_zpass<T, NF, KINDS, ZTX, ZTYH, ZRY, ZD, Epi>
+        DASHA_LAUNCH(tag, bytes, (k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi>
                                   <<<gg, ZTX * ZTYH, ZPc<NF>::smem(), st>>>(g, src, epi, ch)));
     }
     template <int NF, unsigned KINDS, class Epi>
     static cudaError_t zp_attr1() {
-        return cudaFuncSetAttribute(k_zpass<T, NF, KINDS, ZTX, ZTYH, ZRY, ZD, Epi>,
+        return cudaFuncSetAttribute(k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZPc<NF>::smem());
     }
     cudaError_t zs_attr() {
@@ -621,16 +624,25 @@ public:
 
     // ======================= discrete adjoint (FP64 contexts) =======================
     // scratch of one adjoint call (cudaMalloc'd per call, freed at the end)
+    // scratch of one adjoint call: one cudaMalloc carved into fields (freed at the end)
     struct AdjBufs {
-        std::vector<void*> mem;
-        double* take(size_t n) {
-            void* p = nullptr;
-            if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) { cudaGetLastError(); return nullptr; }
-            mem.push_back(p);
-            return (double*)p;
+        char* base = nullptr;
+        size_t cap = 0, used = 0;
+        bool reserve(size_t bytes) {
+            if (cudaMalloc((void**)&base, bytes) != cudaSuccess) { cudaGetLastError(); base = nullptr; return false; }
+            cap = bytes;
+            return true;
         }
-        ~AdjBufs() { for (void* p : mem) cudaFree(p); }
+        double* take(size_t n) {
+            size_t b = (n * sizeof(double) + 255) & ~(size_t)255;
+            if (!base || used + b > cap) return nullptr;
+            double* p = (double*)(base + used);
+            used += b;
+            return p;
+        }
+        ~AdjBufs() { if (base) cudaFree(base); }
     };
+    static size_t adj_field_bytes(long n) { return ((size_t)n * sizeof(double) + 255) & ~(size_t)255; }
     struct V8 { T* f[8]; };
 
     void k8(T** d, T* const* s2) { for (int m = 0; m < 8; ++m) d[m] = s2[m]; }
@@ -755,6 +767,7 @@ public:
         }
     }
 
+    long w_netap_max() const { return (long)grd.x * grd.y * grd.z; }
     double* adj_cr = nullptr;   // radial coefficient field of the current adjoint call
     bool adj_scratch(AdjBufs& B, AdjScratch& w) {
         if constexpr (std::is_same<T, double>::value) {
@@ -780,6 +793,8 @@ public:
             AdjBufs B;
             AdjScratch w;
             T *kap[8], *sig[8];
+            if (!B.reserve(adj_field_bytes(N) * (60 + 16) + adj_field_bytes(w_netap_max()) + 4096))
+                return Status::err(DASHA_E_NOMEM, "adjoint scratch");
             if (!adj_scratch(B, w)) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
             for (int m = 0; m < 8; ++m) {
                 if (!(kap[m] = (T*)B.take(N)) || !(sig[m] = (T*)B.take(N))) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
@@ -803,6 +818,16 @@ public:
             const int nseg = (nsteps + seg - 1) / seg;
             AdjBufs B;
             AdjScratch w;
+            // fields: scratch 60, 13 work vectors of 8, snapshots, segment states, stage states
+            size_t freeb = 0, totb = 0;
+            cudaMemGetInfo(&freeb, &totb);
+            const size_t fb = adj_field_bytes(N);
+            const size_t base_fields = 60 + 13 * 8 + (size_t)std::max(nseg, 1) * 8 + (size_t)(seg + 1) * 8;
+            const size_t extra = adj_field_bytes(w_netap_max()) + adj_field_bytes((long)mx * mz) + 8192;
+            const size_t with_stages = (base_fields + 24 * (size_t)seg) * fb + extra;
+            const bool keep_stages = (double)with_stages < 0.85 * (double)freeb;
+            if (!B.reserve(keep_stages ? with_stages : base_fields * fb + extra))
+                return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
             if (!adj_scratch(B, w)) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
             auto take8 = [&](T** a) { for (int m = 0; m < 8; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
             std::vector<std::vector<T*>> snap(std::max(nseg, 1), std::vector<T*>(8));
@@ -816,15 +841,10 @@ public:
             for (auto& v : snap) ok = ok && take8(v.data());
             for (auto& v : sst) ok = ok && take8(v.data());
             if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
-            {
-                size_t freeb = 0, totb = 0;
-                cudaMemGetInfo(&freeb, &totb);
-                const double need = 24.0 * seg * N * sizeof(T);
-                if (need < 0.8 * (double)freeb) {
-                    stg.assign(3L * seg, std::vector<T*>(8));
-                    for (auto& v : stg) ok = ok && take8(v.data());
-                    if (!ok) { stg.clear(); ok = true; cudaGetLastError(); }
-                }
+            if (keep_stages) {
+                stg.assign(3L * seg, std::vector<T*>(8));
+                for (auto& v : stg) ok = ok && take8(v.data());
+                if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint stage states");
             }
             copy8(X0, X);
             // forward sweep with segment snapshots

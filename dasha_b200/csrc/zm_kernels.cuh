@@ -616,6 +616,9 @@ __global__ void __launch_bounds__(TX* TYH) k_zpass(Geo<T> g, SrcFields<T, NF> sr
 #pragma unroll
     for (int u = 0; u < RY; ++u)
         if (gj[u] < g.my) epi.pre((long)gi + (long)gj[u] * g.sy + (long)cA * g.sz, npre[u]);
+    // own column: planes c-1 and c in registers (z queue); plane c+1 read from the ring
+    T qm[RY][NF], q0[RY][NF];
+    bool primed = false;
     for (int c = cA; c <= cB; ++c) {
         issue(c + 1 + D);
         const T wpz = nwpz, wmz = nwmz;
@@ -632,36 +635,51 @@ __global__ void __launch_bounds__(TX* TYH) k_zpass(Geo<T> g, SrcFields<T, NF> sr
         cp_async_wait<D>();
         __syncthreads();
         const T* pc = ring + (long)(c & (NS - 1)) * NF * SP;
-        const T* pm = ring + (long)((c - 1) & (NS - 1)) * NF * SP;
         const T* pp = ring + (long)((c + 1) & (NS - 1)) * NF * SP;
+        if (!primed) {
+            const T* pm = ring + (long)((c - 1) & (NS - 1)) * NF * SP;
+#pragma unroll
+            for (int u = 0; u < RY; ++u) {
+                const int me = (tyh + u * TYH + 1) * RS + OFF + tx;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) { qm[u][f] = pm[f * SP + me]; q0[u][f] = pc[f * SP + me]; }
+            }
+            primed = true;
+        }
 #pragma unroll
         for (int u = 0; u < RY; ++u) {
-            if (gj[u] >= g.my) continue;
             const int me = (tyh + u * TYH + 1) * RS + OFF + tx;
-            T cr = T(0);
-            if (any_kind0(KINDS, NF)) cr = radial_coef_fast(rr2[u] + zz2);
-            T val[NF];
+            T qp[NF];
 #pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const T* a = pc + f * SP;
-                const T v0 = a[me];
-                const T tx_ = (a[me + 1] - v0) * wpx - (v0 - a[me - 1]) * wmx;
-                const T ty_ = (a[me + RS] - v0) * wpy[u] - (v0 - a[me - RS]) * wmy[u];
-                const T tz_ = (pp[f * SP + me] - v0) * wpz - (v0 - pm[f * SP + me]) * wmz;
-                const unsigned kind = (KINDS >> (2 * f)) & 3u;
-                const T coef = kind == 0u ? cr : (kind == 1u ? T(0.125) : cbx);
-                val[f] = v0 + coef * (tx_ + ty_ + tz_);
-            }
-            const long col = (long)gi + (long)gj[u] * g.sy;
-            epi.store(g, col + (long)c * g.sz, val, cpre[u]);
-            if (c == 2 || c == mz - 3) {
-                T hv[NF], zv[NF];
+            for (int f = 0; f < NF; ++f) qp[f] = pp[f * SP + me];
+            if (gj[u] < g.my) {
+                T cr = T(0);
+                if (any_kind0(KINDS, NF)) cr = radial_coef_fast(rr2[u] + zz2);
+                T val[NF];
 #pragma unroll
-                for (int f = 0; f < NF; ++f) { hv[f] = T(0.5) * val[f]; zv[f] = T(0); }
-                const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
-                epi.store(g, col + (long)kh * g.sz, hv);
-                epi.store(g, col + (long)kz * g.sz, zv);
+                for (int f = 0; f < NF; ++f) {
+                    const T* a = pc + f * SP;
+                    const T v0 = q0[u][f];
+                    const T tx_ = (a[me + 1] - v0) * wpx - (v0 - a[me - 1]) * wmx;
+                    const T ty_ = (a[me + RS] - v0) * wpy[u] - (v0 - a[me - RS]) * wmy[u];
+                    const T tz_ = (qp[f] - v0) * wpz - (v0 - qm[u][f]) * wmz;
+                    const unsigned kind = (KINDS >> (2 * f)) & 3u;
+                    const T coef = kind == 0u ? cr : (kind == 1u ? T(0.125) : cbx);
+                    val[f] = v0 + coef * (tx_ + ty_ + tz_);
+                }
+                const long col = (long)gi + (long)gj[u] * g.sy;
+                epi.store(g, col + (long)c * g.sz, val, cpre[u]);
+                if (c == 2 || c == mz - 3) {
+                    T hv[NF], zv[NF];
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) { hv[f] = T(0.5) * val[f]; zv[f] = T(0); }
+                    const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
+                    epi.store(g, col + (long)kh * g.sz, hv);
+                    epi.store(g, col + (long)kz * g.sz, zv);
+                }
             }
+#pragma unroll
+            for (int f = 0; f < NF; ++f) { qm[u][f] = q0[u][f]; q0[u][f] = qp[f]; }
         }
     }
     cp_async_wait<0>();
