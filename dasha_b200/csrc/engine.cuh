@@ -332,9 +332,10 @@ public:
         return s;
     }
     void k_import_one(const double* stage, long ld1, long ld2, int m, T* dst, bool sub_eq);
-    void k_export_one(const T* src, long ld1, long ld2, int m, double* stage, bool add_eq);
+    void k_export_one(const T* src, const T* comp, long ld1, long ld2, int m, double* stage, bool add_eq);
 
-    Status transfer_out(double* host, long ld1, long ld2, T* const* src, int nf, bool add_eq) {
+    Status transfer_out(double* host, long ld1, long ld2, T* const* src, int nf, bool add_eq,
+                        T* const* comp = nullptr) {
         size_t plane = (size_t)ld1 * ld2 * (mz + 4);
         double* stage = nullptr;
         DASHA_CK(cudaMalloc(&stage, sizeof(double) * plane));
@@ -343,7 +344,7 @@ public:
             // keep the caller's halo entries: start from the host field
             cudaError_t e = cudaMemcpyAsync(stage, host + plane * m, sizeof(double) * plane, cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
-            k_export_one(src[m], ld1, ld2, m, stage, add_eq);
+            k_export_one(src[m], comp ? comp[m] : nullptr, ld1, ld2, m, stage, add_eq);
             e = cudaMemcpyAsync(host + plane * m, stage, sizeof(double) * plane, cudaMemcpyDeviceToHost, st);
             if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
             e = cudaStreamSynchronize(st);
@@ -361,7 +362,9 @@ public:
         DASHA_CK(cudaStreamSynchronize(st));
         return Status::ok();
     }
-    Status get_state(double* x, long ld1, long ld2) override { return transfer_out(x, ld1, ld2, X, 8, true); }
+    Status get_state(double* x, long ld1, long ld2) override {
+        return transfer_out(x, ld1, ld2, X, 8, true, KAHAN ? C : nullptr);
+    }
 
     // ---- the RHS chain (right, t3dsdsc.f:1297-1673) ----
     template <int NFLD>
@@ -390,17 +393,17 @@ public:
     template <int NF>
     using ZPc = ZP<T, NF, ZTX, ZTYH, zry<NF>(), ZD>;
     // one smoothing pass of NF fields: src -> epi
-    template <int NF, unsigned KINDS, class Epi>
+    template <int NF, unsigned KINDS, int MODE = 0, class Epi>
     void zp(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
         dim3 gg(mx / ZTX, (my + ZPc<NF>::TY - 1) / ZPc<NF>::TY, 1);
         int ch = zchunk(gg.x * gg.y, 16);
         gg.z = (mz + ch - 1) / ch;
-        DASHA_LAUNCH(tag, bytes, (k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi>
+        DASHA_LAUNCH(tag, bytes, (k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi, MODE>
                                   <<<gg, ZTX * ZTYH, ZPc<NF>::smem(), st>>>(g, src, epi, ch)));
     }
-    template <int NF, unsigned KINDS, class Epi>
+    template <int NF, unsigned KINDS, class Epi, int MODE = 0>
     static cudaError_t zp_attr1() {
-        return cudaFuncSetAttribute(k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi>,
+        return cudaFuncSetAttribute(k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi, MODE>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZPc<NF>::smem());
     }
     cudaError_t zs_attr() {
@@ -412,6 +415,12 @@ public:
         if ((e = zp_attr1<4, KIND_B4, EpiStore<T, 4>>())) return e;
         if ((e = zp_attr1<4, 0u, EpiRK<T, 4, KAHAN>>())) return e;
         if ((e = zp_attr1<4, KIND_B4, EpiRK<T, 4, KAHAN>>())) return e;
+        if constexpr (KAHAN) {
+            if ((e = zp_attr1<8, 0u, EpiStore<T, 4>, 1>())) return e;
+            if ((e = zp_attr1<8, KIND_B4, EpiStore<T, 4>, 1>())) return e;
+            if ((e = zp_attr1<4, 0u, EpiKF<T, 4>, 2>())) return e;
+            if ((e = zp_attr1<4, KIND_B4, EpiKF<T, 4>, 2>())) return e;
+        }
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
             return e;
@@ -443,6 +452,24 @@ public:
         zp<4, KIND_B4>(tag, 0.5 * bytes_per_cell * N * sizeof(T), b, mk(4));
     }
     static EpiStore<T, 4> st4(T* const* p, int lo) { EpiStore<T, 4> s; for (int q = 0; q < 4; ++q) s.f[q] = p[lo + q]; return s; }
+
+    // avrgtt on the compensated FP32 state (X, C): pass 1 writes its increment of X - C into
+    // t, pass 2 adds the two-pass increment to (X, C) in place with a Kahan step
+    void filter_compensated(T* const* t) {
+        for (int lo = 0; lo < 8; lo += 4) {
+            SrcFields<T, 8> a;
+            for (int q = 0; q < 4; ++q) { a.f[q] = X[lo + q]; a.f[4 + q] = C[lo + q]; }
+            if (lo == 0) zp<8, 0u, 1>("k_zpass_F1", 12.0 * N * sizeof(T), a, st4(t, lo));
+            else zp<8, KIND_B4, 1>("k_zpass_F1", 12.0 * N * sizeof(T), a, st4(t, lo));
+        }
+        for (int lo = 0; lo < 8; lo += 4) {
+            SrcFields<T, 4> d;
+            EpiKF<T, 4> e;
+            for (int q = 0; q < 4; ++q) { d.f[q] = t[lo + q]; e.x[q] = X[lo + q]; e.comp[q] = C[lo + q]; }
+            if (lo == 0) zp<4, 0u, 2>("k_zpass_F2", 20.0 * N * sizeof(T), d, e);
+            else zp<4, KIND_B4, 2>("k_zpass_F2", 20.0 * N * sizeof(T), d, e);
+        }
+    }
 
     T** curF = nullptr;   // smoothed current after launch_current
     T** Ef = nullptr;     // total E after launch_rhs_raw
@@ -553,9 +580,13 @@ public:
         if (nstep % every == 0) {   // avrgtt on the perturbation (t3dsdsc.f:1135-1165)
             T* t[8];
             tmp8(t);
-            pass8("k_zpass_F", 16.0, X, [&](int lo) { return st4(t, lo); });
-            pass8("k_zpass_F", 16.0, t, [&](int lo) { return st4(S, lo); });
-            for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
+            if constexpr (KAHAN) {
+                filter_compensated(t);
+            } else {
+                pass8("k_zpass_F", 16.0, X, [&](int lo) { return st4(t, lo); });
+                pass8("k_zpass_F", 16.0, t, [&](int lo) { return st4(S, lo); });
+                for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
+            }
         }
         if (nstep % 10 == 0) {      // diagn blow-up guard (t3dsdsc.f:1174-1182, 1232)
             Status s = launch_diag(true);
@@ -937,12 +968,14 @@ __global__ void k_import_field(int mx, int my, int mz, const double* src, long l
     dst[(long)i + (long)mx * (j + (long)my * k)] = T(v);
 }
 template <class T>
-__global__ void k_export_field(int mx, int my, int mz, const T* src, const double* eqprof, double* dst, long ld1,
-                               long ld2) {
+__global__ void k_export_field(int mx, int my, int mz, const T* src, const T* comp, const double* eqprof, double* dst,
+                               long ld1, long ld2) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= mx) return;
     int j = blockIdx.y, k = blockIdx.z;
-    double v = (double)src[(long)i + (long)mx * (j + (long)my * k)];
+    const long n = (long)i + (long)mx * (j + (long)my * k);
+    double v = (double)src[n];
+    if (comp) v -= (double)comp[n];   // compensated FP32 state: the value is x - comp
     if (eqprof) v += eqprof[k];
     dst[(i + 2) + ld1 * (j + ld2 * (long)(k + 2))] = v;
 }
@@ -965,9 +998,9 @@ void Engine<T>::k_import_one(const double* stage, long ld1, long ld2, int m, T* 
     k_import_field<T><<<grd, blk, 0, st>>>(mx, my, mz, stage, ld1, ld2, 1.0, prof, dst);
 }
 template <class T>
-void Engine<T>::k_export_one(const T* src, long ld1, long ld2, int m, double* stage, bool add_eq) {
+void Engine<T>::k_export_one(const T* src, const T* comp, long ld1, long ld2, int m, double* stage, bool add_eq) {
     const double* prof = add_eq ? eq_profile(g, m) : nullptr;
-    k_export_field<T><<<grd, blk, 0, st>>>(mx, my, mz, src, prof, stage, ld1, ld2);
+    k_export_field<T><<<grd, blk, 0, st>>>(mx, my, mz, src, comp, prof, stage, ld1, ld2);
 }
 
 }  // namespace dasha

@@ -93,6 +93,37 @@ struct EpiAcc {   // f = a + v   (a may alias f: each node is read and written b
     }
 };
 
+// Post-step filter on a compensated FP32 state (x, comp), exact value x - comp: the filter's
+// increment v is added with a Kahan step, and the wall rows of the result are set to the exact
+// halves / zeros of row 2 and row mz-3 (bndrytt), so the filter loses no more than the
+// increment's own rounding.
+template <class T, int NF>
+struct EpiKF {
+    T* x[NF];
+    T* comp[NF];
+    struct Pre { T x[NF], k[NF]; };
+    __device__ __forceinline__ void pre(long idx, Pre& p) const {
+#pragma unroll
+        for (int q = 0; q < NF; ++q) { p.x[q] = x[q][idx]; p.k[q] = comp[q][idx]; }
+    }
+    // interior node idx; when wall, also the wall-adjacent row ih (half) and the wall row iz (0)
+    __device__ __forceinline__ void store_rows(long idx, bool wall, long ih, long iz, const T v[NF],
+                                               const Pre& p) const {
+#pragma unroll
+        for (int q = 0; q < NF; ++q) {
+            const T y = v[q] - p.k[q];
+            const T t = p.x[q] + y;
+            const T kk = (t - p.x[q]) - y;
+            x[q][idx] = t;
+            comp[q][idx] = kk;
+            if (wall) {
+                x[q][ih] = T(0.5) * t; comp[q][ih] = T(0.5) * kk;
+                x[q][iz] = T(0); comp[q][iz] = T(0);
+            }
+        }
+    }
+};
+
 // RK4 stage update with the smoothed xdif (stepon t3dsdsc.f:1090-1132), same arithmetic as
 // k_rk: plain registers (base, acc = xm, x) in FP64, increment-only acc plus a Kahan base
 // update in FP32.
@@ -521,6 +552,10 @@ __device__ __forceinline__ double radial_coef_fast(double r2) { return radial_co
 // copies for the two halo columns).  The stage being refilled is never one of the three
 // being read, so one barrier per plane suffices.  KINDS: 2 bits per field, 0 radial
 // coefficient, 1 constant 1/8, 2 x-profile (B in avrg/avrgtt).  Needs mx % TX == 0.
+// MODE 0 writes the smoothed fields.  MODES 1 and 2 are the two passes of avrgtt on a
+// compensated FP32 state (x, comp): MODE 1 reads x in fields 0..NF/2-1 and comp in the rest
+// and writes the first pass's increment d of x - comp; MODE 2 reads d and hands the two-pass
+// increment to a Kahan epilogue (EpiKF).
 __host__ __device__ constexpr bool any_kind0(unsigned kinds, int nf) {
     for (int f = 0; f < nf; ++f)
         if (((kinds >> (2 * f)) & 3u) == 0u) return true;
@@ -539,11 +574,13 @@ struct ZP {
     static constexpr size_t smem() { return sizeof(T) * (size_t)NS * NF * SP; }
 };
 
-template <class T, int NF, unsigned KINDS, int TX, int TYH, int RY, int D, class Epi>
+template <class T, int NF, unsigned KINDS, int TX, int TYH, int RY, int D, class Epi, int MODE = 0>
 __global__ void __launch_bounds__(TX* TYH) k_zpass(Geo<T> g, SrcFields<T, NF> src, Epi epi, int chunk) {
     using Z = ZP<T, NF, TX, TYH, RY, D>;
     constexpr int RS = Z::RS, SP = Z::SP, NS = Z::NS, OFF = Z::OFF, CH = Z::CH, TY = Z::TY;
     constexpr int NT = TX * TYH;
+    constexpr int NO = MODE == 1 ? NF / 2 : NF;       // output fields (MODE 1: x then comp in)
+    static_assert(MODE != 1 || NF % 2 == 0, "MODE 1 reads field pairs");
     constexpr int NVEC = Z::NR * CH;                  // vector copies per field-plane
     constexpr int NHAL = 2 * TY;                      // scalar halo-column copies
     static_assert((NS & (NS - 1)) == 0, "ring stages must be a power of two");
@@ -654,28 +691,68 @@ __global__ void __launch_bounds__(TX* TYH) k_zpass(Geo<T> g, SrcFields<T, NF> sr
             for (int f = 0; f < NF; ++f) qp[f] = pp[f * SP + me];
             if (gj[u] < g.my) {
                 T cr = T(0);
-                if (any_kind0(KINDS, NF)) cr = radial_coef_fast(rr2[u] + zz2);
-                T val[NF];
-#pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    const T* a = pc + f * SP;
-                    const T v0 = q0[u][f];
-                    const T tx_ = (a[me + 1] - v0) * wpx - (v0 - a[me - 1]) * wmx;
-                    const T ty_ = (a[me + RS] - v0) * wpy[u] - (v0 - a[me - RS]) * wmy[u];
-                    const T tz_ = (qp[f] - v0) * wpz - (v0 - qm[u][f]) * wmz;
-                    const unsigned kind = (KINDS >> (2 * f)) & 3u;
-                    const T coef = kind == 0u ? cr : (kind == 1u ? T(0.125) : cbx);
-                    val[f] = v0 + coef * (tx_ + ty_ + tz_);
-                }
+                if (any_kind0(KINDS, NO)) cr = radial_coef_fast(rr2[u] + zz2);
                 const long col = (long)gi + (long)gj[u] * g.sy;
-                epi.store(g, col + (long)c * g.sz, val, cpre[u]);
-                if (c == 2 || c == mz - 3) {
-                    T hv[NF], zv[NF];
+                const bool wall = c == 2 || c == mz - 3;
+                const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
+                T val[NO];
+                if constexpr (MODE == 1) {
+                    // increment of the first filter pass on x - comp: differences of x and of
+                    // comp taken apart, then combined, so comp's bits are not rounded away
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) { hv[f] = T(0.5) * val[f]; zv[f] = T(0); }
-                    const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
-                    epi.store(g, col + (long)kh * g.sz, hv);
-                    epi.store(g, col + (long)kz * g.sz, zv);
+                    for (int f = 0; f < NO; ++f) {
+                        const T* a = pc + f * SP;
+                        const T* b = pc + (f + NO) * SP;
+                        const T x0 = q0[u][f], k0 = q0[u][f + NO];
+                        const T txp = (a[me + 1] - x0) - (b[me + 1] - k0), txm = (x0 - a[me - 1]) - (k0 - b[me - 1]);
+                        const T typ = (a[me + RS] - x0) - (b[me + RS] - k0), tym = (x0 - a[me - RS]) - (k0 - b[me - RS]);
+                        const T tzp = (qp[f] - x0) - (qp[f + NO] - k0), tzm = (x0 - qm[u][f]) - (k0 - qm[u][f + NO]);
+                        const unsigned kind = (KINDS >> (2 * f)) & 3u;
+                        const T coef = kind == 0u ? cr : (kind == 1u ? T(0.125) : cbx);
+                        val[f] = coef * (txp * wpx - txm * wmx + typ * wpy[u] - tym * wmy[u] + tzp * wpz - tzm * wmz);
+                    }
+                    epi.store(g, col + (long)c * g.sz, val, cpre[u]);
+                    if (wall) {
+                        // wall rows of the pass result: row kh = half of row c, row kz = 0, as
+                        // increments of x - comp
+                        T hv[NO], zv[NO];
+#pragma unroll
+                        for (int f = 0; f < NO; ++f) {
+                            const T xw = c == 2 ? qm[u][f] : qp[f];
+                            const T kw = c == 2 ? qm[u][f + NO] : qp[f + NO];
+                            hv[f] = ((T(0.5) * q0[u][f] - xw) - (T(0.5) * q0[u][f + NO] - kw)) + T(0.5) * val[f];
+                            const long iz = col + (long)kz * g.sz;
+                            zv[f] = src.f[f + NO][iz] - src.f[f][iz];
+                        }
+                        epi.store(g, col + (long)kh * g.sz, hv);
+                        epi.store(g, col + (long)kz * g.sz, zv);
+                    }
+                } else {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) {
+                        const T* a = pc + f * SP;
+                        const T v0 = q0[u][f];
+                        const T tx_ = (a[me + 1] - v0) * wpx - (v0 - a[me - 1]) * wmx;
+                        const T ty_ = (a[me + RS] - v0) * wpy[u] - (v0 - a[me - RS]) * wmy[u];
+                        const T tz_ = (qp[f] - v0) * wpz - (v0 - qm[u][f]) * wmz;
+                        const unsigned kind = (KINDS >> (2 * f)) & 3u;
+                        const T coef = kind == 0u ? cr : (kind == 1u ? T(0.125) : cbx);
+                        // MODE 2: increment of two passes from the first pass's increment d,
+                        // S(S(z)) - z = 2 d + coef L(d)
+                        val[f] = (MODE == 2 ? T(2) * v0 : v0) + coef * (tx_ + ty_ + tz_);
+                    }
+                    if constexpr (MODE == 2) {
+                        epi.store_rows(col + (long)c * g.sz, wall, col + (long)kh * g.sz, col + (long)kz * g.sz, val, cpre[u]);
+                    } else {
+                        epi.store(g, col + (long)c * g.sz, val, cpre[u]);
+                        if (wall) {
+                            T hv[NF], zv[NF];
+#pragma unroll
+                            for (int f = 0; f < NF; ++f) { hv[f] = T(0.5) * val[f]; zv[f] = T(0); }
+                            epi.store(g, col + (long)kh * g.sz, hv);
+                            epi.store(g, col + (long)kz * g.sz, zv);
+                        }
+                    }
                 }
             }
 #pragma unroll
