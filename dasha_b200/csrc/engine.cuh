@@ -4,6 +4,7 @@
 #include "dasha_capi.h"
 #include "mhd_kernels.cuh"
 #include "zm_kernels.cuh"
+#include "zpv.cuh"
 #include "adjoint.cuh"
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -367,14 +368,6 @@ public:
     }
 
     // ---- the RHS chain (right, t3dsdsc.f:1297-1673) ----
-    template <int NFLD>
-    void smooth(T* const* in, T* const* out, T* const* acc, unsigned kinds) {
-        FS<T, NFLD> a{}, b{}, c{};
-        for (int q = 0; q < NFLD; ++q) { a.f[q] = in[q]; b.f[q] = out[q]; c.f[q] = acc ? acc[q] : out[q]; }
-        const char* tg = NFLD == 8 ? "k_smooth8" : (acc ? "k_smooth3_acc" : "k_smooth3");
-        DASHA_LAUNCH(tg, (double)N * sizeof(T) * (2 * NFLD + (acc ? NFLD : 0)),
-                     k_smooth<T, NFLD><<<grd, blk, 0, st>>>(g, a, b, c, kinds, acc ? 1 : 0));
-    }
     static F8<T> f8(T* const* p) { F8<T> r; for (int m = 0; m < 8; ++m) r.f[m] = p[m]; return r; }
     static F3<T> f3(T* const* p) { F3<T> r; for (int m = 0; m < 3; ++m) r.f[m] = p[m]; return r; }
 
@@ -385,41 +378,56 @@ public:
         nch = std::max(1, std::min(nch, mz / minlen));
         return (mz + nch - 1) / nch;
     }
-    // k_zpass tiling: 32 x 16 columns per CTA (256 threads, 2 rows each), 4 planes in flight
-    static constexpr int ZTX = 32, ZTYH = 8, ZD = 4;
-    // rows per thread: 2 for the 4-field FP32 passes, 1 otherwise (smaller ring, more CTAs/SM)
+    // radius-2 ring kernels (k_zst2): 32 x 8 columns per CTA
+    static constexpr int ZTX = 32;
+    // k_zpv tiling: a warp covers 32*ZVX x nodes (float pairs in FP32), a thread RY
+    // consecutive rows, TYH warps per CTA, D planes in flight.  Measured best on the
+    // 1024x512x1024 FP32 and 512x256x512 FP64 steps: FP32 64x8 tiles of 256 threads (one row
+    // each, 3 planes ahead); FP64 32x8 tiles of 128 threads (two rows each, 2 planes ahead).
+    static constexpr int ZVX = sizeof(T) == 4 ? 2 : 1;
     template <int NF>
-    static constexpr int zry() { return (sizeof(T) == 4 && NF == 4) ? 2 : 1; }
+    struct ZC {
+        static constexpr int TYH = sizeof(T) == 4 ? 8 : 4;
+        static constexpr int RY = sizeof(T) == 4 ? 1 : 2;
+        static constexpr int D = sizeof(T) == 4 ? 3 : 2;
+    };
     template <int NF>
-    using ZPc = ZP<T, NF, ZTX, ZTYH, zry<NF>(), ZD>;
+    using ZVc = ZV<T, NF, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D>;
+    template <int NF, unsigned KINDS, class Epi, int MODE>
+    static constexpr auto zpv_fn() { return k_zpv<T, NF, KINDS, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D, Epi, MODE>; }
     // one smoothing pass of NF fields: src -> epi
     template <int NF, unsigned KINDS, int MODE = 0, class Epi>
     void zp(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
-        dim3 gg(mx / ZTX, (my + ZPc<NF>::TY - 1) / ZPc<NF>::TY, 1);
+        using Z = ZVc<NF>;
+        dim3 gg((mx + Z::TX - 1) / Z::TX, (my + Z::TY - 1) / Z::TY, 1);
         int ch = zchunk(gg.x * gg.y, 16);
         gg.z = (mz + ch - 1) / ch;
-        DASHA_LAUNCH(tag, bytes, (k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi, MODE>
-                                  <<<gg, ZTX * ZTYH, ZPc<NF>::smem(), st>>>(g, src, epi, ch)));
+        DASHA_LAUNCH(tag, bytes, (zpv_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem(), st>>>(g, src, epi, ch)));
     }
     template <int NF, unsigned KINDS, class Epi, int MODE = 0>
     static cudaError_t zp_attr1() {
-        return cudaFuncSetAttribute(k_zpass<T, NF, KINDS, ZTX, ZTYH, zry<NF>(), ZD, Epi, MODE>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZPc<NF>::smem());
+        return cudaFuncSetAttribute(zpv_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ZVc<NF>::smem());
     }
+    using St3 = VStore<T, 3, ZVX>;
+    using St4 = VStore<T, 4, ZVX>;
+    using Acc3 = VAcc<T, 3, ZVX>;
+    using RK4 = VRK<T, 4, ZVX, KAHAN>;
     cudaError_t zs_attr() {
         cudaError_t e;
-        if ((e = zp_attr1<3, 0u, EpiStore<T, 3>>())) return e;
-        if ((e = zp_attr1<3, KIND_H, EpiStore<T, 3>>())) return e;
-        if ((e = zp_attr1<3, KIND_H, EpiAcc<T, 3>>())) return e;
-        if ((e = zp_attr1<4, 0u, EpiStore<T, 4>>())) return e;
-        if ((e = zp_attr1<4, KIND_B4, EpiStore<T, 4>>())) return e;
-        if ((e = zp_attr1<4, 0u, EpiRK<T, 4, KAHAN>>())) return e;
-        if ((e = zp_attr1<4, KIND_B4, EpiRK<T, 4, KAHAN>>())) return e;
+        if ((e = zp_attr1<3, 0u, St3>())) return e;
+        if ((e = zp_attr1<3, KIND_H, St3>())) return e;
+        if ((e = zp_attr1<3, KIND_H, Acc3>())) return e;
+        if ((e = zp_attr1<4, 0u, St4>())) return e;
+        if ((e = zp_attr1<4, KIND_B4, St4>())) return e;
+        if ((e = zp_attr1<4, 0u, RK4>())) return e;
+        if ((e = zp_attr1<4, KIND_B4, RK4>())) return e;
         if constexpr (KAHAN) {
-            if ((e = zp_attr1<8, 0u, EpiStore<T, 4>, 1>())) return e;
-            if ((e = zp_attr1<8, KIND_B4, EpiStore<T, 4>, 1>())) return e;
-            if ((e = zp_attr1<4, 0u, EpiKF<T, 4>, 2>())) return e;
-            if ((e = zp_attr1<4, KIND_B4, EpiKF<T, 4>, 2>())) return e;
+            if ((e = zp_attr1<4, 0u, VStore<T, 2, ZVX>, 1>())) return e;
+            if ((e = zp_attr1<4, KIND_P45, VStore<T, 2, ZVX>, 1>())) return e;
+            if ((e = zp_attr1<4, KIND_P67, VStore<T, 2, ZVX>, 1>())) return e;
+            if ((e = zp_attr1<4, 0u, VKF<T, 4, ZVX>, 2>())) return e;
+            if ((e = zp_attr1<4, KIND_B4, VKF<T, 4, ZVX>, 2>())) return e;
         }
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
@@ -427,20 +435,18 @@ public:
         if ((e = cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, 1>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 3, ZTX, 8>::smem(false))))
             return e;
-        if ((e = cudaFuncSetAttribute(k_zst2<T, 1, ZTX, 8, 2, OpHall<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)ZS2<T, 1, ZTX, 8>::smem(false))))
-            return e;
         return cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, -1>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ZS2<T, 3, ZTX, 8>::smem(false));
     }
     static constexpr int HMINB = sizeof(T) == 4 ? 2 : 1;   // CTAs per SM asked of the register allocator
     static SrcFields<T, 3> src3(T* const* p) { SrcFields<T, 3> s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
     static SrcFields<T, 8> src8(T* const* p) { SrcFields<T, 8> s; for (int q = 0; q < 8; ++q) s.f[q] = p[q]; return s; }
-    static EpiStore<T, 3> st3(T* const* p) { EpiStore<T, 3> s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
-    static EpiStore<T, 8> st8(T* const* p) { EpiStore<T, 8> s; for (int q = 0; q < 8; ++q) s.f[q] = p[q]; return s; }
+    static St3 st3(T* const* p) { St3 s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
     static constexpr unsigned KIND_H = 1u | (1u << 2) | (1u << 4);                 // 1/8 for 3 fields
     static constexpr unsigned KIND_X = (2u << 8) | (2u << 10) | (2u << 12);         // B with the x profile
     static constexpr unsigned KIND_B4 = 2u | (2u << 2) | (2u << 4);                 // fields 4..7: B1 B2 B3 p
+    static constexpr unsigned KIND_P45 = 2u | (2u << 2);                            // field pair (B1, B2)
+    static constexpr unsigned KIND_P67 = 2u;                                        // field pair (B3, p)
 
     // one avrg/avrgtt pass over the 8 state-like fields, as two 4-field launches (rho, m) and
     // (B, p); mk(lo) builds the epilogue of fields lo..lo+3
@@ -451,20 +457,23 @@ public:
         zp<4, 0u>(tag, 0.5 * bytes_per_cell * N * sizeof(T), a, mk(0));
         zp<4, KIND_B4>(tag, 0.5 * bytes_per_cell * N * sizeof(T), b, mk(4));
     }
-    static EpiStore<T, 4> st4(T* const* p, int lo) { EpiStore<T, 4> s; for (int q = 0; q < 4; ++q) s.f[q] = p[lo + q]; return s; }
+    static St4 st4(T* const* p, int lo) { St4 s; for (int q = 0; q < 4; ++q) s.f[q] = p[lo + q]; return s; }
 
     // avrgtt on the compensated FP32 state (X, C): pass 1 writes its increment of X - C into
     // t, pass 2 adds the two-pass increment to (X, C) in place with a Kahan step
     void filter_compensated(T* const* t) {
-        for (int lo = 0; lo < 8; lo += 4) {
-            SrcFields<T, 8> a;
-            for (int q = 0; q < 4; ++q) { a.f[q] = X[lo + q]; a.f[4 + q] = C[lo + q]; }
-            if (lo == 0) zp<8, 0u, 1>("k_zpass_F1", 12.0 * N * sizeof(T), a, st4(t, lo));
-            else zp<8, KIND_B4, 1>("k_zpass_F1", 12.0 * N * sizeof(T), a, st4(t, lo));
+        for (int lo = 0; lo < 8; lo += 2) {   // pass 1 by field pairs: ring (x_a, x_b, comp_a, comp_b)
+            SrcFields<T, 4> a;
+            VStore<T, 2, ZVX> o;
+            for (int q = 0; q < 2; ++q) { a.f[q] = X[lo + q]; a.f[2 + q] = C[lo + q]; o.f[q] = t[lo + q]; }
+            const double by = 6.0 * N * sizeof(T);
+            if (lo < 4) zp<4, 0u, 1>("k_zpass_F1", by, a, o);
+            else if (lo == 4) zp<4, KIND_P45, 1>("k_zpass_F1", by, a, o);
+            else zp<4, KIND_P67, 1>("k_zpass_F1", by, a, o);
         }
         for (int lo = 0; lo < 8; lo += 4) {
             SrcFields<T, 4> d;
-            EpiKF<T, 4> e;
+            VKF<T, 4, ZVX> e;
             for (int q = 0; q < 4; ++q) { d.f[q] = t[lo + q]; e.x[q] = X[lo + q]; e.comp[q] = C[lo + q]; }
             if (lo == 0) zp<4, 0u, 2>("k_zpass_F2", 20.0 * N * sizeof(T), d, e);
             else zp<4, KIND_B4, 2>("k_zpass_F2", 20.0 * N * sizeof(T), d, e);
@@ -512,7 +521,7 @@ public:
             // plain kernel: faster here than the ring framework (one stencil field, seven pointwise)
             DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(Hh[0])));
             T** h = passes3<KIND_H>("k_zpass_H", Hh[0], Hh[1], 4);
-            EpiAcc<T, 3> ea;
+            Acc3 ea;
             for (int q = 0; q < 3; ++q) { ea.f[q] = Ef[q]; ea.a[q] = Ef[q]; }
             zp<3, KIND_H>("k_zpass_H5acc", 9.0 * N * sizeof(T), src3(h), ea);   // 5th pass added into E
         }
@@ -561,7 +570,7 @@ public:
             tmp8(t);
             pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
             auto mkrk = [&](int lo) {
-                EpiRK<T, 4, KAHAN> er;
+                RK4 er;
                 for (int m = 0; m < 4; ++m) {
                     er.x[m] = S[lo + m]; er.base[m] = X[lo + m]; er.acc[m] = A[lo + m];
                     er.comp[m] = KAHAN ? C[lo + m] : nullptr;
@@ -703,7 +712,7 @@ public:
             pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
             T* const* xo = outs[stage - 1];
             auto mkrk = [&](int lo) {
-                EpiRK<T, 4, KAHAN> er;
+                RK4 er;
                 for (int m = 0; m < 4; ++m) { er.x[m] = xo[lo + m]; er.base[m] = Xb[lo + m]; er.acc[m] = Acc[lo + m]; er.comp[m] = nullptr; }
                 er.stage = stage;
                 er.dt = dt;

@@ -125,35 +125,9 @@ __global__ void k_curl(Geo<T> g, F3<T> b, F3<T> j) {
 }
 
 // ---------------------------------------------------------------------------------------
-// One smoothing pass over NFLD fields with the wall rows re-applied (avrg/avrgE/avrgc/avrgh
-// + bndry*).  kind per field: 0 radial coefficient cr, 1 constant 1/8, 2 x-profile cbx.
-// If acc is given: out = acc + smoothed (the Hall term added into E, t3dsdsc.f:1426-1432).
+// NFLD field pointers (the transposed smoothing passes of the adjoint)
 template <class T, int NFLD>
 struct FS { T* f[NFLD]; };
-
-template <class T, int NFLD>
-__global__ void k_smooth(Geo<T> g, FS<T, NFLD> in, FS<T, NFLD> out, FS<T, NFLD> acc, unsigned kinds,
-                         int use_acc) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.mx) return;
-    int jj = blockIdx.y, k = blockIdx.z;
-    bool zero, half;
-    int ks = wall_src(k, g.mz, zero, half);
-    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
-    Nbr<T> n(g, i, jj, ks);
-#pragma unroll
-    for (int q = 0; q < NFLD; ++q) {
-        T val = T(0);
-        if (!zero) {
-            unsigned kind = (kinds >> (2 * q)) & 3u;
-            T coef = kind == 0 ? g.cr[n.c] : (kind == 1 ? T(0.125) : g.cbx[i]);
-            val = in.f[q][n.c] + coef * n.difc3(g, in.f[q]);
-            if (half) val = T(0.5) * val;
-        }
-        if (use_acc) val = acc.f[q][c] + val;
-        out.f[q][c] = val;
-    }
-}
 
 // ---------------------------------------------------------------------------------------
 // E = -v x B + eta*J at every node (t3dsdsc.f:1367-1372).
@@ -201,141 +175,6 @@ __global__ void k_hall(Geo<T> g, F8<T> x, F3<T> cur, F3<T> h) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Right-hand side xdif on interior rows + wall rows (right t3dsdsc.f:1334-1566, bndry).
-template <class T>
-__device__ __forceinline__ void rhs_point(const Geo<T>& g, const F8<T>& x, const F3<T>& cur,
-                                          const F3<T>& e, int i, int jj, int k, T out[NF]) {
-    Nbr<T> n(g, i, jj, k);
-    const T* R = x.f[0];
-    const T* M1 = x.f[1];
-    const T* M2 = x.f[2];
-    const T* M3 = x.f[3];
-    const T* P = x.f[7];
-    const T r0 = T(g.rho0[k]);
-    // density at the x / y neighbours share the centre's row profile; z neighbours do not
-    auto rx = [&](long q) { return r0 + R[q]; };
-    auto rz = [&](long q, int kk) { return T(g.rho0[kk]) + R[q]; };
-    // continuity: -div(rho v)
-    T dxf = n.Dx(g, M1), dyg = n.Dy(g, M2), dzh = n.Dz(g, M3);
-    out[0] = -dxf - dyg - dzh;
-    // momentum fluxes m=2..4 (flux, t3dsdsc.f:2317-2347) evaluated at the stencil points
-    const long sz = g.sz;
-    long zi[5] = {n.c - 2 * sz, n.c - sz, n.c, n.c + sz, n.c + 2 * sz};
-    long xi[5] = {n.xm2, n.xm1, n.c, n.xp1, n.xp2};
-    long yi[5] = {n.ym2, n.ym1, n.c, n.yp1, n.yp2};
-    T fx[3][5], fy[3][5], fz[3][5];
-#pragma unroll
-    for (int s = 0; s < 5; ++s) {
-        long q = xi[s];
-        T r = rx(q), a = M1[q], dp = P[q];
-        fx[0][s] = a * a / r + dp;
-        fx[1][s] = a * M2[q] / r;
-        fx[2][s] = a * M3[q] / r;
-        q = yi[s];
-        r = rx(q);
-        T bq = M2[q];
-        fy[0][s] = M1[q] * bq / r;
-        fy[1][s] = bq * bq / r + P[q];
-        fy[2][s] = M3[q] * bq / r;
-        q = zi[s];
-        r = rz(q, k - 2 + s);
-        T cq = M3[q];
-        fz[0][s] = M1[q] * cq / r;
-        fz[1][s] = M2[q] * cq / r;
-        fz[2][s] = cq * cq / r + P[q];
-    }
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        T ddx = d1fc(fx[m][0], fx[m][1], fx[m][2], fx[m][3], fx[m][4], g.a1x[i], g.b1x[i], g.c1x[i], g.d1x[i]);
-        T ddy = d1fc(fy[m][0], fy[m][1], fy[m][2], fy[m][3], fy[m][4], g.a1y[jj], g.b1y[jj], g.c1y[jj], g.d1y[jj]);
-        T ddz = d1fc(fz[m][0], fz[m][1], fz[m][2], fz[m][3], fz[m][4], g.a1z[k], g.b1z[k], g.c1z[k], g.d1z[k]);
-        out[1 + m] = -ddx - ddy - ddz;
-    }
-    // J x B - xresd (t3dsdsc.f:1355-1360)
-    long c = n.c;
-    T rc = r0 + R[c];
-    T b1 = T(g.bx0[k]) + x.f[4][c], b2 = T(g.by0[k]) + x.f[5][c], b3 = T(g.bz0[k]) + x.f[6][c];
-    T j1 = cur.f[0][c], j2 = cur.f[1][c], j3 = cur.f[2][c];
-    out[1] = out[1] - T(g.rsx[k]) + j2 * b3 - j3 * b2;
-    out[2] = out[2] - T(g.rsy[k]) + j3 * b1 - j1 * b3;
-    out[3] = out[3] - T(g.rsz[k]) + j1 * b2 - j2 * b1;
-    // induction: dB/dt = -curl E (t3dsdsc.f:1438-1452)
-    out[4] = -n.Dy(g, e.f[2]) + n.Dz(g, e.f[1]);
-    out[5] = -n.Dz(g, e.f[0]) + n.Dx(g, e.f[2]);
-    out[6] = -n.Dx(g, e.f[1]) + n.Dy(g, e.f[0]);
-    // pressure (t3dsdsc.f:1550-1566): velocities at the stencil points
-    T vx[5], vy[5], vz[5];
-#pragma unroll
-    for (int s = 0; s < 5; ++s) {
-        vx[s] = M1[xi[s]] / rx(xi[s]);
-        vy[s] = M2[yi[s]] / rx(yi[s]);
-        vz[s] = M3[zi[s]] / rz(zi[s], k - 2 + s);
-    }
-    T v1 = M1[c] / rc, v2 = M2[c] / rc, v3 = M3[c] / rc;
-    T px = n.Dx(g, P), py = n.Dy(g, P), pz = n.Dz(g, P) + T(g.dzp0[k]);
-    T divv = -d1fc(vx[0], vx[1], vx[2], vx[3], vx[4], g.a1x[i], g.b1x[i], g.c1x[i], g.d1x[i])
-             - d1fc(vy[0], vy[1], vy[2], vy[3], vy[4], g.a1y[jj], g.b1y[jj], g.c1y[jj], g.d1y[jj])
-             - d1fc(vz[0], vz[1], vz[2], vz[3], vz[4], g.a1z[k], g.b1z[k], g.c1z[k], g.d1z[k]);
-    T pc = T(g.p0[k]) + P[c];
-    out[7] = -px * v1 - py * v2 - pz * v3 + divv * g.gamma * pc
-             + (g.gamma - T(1)) * g.eta * (j1 * j1 + j2 * j2 + j3 * j3);
-    if (g.viscos) {   // t3dsdsc.f:1612-1634, 5-point second derivatives of v
-        // v at the x/y stencil points of the other components
-        T ux[5], uy[5], uz[5];
-        T af, ag, ah;
-        // af = lap(vx)
-#pragma unroll
-        for (int s = 0; s < 5; ++s) { uy[s] = M1[yi[s]] / rx(yi[s]); uz[s] = M1[zi[s]] / rz(zi[s], k - 2 + s); }
-        af = d1fc(vx[0], vx[1], vx[2], vx[3], vx[4], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i])
-           + d1fc(uy[0], uy[1], uy[2], uy[3], uy[4], g.a2y[jj], g.b2y[jj], g.c2y[jj], g.d2y[jj])
-           + d1fc(uz[0], uz[1], uz[2], uz[3], uz[4], g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
-#pragma unroll
-        for (int s = 0; s < 5; ++s) { ux[s] = M2[xi[s]] / rx(xi[s]); uz[s] = M2[zi[s]] / rz(zi[s], k - 2 + s); }
-        ag = d1fc(ux[0], ux[1], ux[2], ux[3], ux[4], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i])
-           + d1fc(vy[0], vy[1], vy[2], vy[3], vy[4], g.a2y[jj], g.b2y[jj], g.c2y[jj], g.d2y[jj])
-           + d1fc(uz[0], uz[1], uz[2], uz[3], uz[4], g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
-#pragma unroll
-        for (int s = 0; s < 5; ++s) { ux[s] = M3[xi[s]] / rx(xi[s]); uy[s] = M3[yi[s]] / rx(yi[s]); }
-        ah = d1fc(ux[0], ux[1], ux[2], ux[3], ux[4], g.a2x[i], g.b2x[i], g.c2x[i], g.d2x[i])
-           + d1fc(uy[0], uy[1], uy[2], uy[3], uy[4], g.a2y[jj], g.b2y[jj], g.c2y[jj], g.d2y[jj])
-           + d1fc(vz[0], vz[1], vz[2], vz[3], vz[4], g.a2z[k], g.b2z[k], g.c2z[k], g.d2z[k]);
-        out[1] = out[1] + g.mu * af;
-        out[2] = out[2] + g.mu * ag;
-        out[3] = out[3] + g.mu * ah;
-        out[7] = out[7] + g.mu * (v1 * af + v2 * ag + v3 * ah);
-    }
-    if (g.diffu) {    // t3dsdsc.f:1642-1661
-        T lr = n.D2x(g, R) + n.D2y(g, R) + (n.D2z(g, R) + T(g.d2rho0[k]));
-        T lp = n.D2x(g, P) + n.D2y(g, P) + (n.D2z(g, P) + T(g.d2p0[k]));
-        out[0] = out[0] + g.drho * lr;
-        out[7] = out[7] + g.dp * lp;
-    }
-}
-
-template <class T>
-__global__ void k_rhs(Geo<T> g, F8<T> x, F3<T> cur, F3<T> e, F8<T> xdif) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.mx) return;
-    int jj = blockIdx.y, k = blockIdx.z;
-    bool zero, half;
-    int ks = wall_src(k, g.mz, zero, half);
-    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
-    T out[NF];
-    if (zero) {
-#pragma unroll
-        for (int m = 0; m < NF; ++m) out[m] = T(0);
-    } else {
-        rhs_point(g, x, cur, e, i, jj, ks, out);
-        if (half) {
-#pragma unroll
-            for (int m = 0; m < NF; ++m) out[m] = T(0.5) * out[m];
-        }
-    }
-#pragma unroll
-    for (int m = 0; m < NF; ++m) xdif.f[m][c] = out[m];
-}
-
-// ---------------------------------------------------------------------------------------
 // J0 added to the smoothed J1 (j0_mode FULL).
 template <class T>
 __global__ void k_add_j0(Geo<T> g, F3<T> cur) {
@@ -346,43 +185,6 @@ __global__ void k_add_j0(Geo<T> g, F3<T> cur) {
     cur.f[0][c] += T(g.j0x[k]);
     cur.f[1][c] += T(g.j0y[k]);
     cur.f[2][c] += T(g.j0z[k]);
-}
-
-// ---------------------------------------------------------------------------------------
-// RK4 stage updates (stepon t3dsdsc.f:1090-1132).
-//  Plain form (FP64, the reference's registers xfold=base, xm=acc, x):
-//   s1: acc = base + k*dt/6, x = base + k*dt/2;   s2: acc += k*dt/3, x = base + k*dt/2
-//   s3: acc += k*dt/3,   x = base + k*dt;         s4: x = acc + k*dt/6
-//  Compensated form (FP32): acc holds the increment only and the base update of stage 4
-//   is a Kahan sum with the per-node compensation comp.
-template <class T, bool KAHAN>
-__global__ void k_rk(long n, int stage, double dt, F8<T> x, F8<T> base, F8<T> acc, F8<T> comp, F8<T> k) {
-    long c = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    const T tdt = T(dt);
-#pragma unroll
-    for (int m = 0; m < NF; ++m) {
-        T kv = k.f[m][c];
-        if (!KAHAN) {
-            T b = base.f[m][c];
-            if (stage == 1) { acc.f[m][c] = b + kv * tdt / T(6.); x.f[m][c] = b + kv * tdt / T(2.); }
-            else if (stage == 2) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt / T(2.); }
-            else if (stage == 3) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt; }
-            else { x.f[m][c] = acc.f[m][c] + kv * tdt / T(6.); }
-        } else {
-            T b = base.f[m][c];
-            if (stage == 1) { acc.f[m][c] = kv * tdt / T(6.); x.f[m][c] = b + kv * tdt / T(2.); }
-            else if (stage == 2) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt / T(2.); }
-            else if (stage == 3) { acc.f[m][c] = acc.f[m][c] + kv * tdt / T(3.); x.f[m][c] = b + kv * tdt; }
-            else {
-                T inc = acc.f[m][c] + kv * tdt / T(6.);
-                T y = inc - comp.f[m][c];
-                T t = b + y;
-                comp.f[m][c] = (t - b) - y;
-                x.f[m][c] = t;
-            }
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -401,64 +203,6 @@ __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
-}
-
-// CFL time step (setdt t3dsdsc.f:4709-4736) over the reference's region: k 0..mz-3,
-// j 0..my-2, i 0..mx-3 (t3dsdsc.f:4709-4711).  One block per (j,k) row pair chunk; writes
-// one partial minimum per block.
-template <class T>
-__global__ void k_cfl(Geo<T> g, F8<T> x, const double* xc, const double* yc, const double* zc,
-                      const double* dxs, const double* dys, const double* dzs, double cfl, double visc,
-                      double rcr, double gamma, double whistler, double* partial) {
-    int jj = blockIdx.y, k = blockIdx.z;
-    double best = 100.;
-    if (k <= g.mz - 3 && jj <= g.my - 2) {
-        const double r0 = g.rho0[k], bx0 = g.bx0[k], by0 = g.by0[k], bz0 = g.bz0[k], p0 = g.p0[k];
-        for (int i = threadIdx.x; i <= g.mx - 3; i += blockDim.x) {
-            double rr = sqrt(xc[i] * xc[i] + yc[jj] * yc[jj] + zc[k] * zc[k]);
-            if (!(rr >= rcr)) continue;
-            long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
-            double rho = r0 + (double)x.f[0][c];
-            double vx = (double)x.f[1][c] / rho, vy = (double)x.f[2][c] / rho, vz = (double)x.f[3][c] / rho;
-            double b1 = bx0 + (double)x.f[4][c], b2 = by0 + (double)x.f[5][c], b3 = bz0 + (double)x.f[6][c];
-            double va2 = (b1 * b1 + b2 * b2 + b3 * b3) / rho;
-            double cs2 = gamma * (p0 + (double)x.f[7][c]) / rho;
-            double vf = sqrt(fabs(va2 + cs2));
-            double dx = dxs[i], dy = dys[jj], dz = dzs[k];
-            double vpx = fabs(vx) + vf, vpy = fabs(vy) + vf, vpz = fabs(vz) + vf;
-            if (whistler != 0.0) {   // di*pi*|B|/rho per unit length (dt_whistler option)
-                double w = whistler * sqrt(b1 * b1 + b2 * b2 + b3 * b3) / rho;
-                vpx += w / fabs(dx); vpy += w / fabs(dy); vpz += w / fabs(dz);
-            }
-            double dtx = fabs(dx) / (vpx / cfl + visc / dx / 2.);
-            double dty = fabs(dy) / (vpy / cfl + visc / dy / 2.);
-            double dtz = fabs(dz) / (vpz / cfl + visc / dz / 2.);
-            double d = fmin(fmin(dtx, dty), dtz);
-            // NaN must win so that a corrupted state is detected
-            if (d != d) best = d; else if (best == best) best = fmin(best, d);
-        }
-    }
-    __shared__ double sh[32];
-    // NaN-propagating warp min
-    double v = best;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        double w = __shfl_down_sync(0xffffffffu, v, o);
-        v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
-    }
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = v;
-    __syncthreads();
-    if (wid == 0) {
-        int nw = (blockDim.x + 31) >> 5;
-        v = lane < nw ? sh[lane] : 100.;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            double w = __shfl_down_sync(0xffffffffu, v, o);
-            v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
-        }
-        if (lane == 0) partial[(long)blockIdx.z * gridDim.y + blockIdx.y] = v;
-    }
 }
 
 // CFL in rate form: the reference's per-direction step h / (vp/cfl + visc/(2h)) is the
@@ -535,33 +279,6 @@ static __global__ void k_reduce_rate(const double* partial, long n, double* out)
     }
 }
 
-// final reduction of partials by one block, fixed order
-static __global__ void k_reduce_min(const double* partial, long n, double* out) {
-    double v = 100.;
-    for (long q = threadIdx.x; q < n; q += blockDim.x) {
-        double w = partial[q];
-        v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
-    }
-    __shared__ double sh[32];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        double w = __shfl_down_sync(0xffffffffu, v, o);
-        v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
-    }
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = v;
-    __syncthreads();
-    if (wid == 0) {
-        int nw = (blockDim.x + 31) >> 5;
-        v = lane < nw ? sh[lane] : 100.;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            double w = __shfl_down_sync(0xffffffffu, v, o);
-            v = (w != w || v != v) ? (v != v ? v : w) : fmin(v, w);
-        }
-        if (lane == 0) *out = v;
-    }
-}
 
 // Diagnostics partial sums per (j,k) row: mass, energy (trapezoid weights), and the
 // per-row extrema of J on the mid-y plane; partial layout [row][5]: mass, energy, jmax/jmin

@@ -132,18 +132,25 @@ def test_diagnostics_parity(cfg):
     np.testing.assert_allclose(d.diagnostics(), o.diagnostics(), rtol=1e-11, atol=1e-13)
 
 
-def test_fp32_path_close_to_fp64():
-    cfg = harris.CONFIGS["c0"]
+SMALL_SW = harris.RunConfig("small-32x16x40-sinh-whistler", 32, 16, 40, True, 0.003, 1.0, 4, dt_whistler=1)
+
+
+@pytest.mark.parametrize("cfg,steps", [(harris.CONFIGS["c0"], 200), (SMALL_SW, 300)],
+                         ids=["c0-200", "sinh-whistler-300"])
+def test_fp32_path_close_to_fp64(cfg, steps):
+    """FP32 perturbation + Kahan RK4 + compensated filter against the FP64 path on the same dt
+    sequence: every field within 1e-6 relative L2 (measured: <= 1.4e-7).  The di = 1 stretched
+    case is the one where an uncompensated FP32 filter let the small By field drift by 1e-4."""
     d64 = capi.gem_context(cfg, 0)
     d32 = capi.gem_context(cfg, 1)
-    _, dts = d64.run(20)
+    _, dts = d64.run(steps)
     t = 0.0
     for n, dt in enumerate(dts):
         d32.stepon(t, dt, n)
         t += dt
     a, b = d32.get_state(), d64.get_state()
     rel_l2 = np.linalg.norm((a - b).reshape(8, -1), axis=1) / np.linalg.norm(b.reshape(8, -1), axis=1)
-    assert rel_l2.max() < 1e-5, rel_l2
+    assert rel_l2.max() < 1e-6, rel_l2
 
 
 def test_restart_through_host_state():
