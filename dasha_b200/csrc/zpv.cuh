@@ -9,8 +9,11 @@
 // reads from shared memory only plane c+1 of its nodes, the x neighbours at the ends of its
 // pair and the y neighbours above and below its strip: about 2 shared loads per node and field
 // instead of 5.  Only planes c and c+1 are read in a plane step, so the stage refilled at step c
-// (plane c+1+D) is neither of the two planes still read by threads in step c-1: one barrier per
-// plane suffices.
+// (plane c+1+D, the stage of plane c-2) is neither of the two planes still read by threads in
+// step c-1: one barrier per plane suffices; the first step also reads plane c-1 and so ends with
+// a second barrier.  (Loading the planes by TMA instead, as ring-plane boxes with one mbarrier
+// per stage, measured 7-40 % slower per pass on B200 in every arrangement tried: the passes are
+// issue-bound and cp.async's per-thread copies cost about 2 % of their instructions.)
 //
 // KINDS: 2 bits per output field, 0 radial coefficient, 1 constant 1/8, 2 x-profile cbx.
 // MODE 0 writes the smoothed fields through the epilogue.  MODES 1 and 2 are the two passes of
@@ -296,6 +299,8 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
                     IO::ld(pc + f * SP + base + u * RS, q0[u][f]);
                 }
             primed = true;
+            // plane c-1's stage is refilled at the next step: every thread must be done with it
+            __syncthreads();
         }
         T qp[RY][NF][VX], ylo[NF][VX], yhi[NF][VX];
 #pragma unroll
