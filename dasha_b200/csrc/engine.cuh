@@ -228,6 +228,7 @@ public:
         g.dzp0 = eqp + 5 * mz; g.d2rho0 = eqp + 6 * mz; g.d2p0 = eqp + 7 * mz;
         g.rsx = eqp + 8 * mz; g.rsy = eqp + 9 * mz; g.rsz = eqp + 10 * mz;
         g.j0x = eqp + 11 * mz; g.j0y = eqp + 12 * mz; g.j0z = eqp + 13 * mz;
+        g.dzp0r = eqp + 14 * mz;
         zcoord = H.coord[2];
         for (int q2 = 0; q2 < 8; ++q2) coefz[q2] = H.coef[2][q2];
 
@@ -296,6 +297,7 @@ public:
             }
             h[8 * mz + k] = rx; h[9 * mz + k] = ry; h[10 * mz + k] = rz;
             h[11 * mz + k] = jx[k]; h[12 * mz + k] = jy[k]; h[13 * mz + k] = jz[k];
+            h[14 * mz + k] = dzp0[k] / rho0h[k];
         }
         DASHA_CK(cudaMemcpyAsync((void*)g.rho0, h.data(), sizeof(double) * 16 * mz, cudaMemcpyHostToDevice, st));
         DASHA_CK(cudaStreamSynchronize(st));

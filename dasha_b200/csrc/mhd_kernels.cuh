@@ -35,6 +35,7 @@ struct Geo {
     const double *d2rho0, *d2p0;      // D2z rho0, D2z p0 (interior rows)
     const double *rsx, *rsy, *rsz;    // xresd profiles (interior rows)
     const double *j0x, *j0y, *j0z;    // J0 profiles for j0_mode FULL (null otherwise)
+    const double *dzp0r;              // Dz p0 / rho0 (interior rows)
     T eta, di, gamma, mu, drho, dp;
     int hall, viscos, diffu;
 };
@@ -140,9 +141,10 @@ __global__ void k_efield(Geo<T> g, F8<T> x, F3<T> cur, F3<T> e) {
     T r = T(g.rho0[k]) + x.f[0][c];
     T m1 = x.f[1][c], m2 = x.f[2][c], m3 = x.f[3][c];
     T b1 = T(g.bx0[k]) + x.f[4][c], b2 = T(g.by0[k]) + x.f[5][c], b3 = T(g.bz0[k]) + x.f[6][c];
-    e.f[0][c] = (-m2 * b3 + m3 * b2) / r + g.eta * cur.f[0][c];
-    e.f[1][c] = (-m3 * b1 + m1 * b3) / r + g.eta * cur.f[1][c];
-    e.f[2][c] = (-m1 * b2 + m2 * b1) / r + g.eta * cur.f[2][c];
+    const T ri = T(1) / r;
+    e.f[0][c] = (-m2 * b3 + m3 * b2) * ri + g.eta * cur.f[0][c];
+    e.f[1][c] = (-m3 * b1 + m1 * b3) * ri + g.eta * cur.f[1][c];
+    e.f[2][c] = (-m1 * b2 + m2 * b1) * ri + g.eta * cur.f[2][c];
 }
 
 // ---------------------------------------------------------------------------------------
@@ -167,9 +169,10 @@ __global__ void k_hall(Geo<T> g, F8<T> x, F3<T> cur, F3<T> h) {
     // x and y) and is left out; the rest is di dp0/dz (rho - rho0) / (rho0 rho).  This keeps
     // an O(1) field out of the FP32 sum that drives dB/dt.
     T px = n.Dx(g, p), py = n.Dy(g, p), pz = n.Dz(g, p);
-    T h1 = g.di * (j2 * b3 - j3 * b2 - px) / r;
-    T h2 = g.di * (j3 * b1 - j1 * b3 - py) / r;
-    T h3 = g.di * (j1 * b2 - j2 * b1 - pz + T(g.dzp0[ks]) * x.f[0][q] / T(g.rho0[ks])) / r;
+    const T dir = g.di / r;
+    T h1 = (j2 * b3 - j3 * b2 - px) * dir;
+    T h2 = (j3 * b1 - j1 * b3 - py) * dir;
+    T h3 = (j1 * b2 - j2 * b1 - pz + T(g.dzp0r[ks]) * x.f[0][q]) * dir;
     if (half) { h1 = T(0.5) * h1; h2 = T(0.5) * h2; h3 = T(0.5) * h3; }
     h.f[0][c] = h1; h.f[1][c] = h2; h.f[2][c] = h3;
 }
