@@ -185,7 +185,7 @@ class Dasha:
         self._check(self.lib.dasha_diagnostics(self.h, _dp(out)))
         return out
 
-    def adjoint_flux_grad(self, dt_seq, snaps: int = 10):
+    def adjoint_flux_grad(self, dt_seq, snaps: int = 0):
         dt_seq = np.ascontiguousarray(dt_seq, np.float64)
         deta = np.zeros(1)
         dpsi = np.zeros((self.mz, self.mx))

@@ -270,7 +270,7 @@ int dasha_diagnostics(dasha_ctx* c, double* out) {
 int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int snaps, double* dPhi_deta,
                             double* dPhi_dpsi) {
     CAPI_GUARD(c);
-    if (nsteps < 0 || (nsteps > 0 && !dt_seq) || snaps < 1 || !dPhi_deta || !dPhi_dpsi)
+    if (nsteps < 0 || (nsteps > 0 && !dt_seq) || snaps < 0 || !dPhi_deta || !dPhi_dpsi)
         return fail(c, DASHA_E_INVALID, "bad adjoint arguments");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     if (c->P.precision != 0) return fail(c, DASHA_E_UNSUPPORTED, "the adjoint runs on FP64 contexts only");

@@ -469,16 +469,16 @@ public:
             VStore<T, 2, ZVX> o;
             for (int q = 0; q < 2; ++q) { a.f[q] = X[lo + q]; a.f[2 + q] = C[lo + q]; o.f[q] = t[lo + q]; }
             const double by = 6.0 * N * sizeof(T);
-            if (lo < 4) zp<4, 0u, 1>("k_zpass_F1", by, a, o);
-            else if (lo == 4) zp<4, KIND_P45, 1>("k_zpass_F1", by, a, o);
-            else zp<4, KIND_P67, 1>("k_zpass_F1", by, a, o);
+            if (lo < 4) zp<4, 0u, 1>("k_zpv_F1", by, a, o);
+            else if (lo == 4) zp<4, KIND_P45, 1>("k_zpv_F1", by, a, o);
+            else zp<4, KIND_P67, 1>("k_zpv_F1", by, a, o);
         }
         for (int lo = 0; lo < 8; lo += 4) {
             SrcFields<T, 4> d;
             VKF<T, 4, ZVX> e;
             for (int q = 0; q < 4; ++q) { d.f[q] = t[lo + q]; e.x[q] = X[lo + q]; e.comp[q] = C[lo + q]; }
-            if (lo == 0) zp<4, 0u, 2>("k_zpass_F2", 20.0 * N * sizeof(T), d, e);
-            else zp<4, KIND_B4, 2>("k_zpass_F2", 20.0 * N * sizeof(T), d, e);
+            if (lo == 0) zp<4, 0u, 2>("k_zpv_F2", 20.0 * N * sizeof(T), d, e);
+            else zp<4, KIND_B4, 2>("k_zpv_F2", 20.0 * N * sizeof(T), d, e);
         }
     }
 
@@ -507,7 +507,7 @@ public:
         for (int q = 0; q < 3; ++q) oc.out[q] = cur[0][q];
         DASHA_LAUNCH("k_curl", 6.0 * N * sizeof(T),
                      (k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, 1>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(bb), oc, ch)));
-        curF = passes3<0u>("k_zpass_J", cur[0], cur[1], 4);
+        curF = passes3<0u>("k_zpv_J", cur[0], cur[1], 4);
         if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(curF)));
     }
 
@@ -518,14 +518,14 @@ public:
         (void)cother;
         // E0 = -v x B + eta J at every node, then avrgE's 4 passes (t3dsdsc.f:1367-1389)
         DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
-        Ef = passes3<0u>("k_zpass_E", E[0], E[1], 4);
+        Ef = passes3<0u>("k_zpv_E", E[0], E[1], 4);
         if (P.hall) {
             // plain kernel: faster here than the ring framework (one stencil field, seven pointwise)
             DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(Hh[0])));
-            T** h = passes3<KIND_H>("k_zpass_H", Hh[0], Hh[1], 4);
+            T** h = passes3<KIND_H>("k_zpv_H", Hh[0], Hh[1], 4);
             Acc3 ea;
             for (int q = 0; q < 3; ++q) { ea.f[q] = Ef[q]; ea.a[q] = Ef[q]; }
-            zp<3, KIND_H>("k_zpass_H5acc", 9.0 * N * sizeof(T), src3(h), ea);   // 5th pass added into E
+            zp<3, KIND_H>("k_zpv_H5acc", 9.0 * N * sizeof(T), src3(h), ea);   // 5th pass added into E
         }
         // right-hand side: hydro part (xdif 0..3, 7) and induction (xdif 4..6)
         dim3 gg(mx / ZTX, (my + 7) / 8, 1);
@@ -555,8 +555,8 @@ public:
         if (smooth_xdif) {
             T* t[8];
             tmp8(t);
-            pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
-            pass8("k_zpass_X", 16.0, t, [&](int lo) { return st4(out, lo); });
+            pass8("k_zpv_X", 16.0, K, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpv_X", 16.0, t, [&](int lo) { return st4(out, lo); });
         } else {
             for (int m = 0; m < 8; ++m) out[m] = K[m];
         }
@@ -570,7 +570,7 @@ public:
             launch_rhs_raw(stage == 1 ? X : S);
             T* t[8];
             tmp8(t);
-            pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpv_X", 16.0, K, [&](int lo) { return st4(t, lo); });
             auto mkrk = [&](int lo) {
                 RK4 er;
                 for (int m = 0; m < 4; ++m) {
@@ -581,7 +581,7 @@ public:
                 er.dt = dt;
                 return er;
             };
-            static const char* names[4] = {"k_zpass_X_rk1", "k_zpass_X_rk2", "k_zpass_X_rk3", "k_zpass_X_rk4"};
+            static const char* names[4] = {"k_zpv_X_rk1", "k_zpv_X_rk2", "k_zpv_X_rk3", "k_zpv_X_rk4"};
             static const double rkb[4] = {8 + 24, 8 + 32, 8 + 32, 0};
             double b = stage < 4 ? rkb[stage - 1] : (KAHAN ? 8 + 40 : 8 + 24);
             pass8(names[stage - 1], b, t, mkrk);
@@ -594,8 +594,8 @@ public:
             if constexpr (KAHAN) {
                 filter_compensated(t);
             } else {
-                pass8("k_zpass_F", 16.0, X, [&](int lo) { return st4(t, lo); });
-                pass8("k_zpass_F", 16.0, t, [&](int lo) { return st4(S, lo); });
+                pass8("k_zpv_F", 16.0, X, [&](int lo) { return st4(t, lo); });
+                pass8("k_zpv_F", 16.0, t, [&](int lo) { return st4(S, lo); });
                 for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
             }
         }
@@ -711,7 +711,7 @@ public:
             launch_rhs_raw(ins[stage - 1]);
             T* t[8];
             tmp8(t);
-            pass8("k_zpass_X", 16.0, K, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpv_X", 16.0, K, [&](int lo) { return st4(t, lo); });
             T* const* xo = outs[stage - 1];
             auto mkrk = [&](int lo) {
                 RK4 er;
@@ -720,13 +720,13 @@ public:
                 er.dt = dt;
                 return er;
             };
-            pass8("k_zpass_X", 24.0, t, mkrk);
+            pass8("k_zpv_X", 24.0, t, mkrk);
         }
         if (filt) {
             T* t[8];
             tmp8(t);
-            pass8("k_zpass_F", 16.0, Xo, [&](int lo) { return st4(t, lo); });
-            pass8("k_zpass_F", 16.0, t, [&](int lo) { return st4(Xo, lo); });
+            pass8("k_zpv_F", 16.0, Xo, [&](int lo) { return st4(t, lo); });
+            pass8("k_zpv_F", 16.0, t, [&](int lo) { return st4(Xo, lo); });
         }
     }
 
@@ -856,18 +856,24 @@ public:
         } else {
             if (g.viscos || g.diffu) return Status::err(DASHA_E_UNSUPPORTED, "adjoint with viscous/diffusive terms");
             const int every = P.filter_every > 0 ? P.filter_every : 1;
-            const int seg = std::max(1, (nsteps + snaps - 1) / std::max(1, snaps));
-            const int nseg = (nsteps + seg - 1) / seg;
             AdjBufs B;
             AdjScratch w;
             // fields: scratch 60, 13 work vectors of 8, snapshots, segment states, stage states
             size_t freeb = 0, totb = 0;
             cudaMemGetInfo(&freeb, &totb);
             const size_t fb = adj_field_bytes(N);
-            const size_t base_fields = 60 + 13 * 8 + (size_t)std::max(nseg, 1) * 8 + (size_t)(seg + 1) * 8;
             const size_t extra = adj_field_bytes(w_netap_max()) + adj_field_bytes((long)mx * mz) + 8192;
+            const double budget = 0.85 * (double)freeb;
+            // snaps == 0: keep every step and stage state of the forward sweep when they fit
+            // (one segment, nothing recomputed), else sqrt(nsteps) segments
+            const size_t all_fields = 60 + 13 * 8 + 8 + (size_t)(nsteps + 1) * 8 + 24 * (size_t)nsteps;
+            const bool keep_all = snaps == 0 && (double)(all_fields * fb + extra) < budget;
+            if (snaps == 0 && !keep_all) snaps = std::max(1, (int)std::lround(std::sqrt((double)nsteps)));
+            const int seg = keep_all ? std::max(1, nsteps) : std::max(1, (nsteps + snaps - 1) / std::max(1, snaps));
+            const int nseg = (nsteps + seg - 1) / seg;
+            const size_t base_fields = 60 + 13 * 8 + (size_t)std::max(nseg, 1) * 8 + (size_t)(seg + 1) * 8;
             const size_t with_stages = (base_fields + 24 * (size_t)seg) * fb + extra;
-            const bool keep_stages = (double)with_stages < 0.85 * (double)freeb;
+            const bool keep_stages = keep_all || (double)with_stages < budget;
             if (!B.reserve(keep_stages ? with_stages : base_fields * fb + extra))
                 return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
             if (!adj_scratch(B, w)) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
@@ -889,15 +895,24 @@ public:
                 if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint stage states");
             }
             copy8(X0, X);
-            // forward sweep with segment snapshots
+            // forward sweep with segment snapshots (keep_all: every step state into sst and its
+            // stage states into stg, so the reverse sweep recomputes nothing)
             T *cur8[8], *nxt8[8];
-            copy8(ta, X0);
-            k8(cur8, ta);
-            k8(nxt8, tb);
-            for (int n = 0; n < nsteps; ++n) {
-                if (n % seg == 0) copy8(snap[n / seg].data(), cur8);
-                fwd_step(cur8, dts[n], n % every == 0, S1, S2, S3, nxt8, Ac);
-                std::swap_ranges(cur8, cur8 + 8, nxt8);
+            if (keep_all) {
+                copy8(sst[0].data(), X0);
+                for (int n = 0; n < nsteps; ++n)
+                    fwd_step(sst[n].data(), dts[n], n % every == 0, stg[3 * n].data(), stg[3 * n + 1].data(),
+                             stg[3 * n + 2].data(), sst[n + 1].data(), Ac);
+                k8(cur8, sst[nsteps].data());
+            } else {
+                copy8(ta, X0);
+                k8(cur8, ta);
+                k8(nxt8, tb);
+                for (int n = 0; n < nsteps; ++n) {
+                    if (n % seg == 0) copy8(snap[n / seg].data(), cur8);
+                    fwd_step(cur8, dts[n], n % every == 0, S1, S2, S3, nxt8, Ac);
+                    std::swap_ranges(cur8, cur8 + 8, nxt8);
+                }
             }
             // seed: dPhi/dX_N
             zero8(lam);
@@ -908,9 +923,9 @@ public:
             // reverse sweep, one segment at a time
             for (int sgi = nseg - 1; sgi >= 0; --sgi) {
                 const int n0 = sgi * seg, n1 = std::min(nsteps, n0 + seg);
-                copy8(sst[0].data(), snap[sgi].data());
                 const bool keep = !stg.empty();
-                for (int n = n0; n < n1 - 1; ++n) {
+                if (!keep_all) copy8(sst[0].data(), snap[sgi].data());
+                for (int n = n0; n < n1 - 1 && !keep_all; ++n) {
                     const int q = n - n0;
                     fwd_step(sst[q].data(), dts[n], n % every == 0, keep ? stg[3 * q].data() : S1,
                              keep ? stg[3 * q + 1].data() : S2, keep ? stg[3 * q + 2].data() : S3, sst[q + 1].data(), Ac);
@@ -920,7 +935,7 @@ public:
                     T* const* Xn = sst[q].data();
                     const double dt = dts[n];
                     T *const *s1 = S1, *const *s2 = S2, *const *s3 = S3;
-                    if (keep && n < n1 - 1) { s1 = stg[3 * q].data(); s2 = stg[3 * q + 1].data(); s3 = stg[3 * q + 2].data(); }
+                    if (keep && (keep_all || n < n1 - 1)) { s1 = stg[3 * q].data(); s2 = stg[3 * q + 1].data(); s3 = stg[3 * q + 2].data(); }
                     else fwd_step(Xn, dt, false, S1, S2, S3, Xo, Ac);  // stage states of step n
                     // mu = F^T lambda
                     if (n % every == 0) {

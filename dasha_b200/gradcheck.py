@@ -1,6 +1,6 @@
 """Gradient of the reconnected flux (the differentiation configuration) and its checks.
 
-    python -m dasha_b200.gradcheck [--config c3] [--steps 500] [--snaps 10] [--dirs 10]
+    python -m dasha_b200.gradcheck [--config c3] [--steps 500] [--snaps 0] [--dirs 10]
                                    [--out FILE]
 
 FP64 forward run from the Harris/GEM state plus a seeded Gaussian psi perturbation
@@ -53,7 +53,7 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="c3")
     ap.add_argument("--steps", type=int, default=None)
-    ap.add_argument("--snaps", type=int, default=10)
+    ap.add_argument("--snaps", type=int, default=0)   # 0: keep all states when they fit
     ap.add_argument("--dirs", type=int, default=10)
     ap.add_argument("--whistler", type=int, default=None)
     ap.add_argument("--out", default=None)

@@ -114,6 +114,17 @@ def test_adjoint_gradient_matches_finite_differences():
         assert abs(ad - fd) <= 1e-4 * max(abs(fd), 1e-12) + 1e-9, (ad, fd)
 
 
+def test_adjoint_plans_agree():
+    """snaps=0 keeps every forward state (no recompute); snaps>0 re-runs segments: the same
+    arithmetic, so the gradients agree to rounding."""
+    d = _ctx(CFG)
+    _, dts = _ctx(CFG).run(CFG.steps)
+    e0, p0 = d.adjoint_flux_grad(dts, snaps=0)
+    e3, p3 = d.adjoint_flux_grad(dts, snaps=3)
+    assert abs(e0 - e3) <= 1e-13 * max(abs(e3), 1e-300)
+    np.testing.assert_allclose(p0, p3, rtol=1e-12, atol=1e-14 * np.abs(p3).max())
+
+
 def test_adjoint_leaves_state_unchanged_and_rejects_fp32():
     d = _ctx(CFG)
     X = d.get_state()
