@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstring>
 #include <algorithm>
+#include <thread>
 
 namespace dasha {
 
@@ -97,6 +98,14 @@ EngineBase* make_engine_f32(int mx, int my, int mz, const dasha_params_c& p, cud
         if (prof.on) { cudaEvent_t b_ = prof.ev(); cudaEventRecord(b_, st); prof.recs.push_back({tg_, a_, b_}); } \
     } while (0)
 
+// host transfer chunks and equilibrium profile lookup (defined after Engine)
+template <class T>
+__global__ void k_import_chunk(int mx, int my, int k0, const double* src, const double* eqprof, T* dst);
+template <class T>
+__global__ void k_export_chunk(int mx, int my, int k0, const T* src, const T* comp, const double* eqprof, double* dst);
+template <class T>
+inline const double* eq_profile(const Geo<T>& g, int m);
+
 // radial smoothing coefficient per node, computed in FP64 then stored as T
 template <class T>
 __global__ void k_init_cr(int mx, int my, int mz, const double* xc, const double* yc, const double* zc, T* cr) {
@@ -136,6 +145,7 @@ public:
     dim3 blk, grd;
 
     ~Engine() override {
+        xbuf_free();
         if (pool) cudaFree(pool);
         if (tab) cudaFree(tab);
         if (dtab) cudaFree(dtab);
@@ -317,44 +327,121 @@ public:
     }
 
     // ---- host array transfer through a FP64 staging buffer, one field at a time ----
-    Status transfer_in(const double* host, long ld1, long ld2, T* const* dst, int nf, bool sub_eq) {
-        size_t plane = (size_t)ld1 * ld2 * (mz + 4);
-        double* stage = nullptr;
-        DASHA_CK(cudaMalloc(&stage, sizeof(double) * plane));
-        Status s = Status::ok();
-        for (int m = 0; m < nf && s.code == 0; ++m) {
-            cudaError_t e = cudaMemcpyAsync(stage, host + plane * m, sizeof(double) * plane, cudaMemcpyHostToDevice, st);
-            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
-            k_import_one(stage, ld1, ld2, m, dst[m], sub_eq);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+    // ---- host <-> device transfer of fields in the caller's Fortran halo layout ----
+    // Chunks of whole z planes (compact mx x my x nk doubles) move through two pinned host
+    // buffers and two device buffers: host threads gather (scatter) the interior rows of the
+    // caller's array into (out of) one pinned buffer while the other's DMA and conversion
+    // kernel run.  Only interior entries are written back, so the caller's halo entries keep
+    // their values.
+    double* xh[2] = {nullptr, nullptr};   // pinned host chunk buffers
+    double* xd[2] = {nullptr, nullptr};   // device chunk buffers
+    cudaEvent_t xev[2] = {nullptr, nullptr};
+    int xnk = 0;                          // z planes per chunk
+    Status xbuf() {
+        if (xh[0]) return Status::ok();
+        const size_t pb = sizeof(double) * (size_t)mx * my;
+        xnk = (int)std::max<size_t>(1, std::min<size_t>((size_t)mz, (size_t(64) << 20) / pb));
+        for (int b = 0; b < 2; ++b) {
+            DASHA_CK(cudaMallocHost(&xh[b], pb * xnk));
+            DASHA_CK(cudaMalloc(&xd[b], pb * xnk));
+            DASHA_CK(cudaEventCreateWithFlags(&xev[b], cudaEventDisableTiming));
         }
-        cudaError_t e = cudaStreamSynchronize(st);
-        cudaFree(stage);
-        if (s.code == 0 && e != cudaSuccess) s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e));
-        return s;
+        return Status::ok();
     }
-    void k_import_one(const double* stage, long ld1, long ld2, int m, T* dst, bool sub_eq);
-    void k_export_one(const T* src, const T* comp, long ld1, long ld2, int m, double* stage, bool add_eq);
+    void xbuf_free() {
+        for (int b = 0; b < 2; ++b) {
+            if (xh[b]) cudaFreeHost(xh[b]);
+            if (xd[b]) cudaFree(xd[b]);
+            if (xev[b]) cudaEventDestroy(xev[b]);
+            xh[b] = xd[b] = nullptr;
+            xev[b] = nullptr;
+        }
+    }
+    // f(r0, r1) over rows [0, n), split across host threads
+    template <class F>
+    static void par_rows(long n, F f) {
+        const unsigned hw = std::thread::hardware_concurrency();
+        const long nt = std::min<long>(16, std::max<long>(1, (long)hw));
+        if (n < 256 || nt == 1) { f(0L, n); return; }
+        std::vector<std::thread> th;
+        const long per = (n + nt - 1) / nt;
+        for (long t = 0; t < nt; ++t) {
+            const long a0 = t * per, a1 = std::min(n, a0 + per);
+            if (a0 < a1) th.emplace_back(f, a0, a1);
+        }
+        for (auto& x : th) x.join();
+    }
+    // caller node (i, j, k) of field m: (i+2) + ld1 (j + ld2 ((k+2) + (mz+4) m))
+    Status transfer_in(const double* host, long ld1, long ld2, T* const* dst, int nf, bool sub_eq) {
+        Status s = xbuf();
+        if (s.code) return s;
+        const size_t fld = (size_t)ld1 * ld2 * (mz + 4);
+        int q = 0;
+        for (int m = 0; m < nf; ++m) {
+            const double* prof = sub_eq ? eq_profile(g, m) : nullptr;
+            for (int k0 = 0; k0 < mz; k0 += xnk, ++q) {
+                const int k1 = std::min(mz, k0 + xnk), b = q & 1;
+                DASHA_CK(cudaEventSynchronize(xev[b]));        // the DMA out of xh[b] is done
+                const double* src = host + fld * m;
+                double* hb = xh[b];
+                par_rows((long)(k1 - k0) * my, [&](long r0, long r1) {
+                    for (long r = r0; r < r1; ++r) {
+                        const long kk = k0 + r / my, j = r % my;
+                        std::memcpy(hb + r * mx, src + 2 + ld1 * (j + ld2 * (kk + 2)), sizeof(double) * mx);
+                    }
+                });
+                DASHA_CK(cudaMemcpyAsync(xd[b], hb, sizeof(double) * (size_t)mx * my * (k1 - k0), cudaMemcpyHostToDevice, st));
+                DASHA_CK(cudaEventRecord(xev[b], st));
+                k_import_chunk<T><<<dim3((mx + blk.x - 1) / blk.x, my, k1 - k0), blk, 0, st>>>(mx, my, k0, xd[b], prof, dst[m]);
+                DASHA_CK(cudaGetLastError());
+            }
+        }
+        DASHA_CK(cudaStreamSynchronize(st));
+        return Status::ok();
+    }
 
     Status transfer_out(double* host, long ld1, long ld2, T* const* src, int nf, bool add_eq,
                         T* const* comp = nullptr) {
-        size_t plane = (size_t)ld1 * ld2 * (mz + 4);
-        double* stage = nullptr;
-        DASHA_CK(cudaMalloc(&stage, sizeof(double) * plane));
-        Status s = Status::ok();
-        for (int m = 0; m < nf && s.code == 0; ++m) {
-            // keep the caller's halo entries: start from the host field
-            cudaError_t e = cudaMemcpyAsync(stage, host + plane * m, sizeof(double) * plane, cudaMemcpyHostToDevice, st);
-            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
-            k_export_one(src[m], comp ? comp[m] : nullptr, ld1, ld2, m, stage, add_eq);
-            e = cudaMemcpyAsync(host + plane * m, stage, sizeof(double) * plane, cudaMemcpyDeviceToHost, st);
-            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
-            e = cudaStreamSynchronize(st);
-            if (e != cudaSuccess) { s = Status::err(DASHA_E_CUDA, cudaGetErrorString(e)); break; }
+        Status s = xbuf();
+        if (s.code) return s;
+        const size_t fld = (size_t)ld1 * ld2 * (mz + 4);
+        struct Pend { int m, k0, k1, b; };
+        Pend prev{-1, 0, 0, 0};
+        auto scatter = [&](const Pend& c) -> Status {
+            DASHA_CK(cudaEventSynchronize(xev[c.b]));       // its D2H has landed
+            double* dstp = host + fld * c.m;
+            const double* hb = xh[c.b];
+            par_rows((long)(c.k1 - c.k0) * my, [&](long r0, long r1) {
+                for (long r = r0; r < r1; ++r) {
+                    const long kk = c.k0 + r / my, j = r % my;
+                    std::memcpy(dstp + 2 + ld1 * (j + ld2 * (kk + 2)), hb + r * mx, sizeof(double) * mx);
+                }
+            });
+            return Status::ok();
+        };
+        int q = 0;
+        for (int m = 0; m < nf; ++m) {
+            const double* prof = add_eq ? eq_profile(g, m) : nullptr;
+            for (int k0 = 0; k0 < mz; k0 += xnk, ++q) {
+                const int k1 = std::min(mz, k0 + xnk), b = q & 1;
+                k_export_chunk<T><<<dim3((mx + blk.x - 1) / blk.x, my, k1 - k0), blk, 0, st>>>(
+                    mx, my, k0, src[m], comp ? comp[m] : nullptr, prof, xd[b]);
+                DASHA_CK(cudaGetLastError());
+                DASHA_CK(cudaMemcpyAsync(xh[b], xd[b], sizeof(double) * (size_t)mx * my * (k1 - k0), cudaMemcpyDeviceToHost, st));
+                DASHA_CK(cudaEventRecord(xev[b], st));
+                if (prev.m >= 0) {                             // scatter the previous chunk meanwhile
+                    s = scatter(prev);
+                    if (s.code) return s;
+                }
+                prev = {m, k0, k1, b};
+            }
         }
-        cudaFree(stage);
-        return s;
+        if (prev.m >= 0) {
+            s = scatter(prev);
+            if (s.code) return s;
+        }
+        DASHA_CK(cudaStreamSynchronize(st));
+        return Status::ok();
     }
 
     Status set_state(const double* x, long ld1, long ld2) override {
@@ -983,27 +1070,26 @@ public:
     }
 };
 
+// one chunk of whole z planes k0.. (compact mx x my x nk doubles) into / out of field T
 template <class T>
-__global__ void k_import_field(int mx, int my, int mz, const double* src, long ld1, long ld2, double eq_scale,
-                               const double* eqprof, T* dst) {
+__global__ void k_import_chunk(int mx, int my, int k0, const double* src, const double* eqprof, T* dst) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= mx) return;
-    int j = blockIdx.y, k = blockIdx.z;
-    double v = src[(i + 2) + ld1 * (j + ld2 * (long)(k + 2))];
-    if (eqprof) v -= eq_scale * eqprof[k];
+    const int j = blockIdx.y, k = k0 + blockIdx.z;
+    double v = src[(long)i + (long)mx * (j + (long)my * blockIdx.z)];
+    if (eqprof) v -= eqprof[k];
     dst[(long)i + (long)mx * (j + (long)my * k)] = T(v);
 }
 template <class T>
-__global__ void k_export_field(int mx, int my, int mz, const T* src, const T* comp, const double* eqprof, double* dst,
-                               long ld1, long ld2) {
+__global__ void k_export_chunk(int mx, int my, int k0, const T* src, const T* comp, const double* eqprof, double* dst) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= mx) return;
-    int j = blockIdx.y, k = blockIdx.z;
+    const int j = blockIdx.y, k = k0 + blockIdx.z;
     const long n = (long)i + (long)mx * (j + (long)my * k);
     double v = (double)src[n];
     if (comp) v -= (double)comp[n];   // compensated FP32 state: the value is x - comp
     if (eqprof) v += eqprof[k];
-    dst[(i + 2) + ld1 * (j + ld2 * (long)(k + 2))] = v;
+    dst[(long)i + (long)mx * (j + (long)my * blockIdx.z)] = v;
 }
 
 template <class T>
@@ -1016,17 +1102,6 @@ inline const double* eq_profile(const Geo<T>& g, int m) {
         case 7: return g.p0;
         default: return nullptr;
     }
-}
-
-template <class T>
-void Engine<T>::k_import_one(const double* stage, long ld1, long ld2, int m, T* dst, bool sub_eq) {
-    const double* prof = sub_eq ? eq_profile(g, m) : nullptr;
-    k_import_field<T><<<grd, blk, 0, st>>>(mx, my, mz, stage, ld1, ld2, 1.0, prof, dst);
-}
-template <class T>
-void Engine<T>::k_export_one(const T* src, const T* comp, long ld1, long ld2, int m, double* stage, bool add_eq) {
-    const double* prof = add_eq ? eq_profile(g, m) : nullptr;
-    k_export_field<T><<<grd, blk, 0, st>>>(mx, my, mz, src, comp, prof, stage, ld1, ld2);
 }
 
 }  // namespace dasha
