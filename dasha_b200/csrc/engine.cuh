@@ -5,6 +5,7 @@
 #include "mhd_kernels.cuh"
 #include "zm_kernels.cuh"
 #include "zpv.cuh"
+#include "zpv2.cuh"
 #include "adjoint.cuh"
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -498,6 +499,31 @@ public:
         return cudaFuncSetAttribute(zpv_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ZVc<NF>::smem());
     }
+    // k_zpv2 (two passes in one launch): tile 32*ZVX x 8, one row per warp plus two halo-row
+    // warps, D planes in flight
+    template <int NF>
+    struct ZC2 {
+        static constexpr int TY = 8;
+        static constexpr int D = sizeof(T) == 4 ? 3 : 2;
+    };
+    template <int NF>
+    using ZV2c = ZV2<T, NF, ZVX, ZC2<NF>::TY, ZC2<NF>::D>;
+    template <int NF, unsigned KINDS, class Epi>
+    static constexpr auto zpv2_fn() { return k_zpv2<T, NF, KINDS, ZVX, ZC2<NF>::TY, ZC2<NF>::D, Epi>; }
+    // two smoothing passes of NF fields: src -> epi (src must not alias the epilogue's outputs)
+    template <int NF, unsigned KINDS, class Epi>
+    void zp2(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
+        using Z = ZV2c<NF>;
+        dim3 gg((mx + Z::TX - 1) / Z::TX, (my + ZC2<NF>::TY - 1) / ZC2<NF>::TY, 1);
+        int ch = zchunk(gg.x * gg.y, 16);
+        gg.z = (mz + ch - 1) / ch;
+        DASHA_LAUNCH(tag, bytes, (zpv2_fn<NF, KINDS, Epi>()<<<gg, 32 * Z::NW, Z::smem(), st>>>(g, src, epi, ch)));
+    }
+    template <int NF, unsigned KINDS, class Epi>
+    static cudaError_t zp2_attr1() {
+        return cudaFuncSetAttribute(zpv2_fn<NF, KINDS, Epi>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ZV2c<NF>::smem());
+    }
     using St3 = VStore<T, 3, ZVX>;
     using St4 = VStore<T, 4, ZVX>;
     using Acc3 = VAcc<T, 3, ZVX>;
@@ -511,6 +537,7 @@ public:
         if ((e = zp_attr1<4, KIND_B4, St4>())) return e;
         if ((e = zp_attr1<4, 0u, RK4>())) return e;
         if ((e = zp_attr1<4, KIND_B4, RK4>())) return e;
+        if ((e = zp2_attr1<3, KIND_H, St3>())) return e;
         if constexpr (KAHAN) {
             if ((e = zp_attr1<4, 0u, VStore<T, 2, ZVX>, 1>())) return e;
             if ((e = zp_attr1<4, KIND_P45, VStore<T, 2, ZVX>, 1>())) return e;
@@ -547,6 +574,28 @@ public:
         zp<4, KIND_B4>(tag, 0.5 * bytes_per_cell * N * sizeof(T), b, mk(4));
     }
     static St4 st4(T* const* p, int lo) { St4 s; for (int q = 0; q < 4; ++q) s.f[q] = p[lo + q]; return s; }
+    // values per field the RK stage epilogue reads and writes (base, acc, x, comp)
+    static constexpr double rk_io(int stage) { return stage == 1 ? 3.0 : (stage < 4 ? 4.0 : (KAHAN ? 5.0 : 2.0)); }
+    // both xdif avrg passes of the raw RHS k, the second ending in the RK stage update: x =
+    // stage state (or the step result at stage 4), base, acc, comp (FP32 Kahan compensation or
+    // null)
+    void rk_passes(int stage, double dt, T* const* k, T* const* base, T* const* x, T* const* acc, T* const* comp) {
+        static const char* names[4] = {"k_zpv_X_rk1", "k_zpv_X_rk2", "k_zpv_X_rk3", "k_zpv_X_rk4"};
+        T* t[8];
+        tmp8(t);
+        pass8("k_zpv_X", 16.0, k, [&](int lo) { return st4(t, lo); });
+        auto mk = [&](int lo) {
+            RK4 er;
+            for (int m = 0; m < 4; ++m) {
+                er.x[m] = x[lo + m]; er.base[m] = base[lo + m]; er.acc[m] = acc[lo + m];
+                er.comp[m] = comp ? comp[lo + m] : nullptr;
+            }
+            er.stage = stage;
+            er.dt = dt;
+            return er;
+        };
+        pass8(names[stage - 1], 8.0 * (1.0 + rk_io(stage)), t, mk);
+    }
 
     // avrgtt on the compensated FP32 state (X, C): pass 1 writes its increment of X - C into
     // t, pass 2 adds the two-pass increment to (X, C) in place with a Kahan step
@@ -573,15 +622,31 @@ public:
     T** Ef = nullptr;     // total E after launch_rhs_raw
 
     // n smoothing passes of 3 fields, ping-pong between a and b starting from a; returns the
-    // buffer holding the result
+    // buffer holding the result.
+    // Pass pairs of the Hall chain (constant coefficient 1/8) run fused in k_zpv2.  Measured on
+    // B200 (FP32 1024x512x1024 / FP64 512x256x512 step): Hall pairs fused 436.0 / 107.7 ms,
+    // nothing fused 442.1 / 108.4; fusing the radial-coefficient chains J and E as well 437.3 /
+    // 186.7 with everything; the xdif pair with the RK update 138.4 (FP64), the FP64 filter
+    // 114.1: where the coefficient is evaluated per node, or the epilogue is heavy, the doubled
+    // per-node work and the lower occupancy of the 320-thread CTA outweigh the saved traffic.
     template <unsigned KINDS>
     T** passes3(const char* tag, T** a, T** b, int n) {
-        for (int p = 0; p < n; ++p) {
-            T** in = (p & 1) ? b : a;
-            T** out = (p & 1) ? a : b;
-            zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+        if constexpr (KINDS == KIND_H) {
+            for (int p = 0; p < n; p += 2) {   // pairs of passes in one k_zpv2 launch, a lone last one by k_zpv
+                T** in = ((p / 2) & 1) ? b : a;
+                T** out = ((p / 2) & 1) ? a : b;
+                if (p + 1 < n) zp2<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+                else zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+            }
+            return (((n + 1) / 2) & 1) ? b : a;
+        } else {
+            for (int p = 0; p < n; ++p) {
+                T** in = (p & 1) ? b : a;
+                T** out = (p & 1) ? a : b;
+                zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+            }
+            return (n & 1) ? b : a;
         }
-        return (n & 1) ? b : a;
     }
 
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
@@ -651,27 +716,11 @@ public:
 
     Status stepon(double time, double dt, int nstep) override {
         (void)time;
-        // stages 1..4: base = X, stage state in S, accumulator in A; the second xdif
-        // smoothing pass ends in the RK stage update
+        // stages 1..4: base = X, stage state in S, accumulator in A; both xdif smoothing
+        // passes run in one k_zpv2 launch per field pair that ends in the RK stage update
         for (int stage = 1; stage <= 4; ++stage) {
             launch_rhs_raw(stage == 1 ? X : S);
-            T* t[8];
-            tmp8(t);
-            pass8("k_zpv_X", 16.0, K, [&](int lo) { return st4(t, lo); });
-            auto mkrk = [&](int lo) {
-                RK4 er;
-                for (int m = 0; m < 4; ++m) {
-                    er.x[m] = S[lo + m]; er.base[m] = X[lo + m]; er.acc[m] = A[lo + m];
-                    er.comp[m] = KAHAN ? C[lo + m] : nullptr;
-                }
-                er.stage = stage;
-                er.dt = dt;
-                return er;
-            };
-            static const char* names[4] = {"k_zpv_X_rk1", "k_zpv_X_rk2", "k_zpv_X_rk3", "k_zpv_X_rk4"};
-            static const double rkb[4] = {8 + 24, 8 + 32, 8 + 32, 0};
-            double b = stage < 4 ? rkb[stage - 1] : (KAHAN ? 8 + 40 : 8 + 24);
-            pass8(names[stage - 1], b, t, mkrk);
+            rk_passes(stage, dt, K, X, S, A, KAHAN ? C : nullptr);
         }
         for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
         int every = P.filter_every > 0 ? P.filter_every : 1;
@@ -796,18 +845,7 @@ public:
         T* const* ins[4] = {Xb, S1, S2, S3};
         for (int stage = 1; stage <= 4; ++stage) {
             launch_rhs_raw(ins[stage - 1]);
-            T* t[8];
-            tmp8(t);
-            pass8("k_zpv_X", 16.0, K, [&](int lo) { return st4(t, lo); });
-            T* const* xo = outs[stage - 1];
-            auto mkrk = [&](int lo) {
-                RK4 er;
-                for (int m = 0; m < 4; ++m) { er.x[m] = xo[lo + m]; er.base[m] = Xb[lo + m]; er.acc[m] = Acc[lo + m]; er.comp[m] = nullptr; }
-                er.stage = stage;
-                er.dt = dt;
-                return er;
-            };
-            pass8("k_zpv_X", 24.0, t, mkrk);
+            rk_passes(stage, dt, K, Xb, outs[stage - 1], Acc, nullptr);
         }
         if (filt) {
             T* t[8];
