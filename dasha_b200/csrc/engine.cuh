@@ -6,6 +6,7 @@
 #include "zm_kernels.cuh"
 #include "zpv.cuh"
 #include "zpv2.cuh"
+#include "zcurl.cuh"
 #include "adjoint.cuh"
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -524,6 +525,15 @@ public:
         return cudaFuncSetAttribute(zpv2_fn<NF, KINDS, Epi>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ZV2c<NF>::smem());
     }
+    // k_zcurl: tile 32*ZVX x 8, one row per warp, 2 planes in flight beyond c+2
+    using ZC3c = ZC3<T, ZVX, 8, 2>;
+    template <int SIGN>
+    void zcurl(const char* tag, const SrcFields<T, 3>& src, F3<T> out) {
+        dim3 gg((mx + ZC3c::TX - 1) / ZC3c::TX, (my + 7) / 8, 1);
+        int ch = zchunk(gg.x * gg.y, 16);
+        gg.z = (mz + ch - 1) / ch;
+        DASHA_LAUNCH(tag, 6.0 * N * sizeof(T), (k_zcurl<T, ZVX, 8, 2, SIGN><<<gg, 256, ZC3c::smem(), st>>>(g, src, out, ch)));
+    }
     using St3 = VStore<T, 3, ZVX>;
     using St4 = VStore<T, 4, ZVX>;
     using Acc3 = VAcc<T, 3, ZVX>;
@@ -548,11 +558,11 @@ public:
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
             return e;
-        if ((e = cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, 1>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)ZS2<T, 3, ZTX, 8>::smem(false))))
+        if ((e = cudaFuncSetAttribute(k_zcurl<T, ZVX, 8, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ZC3c::smem())))
             return e;
-        return cudaFuncSetAttribute(k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, -1>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)ZS2<T, 3, ZTX, 8>::smem(false));
+        return cudaFuncSetAttribute(k_zcurl<T, ZVX, 8, 2, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)ZC3c::smem());
     }
     static constexpr int HMINB = sizeof(T) == 4 ? 2 : 1;   // CTAs per SM asked of the register allocator
     static SrcFields<T, 3> src3(T* const* p) { SrcFields<T, 3> s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
@@ -652,13 +662,7 @@ public:
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
     void launch_current(T* const* xs) {
         T* bb[3] = {xs[4], xs[5], xs[6]};
-        dim3 gg(mx / ZTX, (my + 7) / 8, 1);
-        int ch = zchunk(gg.x * gg.y, 32);
-        gg.z = (mz + ch - 1) / ch;
-        OpCurl<T, 1> oc;
-        for (int q = 0; q < 3; ++q) oc.out[q] = cur[0][q];
-        DASHA_LAUNCH("k_curl", 6.0 * N * sizeof(T),
-                     (k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, 1>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(bb), oc, ch)));
+        zcurl<1>("k_curl", src3(bb), f3(cur[0]));
         curF = passes3<0u>("k_zpv_J", cur[0], cur[1], 4);
         if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(curF)));
     }
@@ -690,10 +694,8 @@ public:
         oh.j1 = curF[0]; oh.j2 = curF[1]; oh.j3 = curF[2]; oh.b1 = xs[4]; oh.b2 = xs[5]; oh.b3 = xs[6];
         DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
                      (k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>><<<gg, ZTX * 8, ZS2<T, 5, ZTX, 8>::smem(true), st>>>(g, sh, oh, ch)));
-        OpCurl<T, -1> oi;
-        oi.out[0] = K[4]; oi.out[1] = K[5]; oi.out[2] = K[6];
-        DASHA_LAUNCH("k_rhs_induction", 6.0 * N * sizeof(T),
-                     (k_zst2<T, 3, ZTX, 8, 2, OpCurl<T, -1>><<<gg, ZTX * 8, ZS2<T, 3, ZTX, 8>::smem(false), st>>>(g, src3(Ef), oi, ch)));
+        T* kb[3] = {K[4], K[5], K[6]};
+        zcurl<-1>("k_rhs_induction", src3(Ef), f3(kb));
     }
     // 8 scratch fields that are free once the RHS is written
     void tmp8(T** t) {

@@ -3,7 +3,8 @@
 // shared-memory ring filled by cp.async.  Global memory is read once per plane (plus the x-y
 // halo, which neighbouring CTAs read at about the same time and so mostly hits L2) and
 // written once.  This file holds the shared helpers and the radius-2 ring framework k_zst2
-// (curl, induction, hydro RHS); the smoothing passes are k_zpv in zpv.cuh.
+// (hydro RHS); the smoothing passes are k_zpv / k_zpv2 (zpv.cuh, zpv2.cuh), the curls k_zcurl
+// (zcurl.cuh).
 #pragma once
 #include "mhd_kernels.cuh"
 
@@ -211,51 +212,6 @@ __global__ void __launch_bounds__(TX* TYH, MINB) k_zst2(Geo<T> g, SrcFields<T, N
     }
     cp_async_wait<0>();
 }
-
-// SIGN * curl of the 3 ring fields, wall rows applied: SIGN = +1 is J1 = curl(B - B0)
-// (current t3dsdsc.f:2476-2491 with bndryc), SIGN = -1 is dB/dt = -curl E (t3dsdsc.f:1435-1452)
-template <class T, int SIGN>
-struct OpCurl {
-    static constexpr bool RINV = false;
-    T* out[3];
-    struct Col { T ax, bx, cx, dx, ay, by, cy, dy; };
-    struct Pre { T az, bz, cz, dz; };
-    __device__ __forceinline__ void column(const Geo<T>& g, int i, int j, Col& c) const {
-        c.ax = g.a1x[i]; c.bx = g.b1x[i]; c.cx = g.c1x[i]; c.dx = g.d1x[i];
-        c.ay = g.a1y[j]; c.by = g.b1y[j]; c.cy = g.c1y[j]; c.dy = g.d1y[j];
-    }
-    __device__ __forceinline__ void pre(const Geo<T>& g, int, int, int c, Pre& p) const {
-        p.az = g.a1z[c]; p.bz = g.b1z[c]; p.cz = g.c1z[c]; p.dz = g.d1z[c];
-    }
-    template <class V>
-    __device__ __forceinline__ void compute(const Geo<T>& g, const V& v, int i, int j, int c, const Col& k,
-                                            const Pre& p) const {
-        auto DX = [&](int f) { return d1fc(v.X(f, 0), v.X(f, 1), v.X(f, 2), v.X(f, 3), v.X(f, 4), k.ax, k.bx, k.cx, k.dx); };
-        auto DY = [&](int f) { return d1fc(v.Y(f, 0), v.Y(f, 1), v.Y(f, 2), v.Y(f, 3), v.Y(f, 4), k.ay, k.by, k.cy, k.dy); };
-        auto DZ = [&](int f) { return d1fc(v.Zz(f, 0), v.Zz(f, 1), v.Zz(f, 2), v.Zz(f, 3), v.Zz(f, 4), p.az, p.bz, p.cz, p.dz); };
-        T o[3];
-        if (SIGN > 0) {
-            o[0] = DY(2) - DZ(1);
-            o[1] = DZ(0) - DX(2);
-            o[2] = DX(1) - DY(0);
-        } else {
-            o[0] = -DY(2) + DZ(1);
-            o[1] = -DZ(0) + DX(2);
-            o[2] = -DX(1) + DY(0);
-        }
-        const long base = (long)i + (long)j * g.sy;
-#pragma unroll
-        for (int m = 0; m < 3; ++m) out[m][base + (long)c * g.sz] = o[m];
-        if (c == 2 || c == g.mz - 3) {
-            const int kh = c == 2 ? 1 : g.mz - 2, kz = c == 2 ? 0 : g.mz - 1;
-#pragma unroll
-            for (int m = 0; m < 3; ++m) {
-                out[m][base + (long)kh * g.sz] = T(0.5) * o[m];
-                out[m][base + (long)kz * g.sz] = T(0);
-            }
-        }
-    }
-};
 
 template <class T>
 struct OpHydro {
