@@ -7,6 +7,7 @@
 #include "zpv.cuh"
 #include "zpv2.cuh"
 #include "zcurl.cuh"
+#include "zhydro.cuh"
 #include "adjoint.cuh"
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -534,6 +535,11 @@ public:
         gg.z = (mz + ch - 1) / ch;
         DASHA_LAUNCH(tag, 6.0 * N * sizeof(T), (k_zcurl<T, ZVX, 8, 2, SIGN><<<gg, 256, ZC3c::smem(), st>>>(g, src, out, ch)));
     }
+    // k_zhydro: tile 32*ZVX x ZH_TY, 1 plane in flight beyond c+2.  Measured (hydro ms per step,
+    // FP32 1024x512x1024 / FP64 512x256x512): 8 rows, 1 CTA/SM 57.6 / 16.6; 8 rows capped at 2
+    // CTAs/SM (spills) 73.9 / -; 4 rows, 3 CTAs/SM 60.8 / 12.8; 4 rows, 2 CTAs/SM 57.9 / 14.3
+    static constexpr int ZH_TY = sizeof(T) == 4 ? 8 : 4, ZH_MINB = sizeof(T) == 4 ? 1 : 3;
+    using ZHc = ZH<T, ZVX, ZH_TY, 1>;
     using St3 = VStore<T, 3, ZVX>;
     using St4 = VStore<T, 4, ZVX>;
     using Acc3 = VAcc<T, 3, ZVX>;
@@ -557,6 +563,9 @@ public:
         }
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_zhydro<T, ZVX, ZH_TY, 1, ZH_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ZHc::smem())))
             return e;
         if ((e = cudaFuncSetAttribute(k_zcurl<T, ZVX, 8, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZC3c::smem())))
@@ -687,6 +696,17 @@ public:
         dim3 gg(mx / ZTX, (my + 7) / 8, 1);
         int ch = zchunk(gg.x * gg.y, 32);
         gg.z = (mz + ch - 1) / ch;
+        if (!g.viscos && !g.diffu) {   // register-blocked fast path (no viscosity, no diffusion)
+            HydroIO<T> hio;
+            hio.drho = xs[0]; hio.m1 = xs[1]; hio.m2 = xs[2]; hio.m3 = xs[3]; hio.dp = xs[7];
+            hio.j1 = curF[0]; hio.j2 = curF[1]; hio.j3 = curF[2]; hio.b1 = xs[4]; hio.b2 = xs[5]; hio.b3 = xs[6];
+            hio.out[0] = K[0]; hio.out[1] = K[1]; hio.out[2] = K[2]; hio.out[3] = K[3]; hio.out[4] = K[7];
+            dim3 gh((mx + ZHc::TX - 1) / ZHc::TX, (my + ZH_TY - 1) / ZH_TY, 1);
+            int chh = zchunk(gh.x * gh.y, 16);
+            gh.z = (mz + chh - 1) / chh;
+            DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
+                         (k_zhydro<T, ZVX, ZH_TY, 1, ZH_MINB><<<gh, 32 * ZH_TY, ZHc::smem(), st>>>(g, hio, chh)));
+        } else {
         SrcFields<T, 5> sh;
         sh.f[0] = xs[0]; sh.f[1] = xs[1]; sh.f[2] = xs[2]; sh.f[3] = xs[3]; sh.f[4] = xs[7];
         OpHydro<T> oh;
@@ -694,6 +714,7 @@ public:
         oh.j1 = curF[0]; oh.j2 = curF[1]; oh.j3 = curF[2]; oh.b1 = xs[4]; oh.b2 = xs[5]; oh.b3 = xs[6];
         DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
                      (k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>><<<gg, ZTX * 8, ZS2<T, 5, ZTX, 8>::smem(true), st>>>(g, sh, oh, ch)));
+        }
         T* kb[3] = {K[4], K[5], K[6]};
         zcurl<-1>("k_rhs_induction", src3(Ef), f3(kb));
     }

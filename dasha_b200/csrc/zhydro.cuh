@@ -1,0 +1,296 @@
+// k_zhydro: the hydro part of the right-hand side (right, t3dsdsc.f:1334-1566 with bndry):
+// continuity, momentum (fluxes rho v_i v_j + (p - p0) delta_ij, J x B - xresd) and the pressure
+// equation, for the case without viscosity and diffusion; z-marching and register-blocked.
+//
+// A warp covers 32*VX consecutive x nodes (VX = 2 in FP32: float pairs), one row per warp, TY
+// warps per CTA.  Planes of m1, m2, m3, p - p0 and rho - rho0 (tile plus a 2-node x/y halo, no
+// corners) stream into an NS = D + 5 stage shared-memory ring with cp.async; the thread whose
+// copy landed turns rho - rho0 into 1/rho in place.  The five quantities of the own nodes for
+// planes c-2 .. c+2 stay in a register queue (the z stencil), so per plane a thread reads plane
+// c+2 of its nodes, the x neighbours beyond its pair and rows c+-1, c+-2.  Fluxes are formed at
+// each stencil node from (m, p - p0, 1/rho) there, as in the reference.  At step c the ring is
+// read at planes c and c+2, and by threads one step behind at c-1 and c+1; the first step also
+// reads planes c-2 .. c+1 for the queue, so it holds planes c-2 .. c+2+D (hence D + 5 stages),
+// and ends with a second barrier.
+#pragma once
+
+namespace dasha {
+
+template <class T, int VX, int TY, int D>
+struct ZH {
+    static constexpr int TX = 32 * VX;
+    static constexpr int EPC = 16 / (int)sizeof(T);
+    static constexpr int OFF = EPC;                   // interior column offset (>= 2)
+    static constexpr int RS = TX + 2 * OFF;
+    static constexpr int NR = TY + 4;                 // rows y0-2 .. y0+TY+1
+    static constexpr int SP = NR * RS;
+    static constexpr int NF = 5;                      // m1 m2 m3 dp ri
+    static constexpr int NS = D + 5;
+    static constexpr int CH = TX / EPC;
+    static constexpr size_t smem() { return sizeof(T) * (size_t)NS * NF * SP; }
+};
+
+// out: xdif 0 (rho), 1..3 (m), 4 (p); src: rho-rho0, m1, m2, m3, p-p0; pointwise J, B
+template <class T>
+struct HydroIO {
+    const T *drho, *m1, *m2, *m3, *dp;
+    const T *j1, *j2, *j3, *b1, *b2, *b3;
+    T* out[5];
+};
+
+template <class T, int VX, int TY, int D, int MINB = 1>
+__global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> io, int chunk) {
+    using Z = ZH<T, VX, TY, D>;
+    constexpr int TX = Z::TX, EPC = Z::EPC, OFF = Z::OFF, RS = Z::RS, NR = Z::NR, SP = Z::SP, NF = Z::NF,
+                  NS = Z::NS, CH = Z::CH;
+    constexpr int NT = 32 * TY;
+    constexpr int NVEC = NR * CH;
+    constexpr int NHAL = 4 * TY;                      // x-halo columns x0-2, x0-1, x0+wx, x0+wx+1 on the tile rows
+    using IO = VIO<T, VX>;
+    extern __shared__ __align__(16) unsigned char zh_smem_raw[];
+    T* ring = reinterpret_cast<T*>(zh_smem_raw);      // [NS][NF][SP]: m1 m2 m3 dp ri
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int wx = min(TX, g.mx - x0);
+    const int mz = g.mz;
+    const int k0 = blockIdx.z * chunk;
+    const int k1 = min(k0 + chunk, mz);
+    const int cA = max(k0, 2), cB = min(k1 - 1, mz - 3);
+    if (cA > cB) return;
+    const T* srcf[NF] = {io.m1, io.m2, io.m3, io.dp, io.drho};
+    constexpr int NSL = (NVEC + NHAL + NT - 1) / NT;
+    long gsrc[NSL];
+    int sdst[NSL];
+    bool svec[NSL];
+#pragma unroll
+    for (int q = 0; q < NSL; ++q) {
+        const int sl = tid + q * NT;
+        gsrc[q] = -1;
+        sdst[q] = 0;
+        svec[q] = sl < NVEC;
+        if (sl < NVEC) {
+            const int r = sl / CH, ch = sl % CH;
+            if (ch * EPC < wx) {
+                gsrc[q] = (long)(x0 + ch * EPC) + (long)pmod(y0 - 2 + r, g.my) * g.sy;
+                sdst[q] = r * RS + OFF + ch * EPC;
+            }
+        } else if (sl < NVEC + NHAL) {
+            const int h = sl - NVEC, r = h % TY + 2, side = h / TY;   // side 0..3: x0-2, x0-1, x0+wx, x0+wx+1
+            const int dx = side < 2 ? side - 2 : wx + side - 2;
+            gsrc[q] = (long)pmod(x0 + dx, g.mx) + (long)pmod(y0 - 2 + r, g.my) * g.sy;
+            sdst[q] = r * RS + OFF + dx;
+        }
+    }
+    const int phi = cB + 2;
+    auto issue = [&](int p) {
+        if (p <= phi) {
+            T* stg = ring + (size_t)(p % NS) * NF * SP;
+#pragma unroll
+            for (int q = 0; q < NSL; ++q) {
+                if (gsrc[q] >= 0) {
+                    const long zo = gsrc[q] + (long)p * g.sz;
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) {
+                        if (svec[q]) cp_async16(stg + f * SP + sdst[q], srcf[f] + zo);
+                        else cp_async_elem(stg + f * SP + sdst[q], srcf[f] + zo);
+                    }
+                }
+            }
+        }
+        cp_async_commit();
+    };
+    // 1/rho of the nodes this thread copied in plane p (its own copies have landed)
+    auto make_ri = [&](int p) {
+        const T r0 = T(g.rho0[p]);
+        T* ri = ring + (size_t)(p % NS) * NF * SP + 4 * SP;
+#pragma unroll
+        for (int q = 0; q < NSL; ++q) {
+            if (gsrc[q] >= 0) {
+                if (svec[q]) {
+#pragma unroll
+                    for (int e = 0; e < EPC; ++e) ri[sdst[q] + e] = T(1) / (r0 + ri[sdst[q] + e]);
+                } else {
+                    ri[sdst[q]] = T(1) / (r0 + ri[sdst[q]]);
+                }
+            }
+        }
+    };
+#pragma unroll
+    for (int p = 0; p < D + 4; ++p) issue(cA - 2 + p);   // planes cA-2 .. cA+1+D
+
+    const int xl = VX * lane;
+    const bool xon = xl < wx;
+    const int gi = x0 + (xon ? xl : 0);
+    const int gj = y0 + w;
+    const bool yon = gj < g.my;
+    const int jj = yon ? gj : g.my - 1;
+    T ax[VX], bx[VX], cx[VX], dx[VX];
+#pragma unroll
+    for (int e = 0; e < VX; ++e) { ax[e] = g.a1x[gi + e]; bx[e] = g.b1x[gi + e]; cx[e] = g.c1x[gi + e]; dx[e] = g.d1x[gi + e]; }
+    const T ay = g.a1y[jj], by = g.b1y[jj], cy = g.c1y[jj], dy = g.d1y[jj];
+    const int me = (w + 2) * RS + OFF + xl;           // own first node in a ring plane
+    const long col = (long)gi + (long)jj * g.sy;
+    T zq[5][NF][VX];                                  // own (m1 m2 m3 dp ri), planes c-2 .. c+2
+    bool primed = false;
+    for (int c = cA; c <= cB; ++c) {
+        issue(c + 2 + D);
+        // pointwise operands of plane c, loaded before the barrier
+        T j1[VX], j2[VX], j3[VX], b1[VX], b2[VX], b3[VX];
+        if (xon && yon) {
+            const long q = col + (long)c * g.sz;
+            IO::ld(io.j1 + q, j1); IO::ld(io.j2 + q, j2); IO::ld(io.j3 + q, j3);
+            IO::ld(io.b1 + q, b1); IO::ld(io.b2 + q, b2); IO::ld(io.b3 + q, b3);
+        }
+        const T az = g.a1z[c], bz = g.b1z[c], cz = g.c1z[c], dz = g.d1z[c];
+        cp_async_wait<D>();
+        if (!primed)
+            for (int p = c - 2; p <= c + 2; ++p) make_ri(p);
+        else
+            make_ri(c + 2);
+        __syncthreads();
+        const T* pc = ring + (size_t)(c % NS) * NF * SP;
+        if (!primed) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const T* ps = ring + (size_t)((c - 2 + s) % NS) * NF * SP;
+#pragma unroll
+                for (int f = 0; f < NF; ++f) IO::ld(ps + f * SP + me, zq[s][f]);
+            }
+            primed = true;
+            __syncthreads();   // planes c-2, c-1 are refilled within the next steps
+        }
+        {
+            const T* p2 = ring + (size_t)((c + 2) % NS) * NF * SP;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) IO::ld(p2 + f * SP + me, zq[4][f]);
+        }
+        if (xon && yon) {
+            // o[0..4]: xdif of rho, m1, m2, m3, p; dv = -div(v) terms; grad p
+            T o[5][VX], dvv[VX], px[VX], py[VX], pz[VX];
+            // the six x/y/z quantities of one stencil node from (m1 m2 m3 dp ri) there:
+            // direction d: m_d, F_1d, F_2d, F_3d (+ dp on the diagonal), dp, v_d
+            // ---- x ----
+            {
+                T lo[NF][2], hi[NF][2];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    lo[f][0] = pc[f * SP + me - 2]; lo[f][1] = pc[f * SP + me - 1];
+                    hi[f][0] = pc[f * SP + me + VX]; hi[f][1] = pc[f * SP + me + VX + 1];
+                }
+#pragma unroll
+                for (int e = 0; e < VX; ++e) {
+                    T q6[6][5];   // quantity, offset -2..2
+#pragma unroll
+                    for (int s = -2; s <= 2; ++s) {
+                        const int k = e + s;
+                        T v[NF];
+#pragma unroll
+                        for (int f = 0; f < NF; ++f)
+                            v[f] = k < 0 ? lo[f][k + 2] : (k >= VX ? hi[f][k - VX] : zq[2][f][k < 0 ? 0 : (k >= VX ? VX - 1 : k)]);
+                        const T a = v[0] * v[4];
+                        q6[0][s + 2] = v[0];
+                        q6[1][s + 2] = v[0] * v[0] * v[4] + v[3];
+                        q6[2][s + 2] = v[0] * v[1] * v[4];
+                        q6[3][s + 2] = v[0] * v[2] * v[4];
+                        q6[4][s + 2] = v[3];
+                        q6[5][s + 2] = a;
+                    }
+                    T dd[6];
+#pragma unroll
+                    for (int u = 0; u < 6; ++u) dd[u] = d1fc(q6[u][0], q6[u][1], q6[u][2], q6[u][3], q6[u][4], ax[e], bx[e], cx[e], dx[e]);
+                    o[0][e] = -dd[0]; o[1][e] = -dd[1]; o[2][e] = -dd[2]; o[3][e] = -dd[3];
+                    px[e] = dd[4]; dvv[e] = -dd[5];
+                }
+            }
+            // ---- y ----
+            {
+                T ym[2][NF][VX], yp[2][NF][VX];   // rows -2, -1 and +1, +2
+#pragma unroll
+                for (int f = 0; f < NF; ++f) {
+                    IO::ld(pc + f * SP + me - 2 * RS, ym[0][f]); IO::ld(pc + f * SP + me - RS, ym[1][f]);
+                    IO::ld(pc + f * SP + me + RS, yp[0][f]); IO::ld(pc + f * SP + me + 2 * RS, yp[1][f]);
+                }
+#pragma unroll
+                for (int e = 0; e < VX; ++e) {
+                    T q6[6][5];
+#pragma unroll
+                    for (int s = 0; s < 5; ++s) {
+                        T v[NF];
+#pragma unroll
+                        for (int f = 0; f < NF; ++f)
+                            v[f] = s < 2 ? ym[s][f][e] : (s == 2 ? zq[2][f][e] : yp[s - 3 < 0 ? 0 : s - 3][f][e]);
+                        const T b = v[1] * v[4];
+                        q6[0][s] = v[1];
+                        q6[1][s] = v[0] * v[1] * v[4];
+                        q6[2][s] = v[1] * v[1] * v[4] + v[3];
+                        q6[3][s] = v[1] * v[2] * v[4];
+                        q6[4][s] = v[3];
+                        q6[5][s] = b;
+                    }
+                    T dd[6];
+#pragma unroll
+                    for (int u = 0; u < 6; ++u) dd[u] = d1fc(q6[u][0], q6[u][1], q6[u][2], q6[u][3], q6[u][4], ay, by, cy, dy);
+                    o[0][e] -= dd[0]; o[1][e] -= dd[1]; o[2][e] -= dd[2]; o[3][e] -= dd[3];
+                    py[e] = dd[4]; dvv[e] -= dd[5];
+                }
+            }
+            // ---- z ----
+#pragma unroll
+            for (int e = 0; e < VX; ++e) {
+                T q6[6][5];
+#pragma unroll
+                for (int s = 0; s < 5; ++s) {
+                    const T m1 = zq[s][0][e], m2 = zq[s][1][e], m3 = zq[s][2][e], dp = zq[s][3][e], ri = zq[s][4][e];
+                    q6[0][s] = m3;
+                    q6[1][s] = m1 * m3 * ri;
+                    q6[2][s] = m2 * m3 * ri;
+                    q6[3][s] = m3 * m3 * ri + dp;
+                    q6[4][s] = dp;
+                    q6[5][s] = m3 * ri;
+                }
+                T dd[6];
+#pragma unroll
+                for (int u = 0; u < 6; ++u) dd[u] = d1fc(q6[u][0], q6[u][1], q6[u][2], q6[u][3], q6[u][4], az, bz, cz, dz);
+                o[0][e] -= dd[0]; o[1][e] -= dd[1]; o[2][e] -= dd[2]; o[3][e] -= dd[3];
+                pz[e] = dd[4] + T(g.dzp0[c]); dvv[e] -= dd[5];
+            }
+            // ---- pointwise: J x B - xresd, pressure equation ----
+            const T rsx = T(g.rsx[c]), rsy = T(g.rsy[c]), rsz = T(g.rsz[c]), p0 = T(g.p0[c]);
+            const T bx0 = T(g.bx0[c]), by0 = T(g.by0[c]), bz0 = T(g.bz0[c]);
+#pragma unroll
+            for (int e = 0; e < VX; ++e) {
+                const T B1 = bx0 + b1[e], B2 = by0 + b2[e], B3 = bz0 + b3[e];
+                o[1][e] = o[1][e] - rsx + j2[e] * B3 - j3[e] * B2;
+                o[2][e] = o[2][e] - rsy + j3[e] * B1 - j1[e] * B3;
+                o[3][e] = o[3][e] - rsz + j1[e] * B2 - j2[e] * B1;
+                const T ri = zq[2][4][e];
+                const T v1 = zq[2][0][e] * ri, v2 = zq[2][1][e] * ri, v3 = zq[2][2][e] * ri;
+                const T pcn = p0 + zq[2][3][e];
+                o[4][e] = -px[e] * v1 - py[e] * v2 - pz[e] * v3 + dvv[e] * g.gamma * pcn +
+                          (g.gamma - T(1)) * g.eta * (j1[e] * j1[e] + j2[e] * j2[e] + j3[e] * j3[e]);
+            }
+#pragma unroll
+            for (int m = 0; m < 5; ++m) IO::st(io.out[m] + col + (long)c * g.sz, o[m]);
+            if (c == 2 || c == mz - 3) {
+                const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    T hv[VX], zv[VX];
+#pragma unroll
+                    for (int e = 0; e < VX; ++e) { hv[e] = T(0.5) * o[m][e]; zv[e] = T(0); }
+                    IO::st(io.out[m] + col + (long)kh * g.sz, hv);
+                    IO::st(io.out[m] + col + (long)kz * g.sz, zv);
+                }
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+#pragma unroll
+                for (int e = 0; e < VX; ++e) zq[s][f][e] = zq[s + 1][f][e];
+    }
+    cp_async_wait<0>();
+}
+
+}  // namespace dasha
