@@ -8,6 +8,7 @@
 #include "zpv2.cuh"
 #include "zcurl.cuh"
 #include "zhydro.cuh"
+#include "zeh.cuh"
 #include "adjoint.cuh"
 #include <cuda_runtime.h>
 #include <type_traits>
@@ -535,11 +536,14 @@ public:
         gg.z = (mz + ch - 1) / ch;
         DASHA_LAUNCH(tag, 6.0 * N * sizeof(T), (k_zcurl<T, ZVX, 8, 2, SIGN><<<gg, 256, ZC3c::smem(), st>>>(g, src, out, ch)));
     }
-    // k_zhydro: tile 32*ZVX x ZH_TY, 1 plane in flight beyond c+2.  Measured (hydro ms per step,
-    // FP32 1024x512x1024 / FP64 512x256x512): 8 rows, 1 CTA/SM 57.6 / 16.6; 8 rows capped at 2
-    // CTAs/SM (spills) 73.9 / -; 4 rows, 3 CTAs/SM 60.8 / 12.8; 4 rows, 2 CTAs/SM 57.9 / 14.3
-    static constexpr int ZH_TY = sizeof(T) == 4 ? 8 : 4, ZH_MINB = sizeof(T) == 4 ? 1 : 3;
-    using ZHc = ZH<T, ZVX, ZH_TY, 1>;
+    // k_zhydro: one node per thread, tile 32 x 4, 1 plane in flight beyond c+2, 4 (FP32) or 3
+    // (FP64) CTAs per SM.  Measured (hydro ms per step, FP32 1024x512x1024 / FP64 512x256x512):
+    // float pairs, 8 rows, 1 CTA/SM 57.5 / -; pairs capped at 2 CTAs/SM (spills) 73.9 / -; one
+    // node per thread, 4 rows, 4 CTAs/SM 55.3 / -; 8 rows, 1 CTA/SM - / 16.6; 4 rows, 3 CTAs/SM
+    // 60.8 (pairs) / 12.8; 8 rows capped at 3 CTAs (spills) 66.5 / -
+    static constexpr int ZH_VX = 1, ZH_TY = 4, ZH_MINB = sizeof(T) == 4 ? 4 : 3;
+    using ZHc = ZH<T, ZH_VX, ZH_TY, 1>;
+    using ZEHc = ZEH<T, ZVX, 8, 2>;   // k_zeh: tile 32*ZVX x 8, 2 planes in flight beyond c+2
     using St3 = VStore<T, 3, ZVX>;
     using St4 = VStore<T, 4, ZVX>;
     using Acc3 = VAcc<T, 3, ZVX>;
@@ -564,7 +568,10 @@ public:
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
             return e;
-        if ((e = cudaFuncSetAttribute(k_zhydro<T, ZVX, ZH_TY, 1, ZH_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if ((e = cudaFuncSetAttribute(k_zeh<T, ZVX, 8, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)ZEHc::smem())))
+            return e;
+        if ((e = cudaFuncSetAttribute(k_zhydro<T, ZH_VX, ZH_TY, 1, ZH_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZHc::smem())))
             return e;
         if ((e = cudaFuncSetAttribute(k_zcurl<T, ZVX, 8, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -682,11 +689,21 @@ public:
         T** cother = curF == cur[0] ? cur[1] : cur[0];
         (void)cother;
         // E0 = -v x B + eta J at every node, then avrgE's 4 passes (t3dsdsc.f:1367-1389)
-        DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
+        if (P.hall) {   // E0 and the Hall field in one z-march over the state
+            EHIO<T> eh;
+            eh.drho = xs[0]; eh.m1 = xs[1]; eh.m2 = xs[2]; eh.m3 = xs[3];
+            eh.b1 = xs[4]; eh.b2 = xs[5]; eh.b3 = xs[6]; eh.dp = xs[7];
+            eh.j1 = curF[0]; eh.j2 = curF[1]; eh.j3 = curF[2];
+            for (int q = 0; q < 3; ++q) { eh.e[q] = E[0][q]; eh.h[q] = Hh[0][q]; }
+            dim3 ge((mx + ZEHc::TX - 1) / ZEHc::TX, (my + 7) / 8, 1);
+            int che = zchunk(ge.x * ge.y, 16);
+            ge.z = (mz + che - 1) / che;
+            DASHA_LAUNCH("k_efield_hall", 17.0 * N * sizeof(T), (k_zeh<T, ZVX, 8, 2><<<ge, 256, ZEHc::smem(), st>>>(g, eh, che)));
+        } else {
+            DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
+        }
         Ef = passes3<0u>("k_zpv_E", E[0], E[1], 4);
         if (P.hall) {
-            // plain kernel: faster here than the ring framework (one stencil field, seven pointwise)
-            DASHA_LAUNCH("k_hall", 11.0 * N * sizeof(T), k_hall<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(Hh[0])));
             T** h = passes3<KIND_H>("k_zpv_H", Hh[0], Hh[1], 4);
             Acc3 ea;
             for (int q = 0; q < 3; ++q) { ea.f[q] = Ef[q]; ea.a[q] = Ef[q]; }
@@ -705,7 +722,7 @@ public:
             int chh = zchunk(gh.x * gh.y, 16);
             gh.z = (mz + chh - 1) / chh;
             DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
-                         (k_zhydro<T, ZVX, ZH_TY, 1, ZH_MINB><<<gh, 32 * ZH_TY, ZHc::smem(), st>>>(g, hio, chh)));
+                         (k_zhydro<T, ZH_VX, ZH_TY, 1, ZH_MINB><<<gh, 32 * ZH_TY, ZHc::smem(), st>>>(g, hio, chh)));
         } else {
         SrcFields<T, 5> sh;
         sh.f[0] = xs[0]; sh.f[1] = xs[1]; sh.f[2] = xs[2]; sh.f[3] = xs[3]; sh.f[4] = xs[7];

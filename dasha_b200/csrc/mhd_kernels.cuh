@@ -148,50 +148,6 @@ __global__ void k_efield(Geo<T> g, F8<T> x, F3<T> cur, F3<T> e) {
 }
 
 // ---------------------------------------------------------------------------------------
-// Hall term xdh = di*(J x B - grad p)/rho on interior rows + wall rows (t3dsdsc.f:1404-1423).
-template <class T>
-__global__ void k_hall(Geo<T> g, F8<T> x, F3<T> cur, F3<T> h) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= g.mx) return;
-    int jj = blockIdx.y, k = blockIdx.z;
-    bool zero, half;
-    int ks = wall_src(k, g.mz, zero, half);
-    long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
-    if (zero) { h.f[0][c] = T(0); h.f[1][c] = T(0); h.f[2][c] = T(0); return; }
-    const long q = (long)i + (long)jj * g.sy + (long)ks * g.sz;   // node the row takes its value from
-    // stencil offsets from q (32-bit): direct away from the x and y ends, wrapped near them
-    const int sy = (int)g.sy, sz = (int)g.sz;
-    int xo[4] = {-2, -1, 1, 2}, yo[4] = {-2 * sy, -sy, sy, 2 * sy};
-    if (i < 2 || i > g.mx - 3) {
-        xo[0] = wrapi(i - 2, g.mx) - i; xo[1] = wrapi(i - 1, g.mx) - i;
-        xo[2] = wrapi(i + 1, g.mx) - i; xo[3] = wrapi(i + 2, g.mx) - i;
-    }
-    if (jj < 2 || jj > g.my - 3) {
-        yo[0] = (wrapi(jj - 2, g.my) - jj) * sy; yo[1] = (wrapi(jj - 1, g.my) - jj) * sy;
-        yo[2] = (wrapi(jj + 1, g.my) - jj) * sy; yo[3] = (wrapi(jj + 2, g.my) - jj) * sy;
-    }
-    const T* p = x.f[7] + q;
-    const T p0 = p[0];
-    // grad p = grad(p - p0) + dp0/dz ez.  Of -di dp0/dz / rho, the plane-uniform part
-    // -di dp0/dz / rho0 has an exactly zero discrete curl (the Hall passes keep it uniform in
-    // x and y) and is left out; the rest is di dp0/dz (rho - rho0) / (rho0 rho).  This keeps
-    // an O(1) field out of the FP32 sum that drives dB/dt.
-    const T px = d1fc(p[xo[0]], p[xo[1]], p0, p[xo[2]], p[xo[3]], g.a1x[i], g.b1x[i], g.c1x[i], g.d1x[i]);
-    const T py = d1fc(p[yo[0]], p[yo[1]], p0, p[yo[2]], p[yo[3]], g.a1y[jj], g.b1y[jj], g.c1y[jj], g.d1y[jj]);
-    const T pz = d1fc(p[-2 * sz], p[-sz], p0, p[sz], p[2 * sz], g.a1z[ks], g.b1z[ks], g.c1z[ks], g.d1z[ks]);
-    const T dr = x.f[0][q];
-    T r = T(g.rho0[ks]) + dr;
-    T b1 = T(g.bx0[ks]) + x.f[4][q], b2 = T(g.by0[ks]) + x.f[5][q], b3 = T(g.bz0[ks]) + x.f[6][q];
-    T j1 = cur.f[0][q], j2 = cur.f[1][q], j3 = cur.f[2][q];
-    const T dir = g.di / r;
-    T h1 = (j2 * b3 - j3 * b2 - px) * dir;
-    T h2 = (j3 * b1 - j1 * b3 - py) * dir;
-    T h3 = (j1 * b2 - j2 * b1 - pz + T(g.dzp0r[ks]) * dr) * dir;
-    if (half) { h1 = T(0.5) * h1; h2 = T(0.5) * h2; h3 = T(0.5) * h3; }
-    h.f[0][c] = h1; h.f[1][c] = h2; h.f[2][c] = h3;
-}
-
-// ---------------------------------------------------------------------------------------
 // J0 added to the smoothed J1 (j0_mode FULL).
 template <class T>
 __global__ void k_add_j0(Geo<T> g, F3<T> cur) {
