@@ -553,6 +553,7 @@ public:
         if ((e = zp_attr1<3, 0u, St3>())) return e;
         if ((e = zp_attr1<3, KIND_H, St3>())) return e;
         if ((e = zp_attr1<3, KIND_H, Acc3>())) return e;
+        if ((e = zp_attr1<6, KIND_EH, VSum<T, 3, ZVX>>())) return e;
         if ((e = zp_attr1<4, 0u, St4>())) return e;
         if ((e = zp_attr1<4, KIND_B4, St4>())) return e;
         if ((e = zp_attr1<4, 0u, RK4>())) return e;
@@ -588,6 +589,7 @@ public:
     static constexpr unsigned KIND_X = (2u << 8) | (2u << 10) | (2u << 12);         // B with the x profile
     static constexpr unsigned KIND_B4 = 2u | (2u << 2) | (2u << 4);                 // fields 4..7: B1 B2 B3 p
     static constexpr unsigned KIND_P45 = 2u | (2u << 2);                            // field pair (B1, B2)
+    static constexpr unsigned KIND_EH = (1u << 6) | (1u << 8) | (1u << 10);         // E (radial) then Hall (1/8)
     static constexpr unsigned KIND_P67 = 2u;                                        // field pair (B3, p)
 
     // one avrg/avrgtt pass over the 8 state-like fields, as two 4-field launches (rho, m) and
@@ -702,12 +704,19 @@ public:
         } else {
             DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
         }
-        Ef = passes3<0u>("k_zpv_E", E[0], E[1], 4);
         if (P.hall) {
+            // avrgh passes 1-4, avrgE passes 1-3, then one 6-field launch: the 4th E pass and the
+            // 5th Hall pass, summed into E (the two chains are independent until that sum)
             T** h = passes3<KIND_H>("k_zpv_H", Hh[0], Hh[1], 4);
-            Acc3 ea;
-            for (int q = 0; q < 3; ++q) { ea.f[q] = Ef[q]; ea.a[q] = Ef[q]; }
-            zp<3, KIND_H>("k_zpv_H5acc", 9.0 * N * sizeof(T), src3(h), ea);   // 5th pass added into E
+            T** e3 = passes3<0u>("k_zpv_E", E[0], E[1], 3);
+            T** eo = e3 == E[0] ? E[1] : E[0];
+            SrcFields<T, 6> se;
+            VSum<T, 3, ZVX> es;
+            for (int q = 0; q < 3; ++q) { se.f[q] = e3[q]; se.f[3 + q] = h[q]; es.f[q] = eo[q]; }
+            zp<6, KIND_EH>("k_zpv_EH", 9.0 * N * sizeof(T), se, es);
+            Ef = eo;
+        } else {
+            Ef = passes3<0u>("k_zpv_E", E[0], E[1], 4);
         }
         // right-hand side: hydro part (xdif 0..3, 7) and induction (xdif 4..6)
         dim3 gg(mx / ZTX, (my + 7) / 8, 1);

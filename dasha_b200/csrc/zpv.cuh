@@ -84,6 +84,25 @@ struct VAcc {   // f = a + v  (a may alias f: each node is read and written by o
     }
 };
 
+// f = v[q] + v[q + NO]: the pass over 2 NO fields writes the sums of the two halves (the last E
+// smoothing pass and the fifth Hall pass, added into E, in one launch)
+template <class T, int NO, int VX>
+struct VSum {
+    T* f[NO];
+    struct Pre {};
+    __device__ __forceinline__ void pre(long, Pre&) const {}
+    __device__ __forceinline__ void store(long i, const T (&v)[2 * NO][VX], const Pre&) const { wall(i, v); }
+    __device__ __forceinline__ void wall(long i, const T (&v)[2 * NO][VX]) const {
+#pragma unroll
+        for (int q = 0; q < NO; ++q) {
+            T w[VX];
+#pragma unroll
+            for (int e = 0; e < VX; ++e) w[e] = v[q][e] + v[q + NO][e];
+            VIO<T, VX>::st(f[q] + i, w);
+        }
+    }
+};
+
 // RK4 stage update with the smoothed xdif (stepon t3dsdsc.f:1090-1132): plain registers
 // (base, acc = xm, x) in FP64; in FP32 acc holds only the increment and the base update of
 // stage 4 is a Kahan step with the compensation comp (value = x - comp).
