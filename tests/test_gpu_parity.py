@@ -16,6 +16,9 @@ pytestmark = pytest.mark.gpu
 
 SMALL = harris.RunConfig("small-32x16x32", 32, 16, 32, False, 0.005, 0.5, 4)
 SMALL_S = harris.RunConfig("small-32x16x40-sinh", 32, 16, 40, True, 0.003, 1.0, 4)
+# ragged tiles: mx not a multiple of the 64-node FP32 tile, my not a multiple of the 8 or 4
+# rows of a CTA, two z chunks of 18 planes
+RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 4, dt_whistler=1)
 
 
 def rel_err(a, b):
@@ -38,14 +41,14 @@ def test_state_roundtrip(cfg):
     assert rel_err(d.get_state(), o.get_state()).max() < 1e-15
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED], ids=lambda c: c.name)
 def test_current_parity(cfg):
     o, d = pair(cfg)
     e = rel_err(d.current(), o.current())
     assert e.max() < 1e-11, e
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, harris.CONFIGS["c0"]], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, harris.CONFIGS["c0"], RAGGED], ids=lambda c: c.name)
 @pytest.mark.parametrize("t", [0.0, 0.5])
 def test_rhs_parity(cfg, t):
     o, d = pair(cfg)
@@ -95,7 +98,7 @@ def test_setdt_parity_whistler_option():
     assert d.setdt() < 0.5 * plain
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED], ids=lambda c: c.name)
 def test_steps_parity(cfg):
     o, d = pair(cfg)
     t = 0.0
@@ -135,8 +138,8 @@ def test_diagnostics_parity(cfg):
 SMALL_SW = harris.RunConfig("small-32x16x40-sinh-whistler", 32, 16, 40, True, 0.003, 1.0, 4, dt_whistler=1)
 
 
-@pytest.mark.parametrize("cfg,steps", [(harris.CONFIGS["c0"], 200), (SMALL_SW, 300)],
-                         ids=["c0-200", "sinh-whistler-300"])
+@pytest.mark.parametrize("cfg,steps", [(harris.CONFIGS["c0"], 200), (SMALL_SW, 300), (RAGGED, 200)],
+                         ids=["c0-200", "sinh-whistler-300", "ragged-200"])
 def test_fp32_path_close_to_fp64(cfg, steps):
     """FP32 perturbation + Kahan RK4 + compensated filter against the FP64 path on the same dt
     sequence: every field within 1e-6 relative L2 (measured: <= 1.4e-7).  The di = 1 stretched
