@@ -586,7 +586,6 @@ public:
     static SrcFields<T, 8> src8(T* const* p) { SrcFields<T, 8> s; for (int q = 0; q < 8; ++q) s.f[q] = p[q]; return s; }
     static St3 st3(T* const* p) { St3 s; for (int q = 0; q < 3; ++q) s.f[q] = p[q]; return s; }
     static constexpr unsigned KIND_H = 1u | (1u << 2) | (1u << 4);                 // 1/8 for 3 fields
-    static constexpr unsigned KIND_X = (2u << 8) | (2u << 10) | (2u << 12);         // B with the x profile
     static constexpr unsigned KIND_B4 = 2u | (2u << 2) | (2u << 4);                 // fields 4..7: B1 B2 B3 p
     static constexpr unsigned KIND_P45 = 2u | (2u << 2);                            // field pair (B1, B2)
     static constexpr unsigned KIND_EH = (1u << 6) | (1u << 8) | (1u << 10);         // E (radial) then Hall (1/8)
@@ -953,7 +952,7 @@ public:
             for (int m = 0; m < 3; ++m) cudaMemcpyAsync(w.e0[m], w.et[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
             T** eb = adj_passes(w.e0, w.e1, 3, 4, 0u, false);
             T** hb = nullptr;
-            if (P.hall) {   // Hall chain: 5 transposed avrgh passes, then the rows of k_hall folded
+            if (P.hall) {   // Hall chain: 5 transposed avrgh passes, then the rows of the Hall field (k_zeh) folded
                 for (int m = 0; m < 3; ++m) cudaMemcpyAsync(w.h0[m], w.et[m], sizeof(T) * N, cudaMemcpyDeviceToDevice, st);
                 hb = adj_passes(w.h0, w.h1, 3, 5, KIND_H, true);
             }
