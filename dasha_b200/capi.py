@@ -61,6 +61,15 @@ SIGNATURES = {
     "dasha_profile": ([_P, C.c_int], C.c_int),
     "dasha_profile_read": ([_P, C.POINTER(C.c_int), C.c_char_p, _D, C.POINTER(C.c_long), _D], C.c_int),
     "dasha_current_noalloc": ([C.POINTER(GridC), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "dasha_midplane": ([_P, _D], C.c_int),
+    "dasha_restart_write": ([C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                             _D, C.c_long, C.c_long, C.c_long], C.c_int),
+    "dasha_restart_read": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, C.POINTER(C.c_int),
+                            C.c_int, C.c_int, C.c_int, _D, C.c_long, C.c_long], C.c_int),
+    "dasha_m2d_write": ([C.c_char_p, C.c_int, C.c_int, C.c_double, _D, _D, _D], C.c_int),
+    "dasha_midplane_host": ([C.c_int, C.c_int, C.c_int, _D, _D, C.c_long, C.c_long, _D], C.c_int),
+    "dasha_m3d_write": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, _D, _D, _D,
+                         C.c_long, C.c_long], C.c_int),
     "dasha_last_error": ([_P], C.c_char_p),
     "dasha_destroy": ([_P], None),
 }
@@ -174,6 +183,13 @@ class Dasha:
         H = harris.to_halo(np.zeros((3, self.mz, self.my, self.mx)))
         self._check(self.lib.dasha_current(self.h, _dp(H), H.shape[3], H.shape[2]))
         return harris.from_halo(H, self.mx, self.my, self.mz)
+
+    def midplane(self) -> np.ndarray:
+        """The eleven output fields of the reference's m2d file on the plane j = my/2,
+        (11, mz, mx): rho, v, B, p, J (recrd2, t3dsdsc.f:4965-5113)."""
+        out = np.zeros((11, self.mz, self.mx))
+        self._check(self.lib.dasha_midplane(self.h, _dp(out)))
+        return out
 
     def rhs(self, t: float) -> np.ndarray:
         H = harris.to_halo(np.zeros((8, self.mz, self.my, self.mx)))

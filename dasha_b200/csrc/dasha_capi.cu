@@ -253,6 +253,13 @@ int dasha_current(dasha_ctx* c, double* cur_f, long ld1, long ld2) {
     return from_status(c, c->eng->current(cur_f, ld1, ld2));
 }
 
+int dasha_midplane(dasha_ctx* c, double* plane) {
+    CAPI_GUARD(c);
+    if (!plane) return fail(c, DASHA_E_INVALID, "null plane");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return from_status(c, c->eng->midplane(plane));
+}
+
 int dasha_rhs(dasha_ctx* c, double t, double* xdif_f, long ld1, long ld2) {
     CAPI_GUARD(c);
     if (int rc = check_ld(c, xdif_f, ld1, ld2)) return rc;

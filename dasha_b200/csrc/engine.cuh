@@ -81,6 +81,7 @@ struct EngineBase {
     virtual Status setdt(double* dt, int* blowup) = 0;
     virtual Status stepon(double time, double dt, int nstep) = 0;
     virtual Status current(double* cur, long ld1, long ld2) = 0;
+    virtual Status midplane(double* out) = 0;
     virtual Status rhs(double t, double* xdif, long ld1, long ld2) = 0;
     virtual Status diagnostics(double* out) = 0;
     virtual Status adjoint_flux_grad(int nsteps, const double* dt_seq, int snaps, double* deta, double* dpsi) = 0;
@@ -107,6 +108,8 @@ template <class T>
 __global__ void k_import_chunk(int mx, int my, int k0, const double* src, const double* eqprof, T* dst);
 template <class T>
 __global__ void k_export_chunk(int mx, int my, int k0, const T* src, const T* comp, const double* eqprof, double* dst);
+template <class T>
+__global__ void k_midplane(Geo<T> g, int j, F8<T> x, F8<T> comp, F3<T> cur, double* out);
 template <class T>
 inline const double* eq_profile(const Geo<T>& g, int m);
 
@@ -139,6 +142,7 @@ public:
     double* cfltab = nullptr;    // CFL rate tables: ich[mx+my+mz], vv[..], ih[..]
     int* flag = nullptr;         // blow-up flag
     double* hpin = nullptr;      // pinned host scratch
+    double* mpd = nullptr;       // the 11 mid-plane output fields (allocated on first use)
     Geo<T> g{};
     // FP64 device pointers for setdt / diagnostics
     const double *xc, *yc, *zc, *dxs, *dys, *dzs, *wx, *wy, *wz;
@@ -157,6 +161,7 @@ public:
         if (cfltab) cudaFree(cfltab);
         if (flag) cudaFree(flag);
         if (hpin) cudaFreeHost(hpin);
+        if (mpd) cudaFree(mpd);
     }
 
     Status init(int mx_, int my_, int mz_, const dasha_params_c& p, cudaStream_t st_, const HostTables& H) {
@@ -840,6 +845,21 @@ public:
         return transfer_out(curh, ld1, ld2, curF, 3, false);
     }
 
+    // The fields of the reference's 2-D output (recrd2, t3dsdsc.f:4965-5113) on the plane
+    // j = my/2: one kernel gathers them from the state and the freshly smoothed current, and
+    // only mx*mz*11 values cross to the host.
+    Status midplane(double* outh) override {
+        if (!mpd) DASHA_CK(cudaMalloc(&mpd, sizeof(double) * 11 * (size_t)mx * mz));
+        launch_current(X);
+        F8<T> cz;
+        for (int m = 0; m < 8; ++m) cz.f[m] = KAHAN ? C[m] : nullptr;
+        k_midplane<T><<<dim3((mx + 127) / 128, mz), 128, 0, st>>>(g, my / 2, f8(X), cz, f3(curF), mpd);
+        DASHA_CK(cudaGetLastError());
+        DASHA_CK(cudaMemcpyAsync(outh, mpd, sizeof(double) * 11 * (size_t)mx * mz, cudaMemcpyDeviceToHost, st));
+        DASHA_CK(cudaStreamSynchronize(st));
+        return Status::ok();
+    }
+
     Status rhs(double t, double* xdif, long ld1, long ld2) override {
         T* out[8];
         for (int m = 0; m < 8; ++m) out[m] = S[m];
@@ -1176,6 +1196,31 @@ __global__ void k_export_chunk(int mx, int my, int k0, const T* src, const T* co
     if (comp) v -= (double)comp[n];   // compensated FP32 state: the value is x - comp
     if (eqprof) v += eqprof[k];
     dst[(long)i + (long)mx * (j + (long)my * blockIdx.z)] = v;
+}
+
+// out[q][k][i], q = rho, (rho v)/rho, B, p (FP64 totals, formed as k_export_chunk forms them),
+// then the current density; one thread per (i, k) on the plane j
+template <class T>
+__global__ void k_midplane(Geo<T> g, int j, F8<T> x, F8<T> comp, F3<T> cur, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, k = blockIdx.y;
+    if (i >= g.mx) return;
+    const long n = (long)i + (long)g.mx * (j + (long)g.my * k);
+    const long np = (long)g.mx * g.mz, o = (long)i + (long)g.mx * k;
+    const double* prof[8] = {g.rho0, nullptr, nullptr, nullptr, g.bx0, g.by0, g.bz0, g.p0};
+    double v[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        v[m] = (double)x.f[m][n];
+        if (comp.f[m]) v[m] -= (double)comp.f[m][n];
+        if (prof[m]) v[m] += prof[m][k];
+    }
+    out[o] = v[0];
+#pragma unroll
+    for (int m = 1; m < 4; ++m) out[m * np + o] = v[m] / v[0];
+#pragma unroll
+    for (int m = 4; m < 8; ++m) out[m * np + o] = v[m];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) out[(8 + m) * np + o] = (double)cur.f[m][n];
 }
 
 template <class T>

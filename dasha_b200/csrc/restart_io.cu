@@ -1,0 +1,357 @@
+// Host-side files of the reference's output routines, for drivers other than the Fortran main
+// program (which keeps its own recrd / recrd2 / recrd3 / readin on the host arrays that
+// dasha_get_state and dasha_current fill).
+//
+//  - Restart file mhdNNNRRR (recrd / readin, t3dsdsc.f:4814-4861): Fortran unformatted
+//    sequential, two records: (ncase, nstep: INTEGER*4; time: REAL*8; nst: INTEGER*4) and the
+//    whole array x(mxpr, my, mzpr, 8) of REAL*8 (mhd02.for:4; implicit real*8 (a-h,o-z), so
+//    names in i-n are INTEGER*4), native byte order.  Record framing as gfortran writes it:
+//    each record is one or more subrecords, each a 4-byte signed length, the data and the same
+//    length again; the leading length is negative when another subrecord of the record
+//    follows, the trailing one when another precedes; a subrecord holds at most 2147483639
+//    bytes.
+//  - 2-D mid-plane file m2dNNN.dat (recrd2, t3dsdsc.f:5116-5154) and 3-D file m3dNNN (recrd3,
+//    t3dsdsc.f:5365-5402): list-directed lines "2 mx mz" (or "3 mx my mz") and "time", then the
+//    node coordinates (x, z or x, y, z) as one output list, then for q = 1..11 a list-directed
+//    line "q" and field q, x fastest, with the edit descriptors 5(1X,E14.5E3) (m2d) or
+//    11(1X,E10.4) (m3d), a new line after every 5 or 11 numbers and at the end of each list.
+//    Fields: 1 rho, 2-4 v = (rho v)/rho, 5-7 B, 8 p (totals), 9-11 the current density; m2d
+//    holds the plane j = my/2 (0-based; nyh = my/2+1 in the reference).
+#include "dasha_capi.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr long kMaxSub = 2147483639L;   // gfortran's longest subrecord
+
+// Streams one logical record of known length as subrecords of at most maxsub bytes.
+struct RecWriter {
+    FILE* f;
+    long total, maxsub, done = 0, left_in_sub = 0, cur_open_len = 0;
+    bool ok = true, first = true;
+    RecWriter(FILE* f_, long total_, long maxsub_) : f(f_), total(total_), maxsub(maxsub_) {
+        if (total == 0) { open_sub(); close_sub(); }
+    }
+    void marker(int32_t v) { ok = ok && std::fwrite(&v, 4, 1, f) == 1; }
+    void open_sub() {
+        cur_open_len = std::min(total - done, maxsub);
+        left_in_sub = cur_open_len;
+        marker(done + cur_open_len < total ? -(int32_t)cur_open_len : (int32_t)cur_open_len);
+    }
+    void close_sub() {
+        marker(first ? (int32_t)cur_open_len : -(int32_t)cur_open_len);
+        first = false;
+    }
+    void put(const void* data, long n) {
+        const char* p = static_cast<const char*>(data);
+        while (n > 0 && ok) {
+            if (done >= total) { ok = false; break; }   // more data than the record holds
+            if (left_in_sub == 0) open_sub();
+            const long m = std::min(n, left_in_sub);
+            ok = ok && std::fwrite(p, 1, (size_t)m, f) == (size_t)m;
+            p += m; n -= m; done += m; left_in_sub -= m;
+            if (left_in_sub == 0) close_sub();
+        }
+    }
+    bool finish() const { return ok && done == total && left_in_sub == 0; }
+};
+
+// Reads one logical record that must hold exactly `total` bytes, subrecord by subrecord.
+struct RecReader {
+    FILE* f;
+    long total, done = 0, left_in_sub = 0, sub_len = 0;
+    bool ok = true, first = true, more = true;
+    RecReader(FILE* f_, long total_) : f(f_), total(total_) {
+        if (total == 0) { open_sub(); close_sub(); }
+    }
+    int32_t marker() {
+        int32_t v = 0;
+        ok = ok && std::fread(&v, 4, 1, f) == 1;
+        return v;
+    }
+    void open_sub() {
+        if (!more) { ok = false; return; }
+        const int32_t h = marker();
+        more = h < 0;
+        sub_len = more ? -(long)h : (long)h;
+        left_in_sub = sub_len;
+        if (done + sub_len > total) ok = false;
+    }
+    void close_sub() {
+        const int32_t t = marker();
+        if ((first ? (long)t : -(long)t) != sub_len) ok = false;
+        first = false;
+    }
+    void get(void* out, long n) {
+        char* p = static_cast<char*>(out);
+        while (n > 0 && ok) {
+            while (left_in_sub == 0 && ok) {   // zero-length subrecords carry nothing
+                open_sub();
+                if (ok && left_in_sub == 0) close_sub();
+            }
+            if (!ok) break;
+            const long m = std::min(n, left_in_sub);
+            ok = ok && std::fread(p, 1, (size_t)m, f) == (size_t)m;
+            p += m; n -= m; done += m; left_in_sub -= m;
+            if (left_in_sub == 0) close_sub();
+        }
+    }
+    bool finish() const { return ok && done == total && !more && left_in_sub == 0; }
+};
+
+// Fortran Ew.d (edig = 0) or Ew.dEe output editing of v at scale factor 0, as gfortran writes it:
+// [-][0].d1..dd followed by E+xx (Ew.d, |exponent| <= 99), +xxx (Ew.d, 99 < |exponent| <= 999)
+// or E+ and edig digits; the optional zero before the point is written when the width has
+// room; a field that does not fit is w asterisks.  Writes exactly w characters, no terminator.
+void fmt_e(char* out, double v, int w, int d, int edig) {
+    char body[64];
+    const bool neg = std::signbit(v);
+    if (std::isnan(v) || std::isinf(v)) {
+        const char* s = std::isnan(v) ? "NaN" : (neg ? (w >= 9 ? "-Infinity" : "-Inf") : (w >= 8 ? "Infinity" : "Inf"));
+        const int n = (int)std::strlen(s);
+        if (n > w) { std::memset(out, '*', w); return; }
+        std::memset(out, ' ', w - n);
+        std::memcpy(out + w - n, s, n);
+        return;
+    }
+    char digits[32];
+    int e = 0;
+    if (v == 0.0) {
+        std::memset(digits, '0', d);
+    } else {
+        char s[48];
+        std::snprintf(s, sizeof s, "%.*e", d - 1, std::fabs(v));   // d.dd..de+XX: d significant digits
+        digits[0] = s[0];
+        if (d > 1) std::memcpy(digits + 1, s + 2, d - 1);
+        e = std::atoi(std::strchr(s, 'e') + 1) + 1;                 // 0.d1..dd x 10^e
+    }
+    const int ae = e < 0 ? -e : e;
+    char ex[16];
+    if (edig == 0) {
+        if (ae <= 99) std::snprintf(ex, sizeof ex, "E%c%02d", e < 0 ? '-' : '+', ae);
+        else if (ae <= 999) std::snprintf(ex, sizeof ex, "%c%03d", e < 0 ? '-' : '+', ae);
+        else { std::memset(out, '*', w); return; }
+    } else {
+        int lim = 1;
+        for (int q = 0; q < edig; ++q) lim *= 10;
+        if (ae >= lim) { std::memset(out, '*', w); return; }
+        std::snprintf(ex, sizeof ex, "E%c%0*d", e < 0 ? '-' : '+', edig, ae);
+    }
+    const int nex = (int)std::strlen(ex);
+    const int need = (neg ? 1 : 0) + 1 + d + nex;   // without the optional zero
+    if (need > w) { std::memset(out, '*', w); return; }
+    int n = 0;
+    if (neg) body[n++] = '-';
+    if (need + 1 <= w) body[n++] = '0';
+    body[n++] = '.';
+    std::memcpy(body + n, digits, d);
+    n += d;
+    std::memcpy(body + n, ex, nex);
+    n += nex;
+    std::memset(out, ' ', w - n);
+    std::memcpy(out + w - n, body, n);
+}
+
+// One output list under the format r(1X,Ew.d[Ee]): records of r items; `value(n)` gives item n.
+// Blocks of lines are formatted in parallel and written in order.
+template <class F>
+bool write_list(FILE* f, long count, int per_line, int w, int d, int edig, F value) {
+    const long nlines = (count + per_line - 1) / per_line;
+    const int lw = per_line * (w + 1) + 1;
+    const long block = 1L << 14;   // lines per block
+    const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::string> buf(nt);
+    for (long l0 = 0; l0 < nlines; l0 += block * nt) {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) {
+            th.emplace_back([&, t]() {
+                std::string& s = buf[t];
+                s.clear();
+                const long a = l0 + (long)t * block, b = std::min(nlines, a + block);
+                if (a >= b) return;
+                s.resize((size_t)(b - a) * lw);
+                char* p = &s[0];
+                for (long l = a; l < b; ++l) {
+                    const long n0 = l * per_line, n1 = std::min(count, n0 + per_line);
+                    for (long n = n0; n < n1; ++n) {
+                        *p++ = ' ';
+                        fmt_e(p, value(n), w, d, edig);
+                        p += w;
+                    }
+                    *p++ = '\n';
+                }
+                s.resize((size_t)(p - &s[0]));
+            });
+        }
+        for (auto& x : th) x.join();
+        for (unsigned t = 0; t < nt; ++t)
+            if (!buf[t].empty() && std::fwrite(buf[t].data(), 1, buf[t].size(), f) != buf[t].size()) return false;
+    }
+    return true;
+}
+
+// list-directed lines: integers in 12 columns, a REAL*8 as " " + 17 significant digits
+void ld_ints(FILE* f, const int* v, int n) {
+    for (int q = 0; q < n; ++q) std::fprintf(f, " %11d", v[q]);
+    std::fputc('\n', f);
+}
+void ld_real(FILE* f, double v) { std::fprintf(f, " %24.16E\n", v); }
+
+inline long hidx(long ld1, long ld2, int mz, int i, int j, int k, int m) {
+    return (long)(i + 2) + ld1 * ((long)j + ld2 * ((long)(k + 2) + (long)(mz + 4) * m));
+}
+
+// value of m2d/m3d field q (0..10) at node (i,j,k) from the state and current arrays
+inline double out_field(const double* x_f, const double* cur_f, long ld1, long ld2, int mz, int q, int i, int j,
+                        int k) {
+    if (q >= 8) return cur_f[hidx(ld1, ld2, mz, i, j, k, q - 8)];
+    const double v = x_f[hidx(ld1, ld2, mz, i, j, k, q)];
+    return (q >= 1 && q <= 3) ? v / x_f[hidx(ld1, ld2, mz, i, j, k, 0)] : v;
+}
+
+bool dims_ok(int mx, int my, int mz, long ld1, long ld2) {
+    return mx > 0 && my > 0 && mz > 0 && ld1 >= mx + 4 && ld2 >= my;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dasha_restart_write(const char* path, int ncase, int nstep, double time, int nst, int mx, int my, int mz,
+                        const double* x_f, long ld1, long ld2, long max_subrecord) {
+    if (!path || !x_f || !dims_ok(mx, my, mz, ld1, ld2) || max_subrecord < 0) return DASHA_E_INVALID;
+    const long maxsub = max_subrecord == 0 ? kMaxSub : std::min(max_subrecord, kMaxSub);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return DASHA_E_INVALID;
+    bool ok = true;
+    {
+        unsigned char hdr[20];
+        const int32_t a = ncase, b = nstep, d = nst;
+        std::memcpy(hdr, &a, 4);
+        std::memcpy(hdr + 4, &b, 4);
+        std::memcpy(hdr + 8, &time, 8);
+        std::memcpy(hdr + 16, &d, 4);
+        RecWriter w(f, 20, maxsub);
+        w.put(hdr, 20);
+        ok = w.finish();
+    }
+    if (ok) {
+        const long row = mx + 4, nrow = (long)my * (mz + 4) * 8;
+        RecWriter w(f, (long)sizeof(double) * row * nrow, maxsub);
+        if (ld1 == row && ld2 == my) {
+            w.put(x_f, (long)sizeof(double) * row * nrow);
+        } else {
+            for (int m = 0; m < 8 && w.ok; ++m)
+                for (int kk = 0; kk < mz + 4 && w.ok; ++kk)
+                    for (int j = 0; j < my; ++j)
+                        w.put(x_f + ld1 * ((long)j + ld2 * ((long)kk + (long)(mz + 4) * m)), (long)sizeof(double) * row);
+        }
+        ok = w.finish();
+    }
+    const bool closed = std::fclose(f) == 0;
+    return ok && closed ? DASHA_OK : DASHA_E_INVALID;
+}
+
+int dasha_restart_read(const char* path, int* ncase, int* nstep, double* time, int* nst, int mx, int my, int mz,
+                       double* x_f, long ld1, long ld2) {
+    if (!path || !ncase || !nstep || !time || !nst || !x_f || !dims_ok(mx, my, mz, ld1, ld2)) return DASHA_E_INVALID;
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return DASHA_E_INVALID;
+    unsigned char hdr[20];
+    bool ok;
+    {
+        RecReader r(f, 20);
+        r.get(hdr, 20);
+        ok = r.finish();
+    }
+    if (ok) {
+        const long row = mx + 4, nrow = (long)my * (mz + 4) * 8;
+        RecReader r(f, (long)sizeof(double) * row * nrow);
+        if (ld1 == row && ld2 == my) {
+            r.get(x_f, (long)sizeof(double) * row * nrow);
+        } else {
+            for (int m = 0; m < 8 && r.ok; ++m)
+                for (int kk = 0; kk < mz + 4 && r.ok; ++kk)
+                    for (int j = 0; j < my; ++j)
+                        r.get(x_f + ld1 * ((long)j + ld2 * ((long)kk + (long)(mz + 4) * m)), (long)sizeof(double) * row);
+        }
+        ok = r.finish();
+    }
+    std::fclose(f);
+    if (!ok) return DASHA_E_INVALID;
+    int32_t a, b, d;
+    std::memcpy(&a, hdr, 4);
+    std::memcpy(&b, hdr + 4, 4);
+    std::memcpy(time, hdr + 8, 8);
+    std::memcpy(&d, hdr + 16, 4);
+    *ncase = a;
+    *nstep = b;
+    *nst = d;
+    return DASHA_OK;
+}
+
+int dasha_m2d_write(const char* path, int mx, int mz, double time, const double* xc, const double* zc,
+                    const double* plane) {
+    if (!path || mx <= 0 || mz <= 0 || !xc || !zc || !plane) return DASHA_E_INVALID;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return DASHA_E_INVALID;
+    const int hdr[3] = {2, mx, mz};
+    ld_ints(f, hdr, 3);
+    ld_real(f, time);
+    bool ok = write_list(f, (long)mx + mz, 5, 14, 5, 3, [&](long n) { return n < mx ? xc[n] : zc[n - mx]; });
+    const long np = (long)mx * mz;
+    for (int q = 0; q < 11 && ok; ++q) {
+        const int iq = q + 1;
+        ld_ints(f, &iq, 1);
+        const double* p = plane + (size_t)q * np;
+        ok = write_list(f, np, 5, 14, 5, 3, [&](long n) { return p[n]; });
+    }
+    ok = ok && !std::ferror(f);
+    return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
+}
+
+int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const double* xc, const double* yc,
+                    const double* zc, const double* x_f, const double* cur_f, long ld1, long ld2) {
+    if (!path || !xc || !yc || !zc || !x_f || !cur_f || !dims_ok(mx, my, mz, ld1, ld2)) return DASHA_E_INVALID;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return DASHA_E_INVALID;
+    const int hdr[4] = {3, mx, my, mz};
+    ld_ints(f, hdr, 4);
+    ld_real(f, time);
+    bool ok = write_list(f, (long)mx + my + mz, 11, 10, 4, 0, [&](long n) {
+        return n < mx ? xc[n] : (n < (long)mx + my ? yc[n - mx] : zc[n - mx - my]);
+    });
+    const long mxy = (long)mx * my, nv = mxy * mz;
+    for (int q = 0; q < 11 && ok; ++q) {
+        const int iq = q + 1;
+        ld_ints(f, &iq, 1);
+        ok = write_list(f, nv, 11, 10, 4, 0, [&](long n) {
+            const int i = (int)(n % mx), j = (int)((n / mx) % my), k = (int)(n / mxy);
+            return out_field(x_f, cur_f, ld1, ld2, mz, q, i, j, k);
+        });
+    }
+    ok = ok && !std::ferror(f);
+    return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
+}
+
+int dasha_midplane_host(int mx, int my, int mz, const double* x_f, const double* cur_f, long ld1, long ld2,
+                        double* plane) {
+    if (!x_f || !cur_f || !plane || !dims_ok(mx, my, mz, ld1, ld2)) return DASHA_E_INVALID;
+    const int j = my / 2;
+    const long np = (long)mx * mz;
+    for (int q = 0; q < 11; ++q)
+        for (int k = 0; k < mz; ++k)
+            for (int i = 0; i < mx; ++i) plane[q * np + i + (long)mx * k] = out_field(x_f, cur_f, ld1, ld2, mz, q, i, j, k);
+    return DASHA_OK;
+}
+
+}  // extern "C"

@@ -107,6 +107,12 @@ int dasha_stepon(dasha_ctx* ctx, double time, double dt, int nstep);
  * t3dsdsc.f:2452-2500), same layout rules as the state. */
 int dasha_current(dasha_ctx* ctx, double* cur_f, long ld1, long ld2);
 
+/* The eleven fields of the reference's 2-D output on the mid-y plane j = my/2 (0-based; nyh =
+ * my/2+1 in recrd2, t3dsdsc.f:4965-5113), with the smoothed current of the current state:
+ * plane[q*mx*mz + i + mx*k] for q = 0 rho, 1-3 v = (rho v)/rho, 4-6 B, 7 p (totals), 8-10 J.
+ * Only this plane crosses to the host; dasha_m2d_write formats it. */
+int dasha_midplane(dasha_ctx* ctx, double* plane);
+
 /* One right-hand side xdif(mxpr,my,mzpr,8) = dx/dt of the current state at stage time t
  * (right, t3dsdsc.f:1297-1673); the xdif smoothing avrg runs only when t != 0. */
 int dasha_rhs(dasha_ctx* ctx, double t, double* xdif_f, long ld1, long ld2);
@@ -162,6 +168,43 @@ int dasha_profile_read(dasha_ctx* ctx, int* n, char* names, double* ms, long* la
 #define DASHA_NOALLOC_MAX_AXIS 4096
 #define DASHA_NOALLOC_SCRATCH_DOUBLES (3L * DASHA_NOALLOC_MAX_CELLS + 3L * 7 * DASHA_NOALLOC_MAX_AXIS)
 int dasha_current_noalloc(const dasha_grid_c* grid, const double* db_dev, double* cur_dev, void* stream);
+
+/* Host-side files of the reference's output routines (no context, no GPU).  Each returns
+ * DASHA_OK or DASHA_E_INVALID (bad argument, an I/O error, or a file that does not match).
+ *
+ * Restart file mhdNNNRRR, the reference's file name for step index nst and rank RRR (000 at the
+ * 1x1 process grid): recrd writes it and readin reads it (t3dsdsc.f:4814-4861).  Fortran
+ * unformatted sequential, native byte order, gfortran's record markers (4-byte lengths around
+ * subrecords of at most 2147483639 bytes; a longer record is split into subrecords, the
+ * leading length negative while more follow, the trailing one negative after the first).
+ * Record 1: ncase, nstep (INTEGER*4), time (REAL*8), nst (INTEGER*4).  Record 2: the whole
+ * array x(mx+4, my, mz+4, 8), halo entries included, taken from (read into) an array with
+ * leading dimensions ld1 >= mx+4, ld2 >= my as in dasha_get_state.  max_subrecord: 0 for
+ * gfortran's limit, or a smaller subrecord length.  The reader accepts any subrecord split and
+ * rejects a record whose length is not the expected one. */
+int dasha_restart_write(const char* path, int ncase, int nstep, double time, int nst, int mx, int my, int mz,
+                        const double* x_f, long ld1, long ld2, long max_subrecord);
+int dasha_restart_read(const char* path, int* ncase, int* nstep, double* time, int* nst, int mx, int my, int mz,
+                       double* x_f, long ld1, long ld2);
+
+/* ASCII mid-plane file m2dNNN.dat of recrd2 (t3dsdsc.f:5116-5154): list-directed lines
+ * "2 mx mz" and time, the coordinates x[mx] then z[mz] as one list, then for q = 1..11 a line
+ * "q" and plane field q-1 (the layout dasha_midplane returns), all lists in the format
+ * 5(1X,E14.5E3). */
+int dasha_m2d_write(const char* path, int mx, int mz, double time, const double* x, const double* z,
+                    const double* plane);
+
+/* The same eleven fields as dasha_midplane, gathered on the host from a state array and a
+ * current array in the dasha_get_state / dasha_current layout. */
+int dasha_midplane_host(int mx, int my, int mz, const double* x_f, const double* cur_f, long ld1, long ld2,
+                        double* plane);
+
+/* ASCII 3-D file m3dNNN of recrd3 (t3dsdsc.f:5365-5402): "3 mx my mz", time, x, y, z as one
+ * list, then for q = 1..11 a line "q" and field q on all nodes (x fastest, then y, then z),
+ * the fields of dasha_midplane formed from the state x_f and the current cur_f (layouts of
+ * dasha_get_state / dasha_current), all lists in the format 11(1X,E10.4). */
+int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const double* x, const double* y,
+                    const double* z, const double* x_f, const double* cur_f, long ld1, long ld2);
 
 const char* dasha_last_error(dasha_ctx* ctx);
 void dasha_destroy(dasha_ctx* ctx);

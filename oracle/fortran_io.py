@@ -1,0 +1,147 @@
+"""TEST INFRASTRUCTURE ONLY: a pure-Python restatement of the reference's restart and output
+files, used by tests/ to check libdasha.so's writers and readers; never imported by the
+product.  Parity unpinned: no Fortran compiler and no file written by the reference exist
+here, so the formats follow the reference's WRITE statements, the Fortran rules for
+unformatted records and for E editing, and gfortran's published record layout.
+
+* restart (recrd / readin, t3dsdsc.f:4814-4861): records (ncase, nstep, time, nst) and x; each
+  record is gfortran subrecords: int32 length, data, int32 length; the leading length negated
+  when another subrecord follows, the trailing one negated when one precedes.
+* m2d / m3d (recrd2 t3dsdsc.f:5116-5154, recrd3 t3dsdsc.f:5365-5402): list-directed header
+  lines (written here as the library writes them: integers in 12 columns, the time with 17
+  significant digits), then lists under 5(1X,E14.5E3) or 11(1X,E10.4).
+* the eleven output fields (t3dsdsc.f:5009-5110): bl 1..8 = x at the plane nyh = my/2+1,
+  bl 2..4 divided by bl 1, bl 9..11 = cur.
+"""
+from __future__ import annotations
+
+import struct
+from decimal import Decimal, ROUND_HALF_EVEN, localcontext
+
+import numpy as np
+
+GFORTRAN_MAX_SUBRECORD = 2147483639
+
+
+def write_record(data: bytes, maxsub: int = GFORTRAN_MAX_SUBRECORD) -> bytes:
+    parts = []
+    n = len(data)
+    starts = list(range(0, n, maxsub)) or [0]
+    for q, s in enumerate(starts):
+        chunk = data[s:s + maxsub]
+        more = s + len(chunk) < n
+        head = -len(chunk) if more else len(chunk)
+        tail = len(chunk) if q == 0 else -len(chunk)
+        parts.append(struct.pack("<i", head) + chunk + struct.pack("<i", tail))
+    return b"".join(parts)
+
+
+def read_records(buf: bytes) -> list[bytes]:
+    out, pos = [], 0
+    while pos < len(buf):
+        rec, first = [], True
+        while True:
+            (head,) = struct.unpack_from("<i", buf, pos)
+            n = abs(head)
+            rec.append(buf[pos + 4:pos + 4 + n])
+            (tail,) = struct.unpack_from("<i", buf, pos + 4 + n)
+            if (tail if first else -tail) != n:
+                raise ValueError("record markers disagree")
+            pos += 8 + n
+            first = False
+            if head >= 0:
+                break
+        out.append(b"".join(rec))
+    return out
+
+
+def restart_bytes(ncase: int, nstep: int, time: float, nst: int, x_fortran: np.ndarray,
+                  maxsub: int = GFORTRAN_MAX_SUBRECORD) -> bytes:
+    """x_fortran: C-order (8, mz+4, my, mx+4) == Fortran x(mx+4, my, mz+4, 8)."""
+    hdr = struct.pack("<iidi", ncase, nstep, time, nst)
+    return write_record(hdr, maxsub) + write_record(np.ascontiguousarray(x_fortran, "<f8").tobytes(), maxsub)
+
+
+def e_edit(v: float, w: int, d: int, e: int | None = None) -> str:
+    """Fortran Ew.d / Ew.dEe output of v (scale factor 0), w characters; the optional zero
+    before the point is written when it fits."""
+    v = float(v)
+    neg = bool(np.signbit(v))
+    if v != v:
+        s = "NaN"
+        return s.rjust(w) if len(s) <= w else "*" * w
+    if v in (float("inf"), float("-inf")):
+        s = ("-" if neg else "") + ("Infinity" if w >= 8 + neg else "Inf")
+        return s.rjust(w) if len(s) <= w else "*" * w
+    if v == 0.0:
+        digits, ex = "0" * d, 0
+    else:
+        with localcontext() as ctx:
+            ctx.prec = 1200                       # every double's decimal expansion, exactly
+            a = Decimal(abs(v))
+            ex = a.adjusted() + 1                 # a = 0.d1d2... x 10^ex
+            q = a.scaleb(-ex).quantize(Decimal(1).scaleb(-d), rounding=ROUND_HALF_EVEN)
+            if q >= 1:                            # rounding carried into a new digit
+                ex += 1
+                q = a.scaleb(-ex).quantize(Decimal(1).scaleb(-d), rounding=ROUND_HALF_EVEN)
+        digits = str(q)[2:2 + d].ljust(d, "0")
+    sgn = "-" if ex < 0 else "+"
+    if e is None:
+        if abs(ex) <= 99:
+            exs = f"E{sgn}{abs(ex):02d}"
+        elif abs(ex) <= 999:
+            exs = f"{sgn}{abs(ex):03d}"
+        else:
+            return "*" * w
+    else:
+        if abs(ex) >= 10 ** e:
+            return "*" * w
+        exs = f"E{sgn}{abs(ex):0{e}d}"
+    body = ("-" if neg else "") + "." + digits + exs
+    if len(body) > w:
+        return "*" * w
+    if len(body) + 1 <= w:
+        body = ("-" if neg else "") + "0." + digits + exs
+    return body.rjust(w)
+
+
+def format_list(values, per_line: int, w: int, d: int, e: int | None = None) -> str:
+    vals = list(values)
+    lines = []
+    for s in range(0, len(vals), per_line):
+        lines.append("".join(" " + e_edit(v, w, d, e) for v in vals[s:s + per_line]) + "\n")
+    return "".join(lines)
+
+
+def _ints(*v) -> str:
+    return "".join(f" {q:11d}" for q in v) + "\n"
+
+
+def _real(t: float) -> str:
+    return f" {t:24.16E}\n"
+
+
+def output_fields(X: np.ndarray, cur: np.ndarray) -> np.ndarray:
+    """Eleven fields on all nodes from the compact state (8, mz, my, mx) and current (3, ...)."""
+    bl = np.concatenate([X, cur]).astype(np.float64)
+    bl[1:4] = bl[1:4] / bl[0]
+    return bl
+
+
+def m2d_text(time: float, x, z, X: np.ndarray, cur: np.ndarray) -> str:
+    my = X.shape[2]
+    bl = output_fields(X, cur)[:, :, my // 2, :]           # (11, mz, mx)
+    out = [_ints(2, len(x), len(z)), _real(time), format_list(list(x) + list(z), 5, 14, 5, 3)]
+    for q in range(11):
+        out.append(_ints(q + 1))
+        out.append(format_list(bl[q].reshape(-1), 5, 14, 5, 3))
+    return "".join(out)
+
+
+def m3d_text(time: float, x, y, z, X: np.ndarray, cur: np.ndarray) -> str:
+    bl = output_fields(X, cur)
+    out = [_ints(3, len(x), len(y), len(z)), _real(time), format_list(list(x) + list(y) + list(z), 11, 10, 4)]
+    for q in range(11):
+        out.append(_ints(q + 1))
+        out.append(format_list(bl[q].reshape(-1), 11, 10, 4))
+    return "".join(out)

@@ -1,0 +1,63 @@
+"""GPU side of the output and restart files: the mid-plane fields that dasha_midplane gathers
+on the device equal the host gather from dasha_get_state and dasha_current bit for bit (the
+same FP64 operations on the same values), the m2d file made from them equals the checker's
+text, and a run restored from its restart file continues as the uninterrupted run does."""
+import numpy as np
+import pytest
+
+from dasha_b200 import capi, harris, restart
+from oracle import fortran_io as fio
+
+pytestmark = pytest.mark.gpu
+
+SMALL = harris.RunConfig("small-32x16x32", 32, 16, 32, False, 0.005, 0.5, 4)
+RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 4, dt_whistler=1)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("cfg", [SMALL, RAGGED], ids=lambda c: c.name)
+def test_midplane_matches_host_gather(cfg, precision):
+    d = capi.gem_context(cfg, precision)
+    d.run(2)
+    mp = d.midplane()
+    X, cur = d.get_state(), d.current()
+    host = restart.midplane_host(harris.to_halo(X), harris.to_halo(cur))
+    assert np.array_equal(mp, host)
+    assert np.array_equal(mp, fio.output_fields(X, cur)[:, :, cfg.my // 2, :])
+    d.close()
+
+
+def test_m2d_from_device_plane(tmp_path):
+    d = capi.gem_context(SMALL, 0)
+    t, _ = d.run(1)
+    p = tmp_path / "m2d001.dat"
+    restart.write_m2d(str(p), t, d.x, d.z, d.midplane())
+    assert p.read_text() == fio.m2d_text(t, d.x, d.z, d.get_state(), d.current())
+    d.close()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-13), (1, 1e-6)], ids=["fp64", "fp32"])
+def test_restart_continues_the_run(tmp_path, precision, tol):
+    """Checkpoint after 2 steps, restore into a fresh context, 2 more steps on both.  The file
+    holds FP64 totals; a context stores x - eq, so the restored state may differ from the live
+    one by the rounding of that subtraction (FP64) or by the compensation term that the file
+    does not carry (FP32)."""
+    a = capi.gem_context(SMALL, precision)
+    t, _ = a.run(2)
+    path = restart.checkpoint(a, str(tmp_path), ncase=1, nstep=2, time=t, nst=3)
+    assert path.endswith("mhd003000")
+    b = capi.gem_context(SMALL, precision)
+    ncase, nstep, tb, nst = restart.restore(b, str(tmp_path), 3)
+    assert (ncase, nstep, tb, nst) == (1, 2, t, 3)
+    xa, xb = a.get_state(), b.get_state()
+    scale = np.abs(xa).reshape(8, -1).max(axis=1)
+    rt = np.abs(xa - xb).reshape(8, -1).max(axis=1) / scale
+    assert rt.max() < (1e-15 if precision == 0 else 1e-7), rt   # one FP64 / FP32 rounding
+    ta, _ = a.run(2, t, 2)
+    tb2, _ = b.run(2, tb, 2)
+    assert abs(ta - tb2) <= 1e-12 * ta
+    xa, xb = a.get_state(), b.get_state()
+    err = np.abs(xa - xb).reshape(8, -1).max(axis=1) / scale
+    assert err.max() < tol, err
+    a.close()
+    b.close()

@@ -1,0 +1,196 @@
+"""Restart and output files of libdasha.so (host code, no GPU) against the pure-Python
+restatement in oracle/fortran_io.py: the unformatted restart of recrd / readin
+(t3dsdsc.f:4814-4861) byte for byte, its gfortran subrecord framing, the readers' rejection of
+files that do not match, the ASCII m2d / m3d files of recrd2 / recrd3 (t3dsdsc.f:4965-5412)
+character for character, and the eleven output fields of the mid-y plane."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from dasha_b200 import capi, harris, restart
+from oracle import fortran_io as fio
+
+
+def _state(mx, my, mz, seed=3):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((8, mz, my, mx))
+    X[0] = 1.0 + 0.5 * rng.random((mz, my, mx))            # positive density
+    cur = rng.standard_normal((3, mz, my, mx)) * 10.0 ** rng.integers(-3, 4, (3, mz, my, mx))
+    return X, cur
+
+
+# --- E editing, hand-derived from the Fortran rules (scale factor 0, optional zero written) ---
+KAT_E14_5E3 = [(1.0, "  0.10000E+001"), (-123.456, " -0.12346E+003"), (0.0, "  0.00000E+000"),
+               (1e-5, "  0.10000E-004"), (1.23456789e300, "  0.12346E+301"), (-0.0, " -0.00000E+000"),
+               (0.999996, "  0.10000E+001"), (9.999996e-100, "  0.10000E-098")]
+KAT_E10_4 = [(1.0, "0.1000E+01"), (-1.0, "-.1000E+01"), (0.0, "0.0000E+00"), (1.5e100, "0.1500+101"),
+             (-2.5e-120, "-.2500-119"), (0.99996, "0.1000E+01"), (123.456, "0.1235E+03")]
+
+
+def test_checker_e_editing_known_answers():
+    for v, s in KAT_E14_5E3:
+        assert fio.e_edit(v, 14, 5, 3) == s, v
+    for v, s in KAT_E10_4:
+        assert fio.e_edit(v, 10, 4) == s, v
+
+
+def test_library_e_editing_known_answers(tmp_path):
+    vals = np.array([v for v, _ in KAT_E14_5E3])
+    plane = np.zeros((11, 1, vals.size))
+    plane[0, 0] = vals
+    p = tmp_path / "m2d.dat"
+    restart.write_m2d(str(p), 0.0, np.zeros(vals.size), np.zeros(1), plane)
+    lines = p.read_text().splitlines()
+    i1 = lines.index(f" {1:11d}")
+    got = "".join(lines[i1 + 1:i1 + 3])
+    assert got == "".join(" " + s for _, s in KAT_E14_5E3)
+    # E10.4 through the 3-D writer: the values as x coordinates
+    xs = np.array([v for v, _ in KAT_E10_4])
+    X = np.ones((8, 1, 1, xs.size))
+    H = harris.to_halo(X)
+    Hc = harris.to_halo(np.zeros((3, 1, 1, xs.size)))
+    p3 = tmp_path / "m3d"
+    restart.write_m3d(str(p3), 0.0, xs, np.zeros(1), np.zeros(1), H, Hc)
+    line = p3.read_text().splitlines()[2]
+    assert line == "".join(" " + s for _, s in KAT_E10_4) + (" " + fio.e_edit(0.0, 10, 4)) * 2   # y, z
+
+
+def test_checker_records_round_trip():
+    data = bytes(range(256)) * 3
+    for maxsub in (fio.GFORTRAN_MAX_SUBRECORD, 100, 7, 1):
+        assert fio.read_records(fio.write_record(data, maxsub) + fio.write_record(b"", maxsub)) == [data, b""]
+    # gfortran's markers for a record split in three
+    b = fio.write_record(b"abcdefgh", 3)
+    assert b == (b"\xfd\xff\xff\xffabc\x03\x00\x00\x00" + b"\xfd\xff\xff\xffdef\xfd\xff\xff\xff"
+                 + b"\x02\x00\x00\x00gh\xfe\xff\xff\xff")
+
+
+@pytest.mark.parametrize("maxsub", [0, 4096, 1000, 12])
+def test_restart_bytes_match_checker(tmp_path, maxsub):
+    mx, my, mz = 9, 5, 7
+    X, _ = _state(mx, my, mz)
+    H = restart.restart_array(X)
+    p = tmp_path / restart.restart_name(12)
+    restart.write_restart(str(p), 3, 4567, 12.375, 12, H, max_subrecord=maxsub)
+    ref = fio.restart_bytes(3, 4567, 12.375, 12, H, maxsub or fio.GFORTRAN_MAX_SUBRECORD)
+    assert p.read_bytes() == ref
+    ncase, nstep, time, nst, H2 = restart.read_restart(str(p), mx, my, mz)
+    assert (ncase, nstep, time, nst) == (3, 4567, 12.375, 12)
+    assert np.array_equal(H2, H)
+
+
+def test_restart_padded_leading_dimensions(tmp_path):
+    mx, my, mz = 8, 6, 5
+    X, _ = _state(mx, my, mz, seed=5)
+    H = restart.restart_array(X)
+    ld1, ld2 = mx + 9, my + 3
+    Hp = np.full((8, mz + 4, ld2, ld1), -7.0)
+    Hp[:, :, :my, :mx + 4] = H
+    p1, p2 = tmp_path / "a", tmp_path / "b"
+    restart.write_restart(str(p1), 1, 2, 3.0, 4, H)
+    lib = capi.load()
+    assert lib.dasha_restart_write(str(p2).encode(), 1, 2, 3.0, 4, mx, my, mz, capi._dp(Hp), ld1, ld2, 0) == 0
+    assert p1.read_bytes() == p2.read_bytes()
+    # read back into a padded array: only the (mx+4, my, mz+4) block changes
+    out = np.full_like(Hp, 99.0)
+    a, b, d, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    assert lib.dasha_restart_read(str(p1).encode(), ctypes.byref(a), ctypes.byref(b), ctypes.byref(t),
+                                  ctypes.byref(d), mx, my, mz, capi._dp(out), ld1, ld2) == 0
+    assert np.array_equal(out[:, :, :my, :mx + 4], H)
+    assert (out[:, :, my:, :] == 99.0).all() and (out[:, :, :, mx + 4:] == 99.0).all()
+
+
+def test_restart_reader_accepts_any_split_and_rejects_mismatches(tmp_path):
+    mx, my, mz = 6, 4, 5
+    X, _ = _state(mx, my, mz, seed=9)
+    H = restart.restart_array(X)
+    p = tmp_path / "f"
+    for maxsub in (7, 13, 8 * 1000 + 3):                       # splits inside doubles
+        p.write_bytes(fio.restart_bytes(2, 3, 0.5, 1, H, maxsub))
+        assert np.array_equal(restart.read_restart(str(p), mx, my, mz)[4], H)
+    good = fio.restart_bytes(2, 3, 0.5, 1, H)
+    with pytest.raises(capi.DashaError):
+        restart.read_restart(str(p), mx + 1, my, mz)          # wrong grid: record 2 too short
+    p.write_bytes(good)
+    with pytest.raises(capi.DashaError):
+        restart.read_restart(str(p), mx, my, mz - 1)          # record 2 too long
+    p.write_bytes(good[:-9])
+    with pytest.raises(capi.DashaError):
+        restart.read_restart(str(p), mx, my, mz)              # truncated
+    bad = bytearray(good)
+    bad[-1] ^= 1                                              # trailing marker of record 2
+    p.write_bytes(bytes(bad))
+    with pytest.raises(capi.DashaError):
+        restart.read_restart(str(p), mx, my, mz)
+    with pytest.raises(capi.DashaError):
+        restart.read_restart(str(tmp_path / "missing"), mx, my, mz)
+
+
+def test_restart_names():
+    assert restart.restart_name(7) == "mhd007000"
+    assert restart.restart_name(123, 45) == "mhd123045"
+    with pytest.raises(ValueError):
+        restart.restart_name(1000)
+
+
+def test_midplane_host_matches_checker():
+    mx, my, mz = 10, 6, 9
+    X, cur = _state(mx, my, mz, seed=21)
+    got = restart.midplane_host(harris.to_halo(X), harris.to_halo(cur))
+    ref = fio.output_fields(X, cur)[:, :, my // 2, :]
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("mx,my,mz", [(10, 6, 9), (7, 3, 11), (1, 1, 1)])
+def test_m2d_matches_checker(tmp_path, mx, my, mz):
+    X, cur = _state(mx, my, mz, seed=mx + mz)
+    x = np.linspace(-12.8, 12.8, mx)
+    z = np.sinh(np.linspace(-3, 3, mz))
+    plane = restart.midplane_host(harris.to_halo(X), harris.to_halo(cur))
+    p = tmp_path / "m2d001.dat"
+    restart.write_m2d(str(p), 17.25, x, z, plane)
+    txt = p.read_text()
+    assert txt == fio.m2d_text(17.25, x, z, X, cur)
+    # list-directed reading back: 0.ddddd, at most half a unit of the 5th digit, 5e-5 relative
+    tok = txt.split()
+    assert [int(t) for t in tok[:3]] == [2, mx, mz] and float(tok[3]) == 17.25
+    vals = np.array([float(t) for t in tok[4:4 + mx + mz]])
+    assert np.allclose(vals, np.concatenate([x, z]), rtol=5e-5, atol=0)
+
+
+def test_m3d_matches_checker(tmp_path):
+    mx, my, mz = 7, 4, 6
+    X, cur = _state(mx, my, mz, seed=2)
+    x, y, z = np.linspace(0, 1, mx), np.linspace(-2, 2, my), np.linspace(-3, 3, mz)
+    p = tmp_path / "m3d004"
+    restart.write_m3d(str(p), 3.5, x, y, z, harris.to_halo(X), harris.to_halo(cur))
+    assert p.read_text() == fio.m3d_text(3.5, x, y, z, X, cur)
+
+
+def test_large_list_parallel_formatting(tmp_path):
+    """Lists longer than one formatting block of the library (2^14 lines per thread)."""
+    mx, mz = 512, 200
+    rng = np.random.default_rng(4)
+    plane = rng.standard_normal((11, mz, mx)) * 10.0 ** rng.integers(-120, 120, (11, mz, mx))
+    x, z = np.arange(mx, dtype=float), np.arange(mz, dtype=float)
+    p = tmp_path / "m2d.dat"
+    restart.write_m2d(str(p), 0.0, x, z, plane)
+    lines = p.read_text().splitlines()
+    i5 = lines.index(f" {5:11d}")
+    q = plane[4].reshape(-1)
+    body = lines[i5 + 1:i5 + 1 + (q.size + 4) // 5]
+    assert len(body) == (q.size + 4) // 5
+    for li in rng.integers(0, len(body), 200):
+        assert body[li] == fio.format_list(q[5 * li:5 * li + 5], 5, 14, 5, 3).rstrip("\n")
+
+
+def test_bad_arguments_rejected(tmp_path):
+    lib = capi.load()
+    assert lib.dasha_restart_write(None, 0, 0, 0.0, 0, 4, 4, 4, None, 8, 4, 0) == capi.E_INVALID
+    H = np.zeros((8, 8, 4, 8))
+    assert lib.dasha_restart_write(str(tmp_path / "a").encode(), 0, 0, 0.0, 0, 4, 4, 4, capi._dp(H), 7, 4, 0) == capi.E_INVALID
+    assert lib.dasha_restart_write(str(tmp_path / "a").encode(), 0, 0, 0.0, 0, 4, 4, 4, capi._dp(H), 8, 4, -1) == capi.E_INVALID
+    assert lib.dasha_m2d_write(str(tmp_path / "m").encode(), 0, 4, 0.0, None, None, None) == capi.E_INVALID
+    assert lib.dasha_midplane(None, None) == capi.E_INVALID
+    assert lib.dasha_restart_write(str(tmp_path / "no" / "dir").encode(), 0, 0, 0.0, 0, 4, 4, 4, capi._dp(H), 8, 4, 0) == capi.E_INVALID
