@@ -17,6 +17,10 @@
 //    11(1X,E10.4) (m3d), a new line after every 5 or 11 numbers and at the end of each list.
 //    Fields: 1 rho, 2-4 v = (rho v)/rho, 5-7 B, 8 p (totals), 9-11 the current density; m2d
 //    holds the plane j = my/2 (0-based; nyh = my/2+1 in the reference).
+//  - current.dat of diagn (t3dsdsc.f:1226-1232): one line per call, the mid-y-plane extrema
+//    Jx max, Jx min, Jy max, Jy min, Jz max, Jz min and time in the format 7(1X,E13.4).  The
+//    reference opens unit 9 on every call and never closes it, so the lines of a run follow
+//    one another in the file.
 #include "dasha_capi.h"
 
 #include <algorithm>
@@ -339,6 +343,16 @@ int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const
             return out_field(x_f, cur_f, ld1, ld2, mz, q, i, j, k);
         });
     }
+    ok = ok && !std::ferror(f);
+    return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
+}
+
+int dasha_current_dat_write(const char* path, const double* diag, double time, int append) {
+    if (!path || !diag) return DASHA_E_INVALID;
+    FILE* f = std::fopen(path, append ? "a" : "w");
+    if (!f) return DASHA_E_INVALID;
+    const double v[7] = {diag[3], diag[4], diag[5], diag[6], diag[7], diag[8], time};
+    bool ok = write_list(f, 7, 7, 13, 4, 0, [&](long n) { return v[n]; });
     ok = ok && !std::ferror(f);
     return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
 }

@@ -7,6 +7,7 @@
   x(mx+4, my, mz+4, 8).
 * `write_m2d` / `write_m3d`: the ASCII files data/m2dNNN.dat and data/m3dNNN of recrd2 / recrd3
   (t3dsdsc.f:4965-5412); `Dasha.midplane()` gives the eleven mid-plane fields from the GPU.
+* `write_current_dat`: the line diagn appends to current.dat (t3dsdsc.f:1226-1232).
 
 Arrays follow `harris.to_halo`: C-order (nf, mz+4, ld2, ld1) == Fortran x(ld1, ld2, mz+4, nf).
 Everything goes through the C library; without it every call raises.
@@ -109,6 +110,15 @@ def write_m3d(path: str, time: float, x: np.ndarray, y: np.ndarray, z: np.ndarra
     assert Hcur.shape[1:] == H.shape[1:] and (x.size, y.size, z.size) == (ld1 - 4, ld2, mz4 - 4)
     _check(lib.dasha_m3d_write(os.fsencode(path), x.size, y.size, z.size, float(time), capi._dp(x), capi._dp(y),
                                capi._dp(z), capi._dp(H), capi._dp(Hcur), ld1, ld2), f"m3d write {path}")
+
+
+def write_current_dat(path: str, diag: np.ndarray, time: float, append: bool = True):
+    """diagn's current.dat line: the J extrema diag[3:9] of `Dasha.diagnostics()` and time."""
+    lib = capi.load()
+    diag = np.ascontiguousarray(diag, np.float64)
+    assert diag.size >= capi.NDIAG
+    _check(lib.dasha_current_dat_write(os.fsencode(path), capi._dp(diag), float(time), 1 if append else 0),
+           f"current.dat write {path}")
 
 
 def checkpoint(d: "capi.Dasha", directory: str, ncase: int, nstep: int, time: float, nst: int) -> str:

@@ -206,6 +206,12 @@ int dasha_midplane_host(int mx, int my, int mz, const double* x_f, const double*
 int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const double* x, const double* y,
                     const double* z, const double* x_f, const double* cur_f, long ld1, long ld2);
 
+/* One line of current.dat, the file diagn writes every 10 steps (t3dsdsc.f:1226-1232): the
+ * mid-y-plane current extrema diag[3..8] of dasha_diagnostics (Jx max, Jx min, Jy max, Jy min,
+ * Jz max, Jz min) and time, in the format 7(1X,E13.4).  append = 0 starts the file (the first
+ * call of a run), 1 adds the line at its end. */
+int dasha_current_dat_write(const char* path, const double* diag, double time, int append);
+
 const char* dasha_last_error(dasha_ctx* ctx);
 void dasha_destroy(dasha_ctx* ctx);
 

@@ -10,6 +10,7 @@ unformatted records and for E editing, and gfortran's published record layout.
 * m2d / m3d (recrd2 t3dsdsc.f:5116-5154, recrd3 t3dsdsc.f:5365-5402): list-directed header
   lines (written here as the library writes them: integers in 12 columns, the time with 17
   significant digits), then lists under 5(1X,E14.5E3) or 11(1X,E10.4).
+* current.dat (diagn, t3dsdsc.f:1226-1232): 7(1X,E13.4) per line.
 * the eleven output fields (t3dsdsc.f:5009-5110): bl 1..8 = x at the plane nyh = my/2+1,
   bl 2..4 divided by bl 1, bl 9..11 = cur.
 """
@@ -136,6 +137,11 @@ def m2d_text(time: float, x, z, X: np.ndarray, cur: np.ndarray) -> str:
         out.append(_ints(q + 1))
         out.append(format_list(bl[q].reshape(-1), 5, 14, 5, 3))
     return "".join(out)
+
+
+def current_dat_line(jx_max, jx_min, jy_max, jy_min, jz_max, jz_min, time) -> str:
+    """diagn's write(9,15) with 15 format(7(1x,e13.4)) (t3dsdsc.f:1228-1230)."""
+    return format_list([jx_max, jx_min, jy_max, jy_min, jz_max, jz_min, time], 7, 13, 4)
 
 
 def m3d_text(time: float, x, y, z, X: np.ndarray, cur: np.ndarray) -> str:

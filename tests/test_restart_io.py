@@ -185,6 +185,23 @@ def test_large_list_parallel_formatting(tmp_path):
         assert body[li] == fio.format_list(q[5 * li:5 * li + 5], 5, 14, 5, 3).rstrip("\n")
 
 
+def test_current_dat_lines(tmp_path):
+    """diagn's current.dat: a first line, then appended lines, each 7(1X,E13.4)."""
+    p = tmp_path / "current.dat"
+    rng = np.random.default_rng(8)
+    lines = []
+    for q in range(3):
+        diag = rng.standard_normal(capi.NDIAG) * 10.0 ** rng.integers(-5, 5, capi.NDIAG)
+        t = 0.125 * q
+        restart.write_current_dat(str(p), diag, t, append=q > 0)
+        lines.append(fio.current_dat_line(*diag[3:9], t))
+    assert p.read_text() == "".join(lines)
+    assert len(lines[0]) == 7 * 14 + 1                        # 7 x (1X + 13 columns) + newline
+    restart.write_current_dat(str(p), np.ones(capi.NDIAG), 1.0, append=False)   # starts over
+    assert p.read_text() == fio.current_dat_line(*([1.0] * 6), 1.0)
+    assert fio.e_edit(-1.0, 13, 4) == "  -0.1000E+01"
+
+
 def test_bad_arguments_rejected(tmp_path):
     lib = capi.load()
     assert lib.dasha_restart_write(None, 0, 0, 0.0, 0, 4, 4, 4, None, 8, 4, 0) == capi.E_INVALID
