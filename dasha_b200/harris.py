@@ -1,7 +1,7 @@
 """Seeded Harris-sheet / GEM initial states, grids and run parameters.
 
 The reference program builds a dipole magnetosphere (initia, t3dsdsc.f:612-850) from input
-files that are not part of it; the Harris-sheet configurations of this build replace that
+files that are not part of it; the Harris-sheet configurations here replace that
 initializer.  Everything here is host-side FP64 numpy, generated in the Fortran index order
 of x(mx,my,mz,8) (x fastest) so that the CUDA library and the CPU oracle start from
 bit-identical inputs.

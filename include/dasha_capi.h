@@ -9,7 +9,7 @@
  * (t3dsdsc.f:2452-2500).  All data moves through COMMON blocks (mhd01.for:55-66,
  * mhd02.for:1-6).  This header replaces those bodies: the state lives on the GPU inside an
  * opaque context, and the Fortran loop calls the functions below through an ISO_C_BINDING
- * interface (INTEGRATION.md shows the module).
+ * interface.
  *
  * Conventions
  *  - Every function returns 0 (DASHA_OK) or a DASHA_E_* code; no exception or exit() crosses
@@ -37,7 +37,9 @@ typedef struct dasha_ctx dasha_ctx;
 enum {
     DASHA_OK = 0,
     DASHA_E_INVALID = 1,      /* bad argument (null pointer, size, leading dimension) */
-    DASHA_E_UNSUPPORTED = 2,  /* an option the build does not implement */
+    DASHA_E_UNSUPPORTED = 2,  /* an option the library does not implement: mx not a multiple of 32,
+                                 periodicity other than {1,1,0}, total_e != 1, rcr > 0, or the
+                                 adjoint on an FP32 context */
     DASHA_E_CUDA = 3,         /* a CUDA runtime error; the context should be destroyed */
     DASHA_E_NOMEM = 4,        /* the grid does not fit in device memory */
     DASHA_E_DT_COLLAPSE = 5,  /* dt < 0.1*dt0 or not finite: the guard of t3dsdsc.f:142-154 */

@@ -3,8 +3,8 @@
  *
  * This file restates, in plain C++ (FP64, scalar loops, optional OpenMP), the RK4
  * finite-difference Hall-MHD time step of the reference Fortran program t3dsdsc.f
- * (with its include files mhd01.for, mhd02.for, mhd03.for).  It is the checker for the
- * CUDA library in dasha_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline /
+ * (with its include files mhd01.for, mhd02.for, mhd03.for).  It is the oracle the tests compare
+ * the CUDA library in dasha_b200/ with: only tests/, __graft_entry__.smoke() and the cpu_baseline /
  * reference leg of bench.py may load it.  The product never links or calls it.
  *
  * PARITY UNPINNED.  The reference ships no tests, golden vectors or fixtures, and it cannot

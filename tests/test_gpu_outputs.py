@@ -1,6 +1,6 @@
 """GPU side of the output and restart files: the mid-plane fields that dasha_midplane gathers
 on the device equal the host gather from dasha_get_state and dasha_current bit for bit (the
-same FP64 operations on the same values), the m2d file made from them equals the checker's
+same FP64 operations on the same values), the m2d file made from them equals the oracle's
 text, and a run restored from its restart file continues as the uninterrupted run does."""
 import numpy as np
 import pytest

@@ -28,7 +28,7 @@ KAT_E10_4 = [(1.0, "0.1000E+01"), (-1.0, "-.1000E+01"), (0.0, "0.0000E+00"), (1.
              (-2.5e-120, "-.2500-119"), (0.99996, "0.1000E+01"), (123.456, "0.1235E+03")]
 
 
-def test_checker_e_editing_known_answers():
+def test_oracle_e_editing_known_answers():
     for v, s in KAT_E14_5E3:
         assert fio.e_edit(v, 14, 5, 3) == s, v
     for v, s in KAT_E10_4:
@@ -56,7 +56,7 @@ def test_library_e_editing_known_answers(tmp_path):
     assert line == "".join(" " + s for _, s in KAT_E10_4) + (" " + fio.e_edit(0.0, 10, 4)) * 2   # y, z
 
 
-def test_checker_records_round_trip():
+def test_oracle_records_round_trip():
     data = bytes(range(256)) * 3
     for maxsub in (fio.GFORTRAN_MAX_SUBRECORD, 100, 7, 1):
         assert fio.read_records(fio.write_record(data, maxsub) + fio.write_record(b"", maxsub)) == [data, b""]
@@ -67,7 +67,7 @@ def test_checker_records_round_trip():
 
 
 @pytest.mark.parametrize("maxsub", [0, 4096, 1000, 12])
-def test_restart_bytes_match_checker(tmp_path, maxsub):
+def test_restart_bytes_match_oracle(tmp_path, maxsub):
     mx, my, mz = 9, 5, 7
     X, _ = _state(mx, my, mz)
     H = restart.restart_array(X)
@@ -134,7 +134,7 @@ def test_restart_names():
         restart.restart_name(1000)
 
 
-def test_midplane_host_matches_checker():
+def test_midplane_host_matches_oracle():
     mx, my, mz = 10, 6, 9
     X, cur = _state(mx, my, mz, seed=21)
     got = restart.midplane_host(harris.to_halo(X), harris.to_halo(cur))
@@ -143,7 +143,7 @@ def test_midplane_host_matches_checker():
 
 
 @pytest.mark.parametrize("mx,my,mz", [(10, 6, 9), (7, 3, 11), (1, 1, 1)])
-def test_m2d_matches_checker(tmp_path, mx, my, mz):
+def test_m2d_matches_oracle(tmp_path, mx, my, mz):
     X, cur = _state(mx, my, mz, seed=mx + mz)
     x = np.linspace(-12.8, 12.8, mx)
     z = np.sinh(np.linspace(-3, 3, mz))
@@ -159,7 +159,7 @@ def test_m2d_matches_checker(tmp_path, mx, my, mz):
     assert np.allclose(vals, np.concatenate([x, z]), rtol=5e-5, atol=0)
 
 
-def test_m3d_matches_checker(tmp_path):
+def test_m3d_matches_oracle(tmp_path):
     mx, my, mz = 7, 4, 6
     X, cur = _state(mx, my, mz, seed=2)
     x, y, z = np.linspace(0, 1, mx), np.linspace(-2, 2, my), np.linspace(-3, 3, mz)
