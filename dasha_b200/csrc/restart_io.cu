@@ -112,6 +112,42 @@ struct RecReader {
     bool finish() const { return ok && done == total && !more && left_in_sub == 0; }
 };
 
+// Powers of ten 1e-300 .. 1e300 as correctly rounded doubles (strtod), exact up to 1e22.
+struct Pow10 {
+    double p[601];
+    Pow10() {
+        for (int k = -300; k <= 300; ++k) p[k + 300] = std::strtod(("1e" + std::to_string(k)).c_str(), nullptr);
+    }
+};
+const Pow10& pow10_table() {
+    static const Pow10 t;
+    return t;
+}
+
+// The d (<= 6) significant decimal digits of a > 0, correctly rounded, and the exponent e of
+// a ~ 0.d1..dd x 10^e, by scaling in double: m = a * 10^(d-1-e10) lies in [10^(d-1), 10^d)
+// with a relative error below 3e-16 (two roundings), so below 3e-10 in absolute terms, and
+// rounding m to the nearest integer gives the exact result unless m lies within 1e-6 of a
+// tie (xxx.5) or of either end of the interval, where the function declines (returns false)
+// and the caller uses the exact conversion of snprintf.
+bool fast_digits(double a, int d, char* digits, int* e) {
+    if (d < 1 || d > 6 || !(a >= 1e-280 && a <= 1e280)) return false;
+    static const double P[7] = {1, 10, 100, 1000, 10000, 100000, 1000000};
+    int e10 = (int)std::floor(std::log10(a));
+    const int sc = d - 1 - e10;
+    if (sc < -300 || sc > 300) return false;
+    const double m = a * pow10_table().p[sc + 300];
+    const double lo = P[d - 1], hi = P[d];
+    if (!(m >= lo + 1e-6 && m <= hi - 1e-6)) return false;   // exponent near a power of ten
+    const double fl = std::floor(m), fr = m - fl;            // exact: m < 1e6
+    if (std::fabs(fr - 0.5) < 1e-6) return false;            // near a decimal tie
+    long r = (long)fl + (fr > 0.5 ? 1 : 0);
+    if (r >= (long)hi) { r = (long)lo; ++e10; }              // 9..9.7 rounds up to 10..0
+    for (int q = d - 1; q >= 0; --q) { digits[q] = char('0' + r % 10); r /= 10; }
+    *e = e10 + 1;
+    return true;
+}
+
 // Fortran Ew.d (edig = 0) or Ew.dEe output editing of v at scale factor 0, as gfortran writes it:
 // [-][0].d1..dd followed by E+xx (Ew.d, |exponent| <= 99), +xxx (Ew.d, 99 < |exponent| <= 999)
 // or E+ and edig digits; the optional zero before the point is written when the width has
@@ -131,7 +167,7 @@ void fmt_e(char* out, double v, int w, int d, int edig) {
     int e = 0;
     if (v == 0.0) {
         std::memset(digits, '0', d);
-    } else {
+    } else if (!fast_digits(std::fabs(v), d, digits, &e)) {
         char s[48];
         std::snprintf(s, sizeof s, "%.*e", d - 1, std::fabs(v));   // d.dd..de+XX: d significant digits
         digits[0] = s[0];
@@ -139,18 +175,25 @@ void fmt_e(char* out, double v, int w, int d, int edig) {
         e = std::atoi(std::strchr(s, 'e') + 1) + 1;                 // 0.d1..dd x 10^e
     }
     const int ae = e < 0 ? -e : e;
-    char ex[16];
+    // exponent field: E, sign and nd digits (Ew.d with |e| <= 99, Ew.dEe), or sign and 3 digits
+    int nd;
+    bool with_e = true;
     if (edig == 0) {
-        if (ae <= 99) std::snprintf(ex, sizeof ex, "E%c%02d", e < 0 ? '-' : '+', ae);
-        else if (ae <= 999) std::snprintf(ex, sizeof ex, "%c%03d", e < 0 ? '-' : '+', ae);
+        if (ae <= 99) nd = 2;
+        else if (ae <= 999) { nd = 3; with_e = false; }
         else { std::memset(out, '*', w); return; }
     } else {
         int lim = 1;
         for (int q = 0; q < edig; ++q) lim *= 10;
         if (ae >= lim) { std::memset(out, '*', w); return; }
-        std::snprintf(ex, sizeof ex, "E%c%0*d", e < 0 ? '-' : '+', edig, ae);
+        nd = edig;
     }
-    const int nex = (int)std::strlen(ex);
+    char ex[16];
+    int nex = 0;
+    if (with_e) ex[nex++] = 'E';
+    ex[nex++] = e < 0 ? '-' : '+';
+    for (int q = nd - 1, a = ae; q >= 0; --q, a /= 10) ex[nex + q] = char('0' + a % 10);
+    nex += nd;
     const int need = (neg ? 1 : 0) + 1 + d + nex;   // without the optional zero
     if (need > w) { std::memset(out, '*', w); return; }
     int n = 0;

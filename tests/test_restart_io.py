@@ -202,6 +202,45 @@ def test_current_dat_lines(tmp_path):
     assert fio.e_edit(-1.0, 13, 4) == "  -0.1000E+01"
 
 
+def _hard_values(n, seed):
+    """Values where a shortcut conversion to 4 or 5 digits would go wrong: random magnitudes
+    over 1e-300..1e300, exact decimal ties at the 5th and 6th digit (k + 0.5 and k/10 + 0.05
+    scaled by powers of two are not ties; k + 0.5 with 4 and 5 digits are), powers of ten and
+    their neighbours, values just below a carry (9.99995e-k), subnormals and extremes."""
+    rng = np.random.default_rng(seed)
+    v = [rng.uniform(1, 10, n) * 10.0 ** rng.integers(-300, 300, n)]
+    v.append(np.concatenate([np.arange(1000, 1100) + 0.5, np.arange(99990, 100000) + 0.5,
+                             np.arange(10000, 10100) + 0.5]))
+    tens = 10.0 ** np.arange(-300, 301, 7)
+    v.append(np.concatenate([tens, np.nextafter(tens, 0), np.nextafter(tens, np.inf)]))
+    v.append(9.99995 * 10.0 ** np.arange(-20, 20.0))
+    v.append(9.9995 * 10.0 ** np.arange(-20, 20.0))
+    v.append(np.array([5e-324, 1e-310, 2.2250738585072014e-308, 1.7976931348623157e308, 1e299, 1e-299]))
+    x = np.concatenate(v)
+    sgn = np.where(rng.random(x.size) < 0.5, -1.0, 1.0)
+    return x * sgn
+
+
+def test_formatting_matches_exact_decimal_conversion(tmp_path):
+    """The library's digits (a double-arithmetic fast path with an exact fallback) against the
+    oracle's exact decimal expansion, for E14.5E3 (m2d) and E10.4 (m3d)."""
+    vals = _hard_values(3000, 17)
+    p = tmp_path / "m2d.dat"
+    plane = np.zeros((11, 1, vals.size))
+    plane[0, 0] = vals
+    restart.write_m2d(str(p), 0.0, np.zeros(vals.size), np.zeros(1), plane)
+    lines = p.read_text().splitlines()
+    i1 = lines.index(f" {1:11d}")
+    got = lines[i1 + 1:i1 + 1 + (vals.size + 4) // 5]
+    assert "\n".join(got) + "\n" == fio.format_list(vals, 5, 14, 5, 3)
+    p3 = tmp_path / "m3d"
+    restart.write_m3d(str(p3), 0.0, vals, np.zeros(1), np.zeros(1), harris.to_halo(np.ones((8, 1, 1, vals.size))),
+                      harris.to_halo(np.zeros((3, 1, 1, vals.size))))
+    lines = p3.read_text().splitlines()
+    got = lines[2:2 + (vals.size + 2 + 10) // 11]
+    assert "\n".join(got) + "\n" == fio.format_list(list(vals) + [0.0, 0.0], 11, 10, 4)
+
+
 def test_bad_arguments_rejected(tmp_path):
     lib = capi.load()
     assert lib.dasha_restart_write(None, 0, 0, 0.0, 0, 4, 4, 4, None, 8, 4, 0) == capi.E_INVALID
