@@ -62,6 +62,8 @@ SIGNATURES = {
     "dasha_profile_read": ([_P, C.POINTER(C.c_int), C.c_char_p, _D, C.POINTER(C.c_long), _D], C.c_int),
     "dasha_current_noalloc": ([C.POINTER(GridC), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "dasha_midplane": ([_P, _D], C.c_int),
+    "dasha_checkpoint": ([_P, C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_long], C.c_int),
+    "dasha_restore": ([_P, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, C.POINTER(C.c_int)], C.c_int),
     "dasha_restart_write": ([C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                              _D, C.c_long, C.c_long, C.c_long], C.c_int),
     "dasha_restart_read": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, C.POINTER(C.c_int),

@@ -3,6 +3,7 @@
 #include "dasha_capi.h"
 #include "mhd_kernels.cuh"
 #include "engine.cuh"
+#include "fortran_records.h"
 
 #include <cmath>
 #include <cstdio>
@@ -220,6 +221,100 @@ int dasha_get_state(dasha_ctx* c, double* x_f, long ld1, long ld2) {
     if (int rc = check_ld(c, x_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return from_status(c, c->eng->get_state(x_f, ld1, ld2));
+}
+
+// Restart file of recrd / readin (t3dsdsc.f:4814-4861) streamed to or from the device state in
+// z-plane chunks: record 2 is x(mx+4, my, mz+4, 8) in the reference's order, so each field is
+// 2 planes of zero z halo, the mz planes of the chunks (each row with the periodic x halo
+// copies that message4 leaves at a 1x1 process grid) and 2 more zero planes.
+int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, double time, int nst,
+                     long max_subrecord) {
+    CAPI_GUARD(c);
+    if (!path || max_subrecord < 0) return fail(c, DASHA_E_INVALID, "bad checkpoint arguments");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
+    const int mx = c->mx, my = c->my, mz = c->mz;
+    const long row = mx + 4;
+    unsigned char hdr[20];
+    const int32_t a = ncase, b = nstep, d = nst;
+    std::memcpy(hdr, &a, 4);
+    std::memcpy(hdr + 4, &b, 4);
+    std::memcpy(hdr + 8, &time, 8);
+    std::memcpy(hdr + 16, &d, 4);
+    RecWriter w1(f, 20, maxsub);
+    w1.put(hdr, 20);
+    bool ok = w1.finish();
+    RecWriter w(f, (long)sizeof(double) * row * my * (mz + 4) * 8, maxsub);
+    std::vector<double> rb(row), zero(row, 0.0);
+    auto zplanes = [&]() { for (long r = 0; r < 2L * my && w.ok; ++r) w.put(zero.data(), (long)sizeof(double) * row); };
+    int rc = DASHA_OK;
+    if (ok) {
+        rc = from_status(c, c->eng->state_out([&](int, int k0, int k1, const double* rows) {
+            if (k0 == 0) zplanes();
+            for (long r = 0; r < (long)(k1 - k0) * my && w.ok; ++r) {
+                const double* v = rows + r * mx;
+                rb[0] = v[mx - 2]; rb[1] = v[mx - 1];
+                std::memcpy(rb.data() + 2, v, sizeof(double) * mx);
+                rb[mx + 2] = v[0]; rb[mx + 3] = v[1];
+                w.put(rb.data(), (long)sizeof(double) * row);
+            }
+            if (k1 == mz) zplanes();
+            return w.ok;
+        }));
+        ok = w.finish();
+    }
+    const bool closed = std::fclose(f) == 0;
+    if (rc != DASHA_OK) return rc;
+    if (!ok || !closed) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
+    return DASHA_OK;
+}
+
+int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double* time, int* nst) {
+    CAPI_GUARD(c);
+    if (!path || !ncase || !nstep || !time || !nst) return fail(c, DASHA_E_INVALID, "bad restore arguments");
+    if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium before the state");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
+    const int mx = c->mx, my = c->my, mz = c->mz;
+    const long row = mx + 4, total = (long)sizeof(double) * row * my * (mz + 4) * 8;
+    unsigned char hdr[20];
+    RecReader r1(f, 20);
+    r1.get(hdr, 20);
+    // the markers of record 2 are checked before the device state is touched
+    if (!r1.finish() || !scan_record(f, total)) {
+        std::fclose(f);
+        return fail(c, DASHA_E_INVALID, std::string(path) + " is not a restart file of this grid");
+    }
+    RecReader r(f, total);
+    std::vector<double> rb(row), skip(row);
+    auto zplanes = [&]() { for (long q = 0; q < 2L * my && r.ok; ++q) r.get(skip.data(), (long)sizeof(double) * row); };
+    int rc = from_status(c, c->eng->state_in([&](int, int k0, int k1, double* rows) {
+        if (k0 == 0) zplanes();
+        for (long q = 0; q < (long)(k1 - k0) * my && r.ok; ++q) {
+            r.get(rb.data(), (long)sizeof(double) * row);
+            std::memcpy(rows + q * mx, rb.data() + 2, sizeof(double) * mx);
+        }
+        if (k1 == mz) zplanes();
+        return r.ok;
+    }));
+    const bool ok = rc == DASHA_OK && r.finish();
+    std::fclose(f);
+    if (!ok) {
+        c->state_set = false;   // part of the state may have been replaced
+        return rc != DASHA_OK ? rc : fail(c, DASHA_E_INVALID, std::string("reading ") + path + " failed");
+    }
+    int32_t a, b, d;
+    std::memcpy(&a, hdr, 4);
+    std::memcpy(&b, hdr + 4, 4);
+    std::memcpy(time, hdr + 8, 8);
+    std::memcpy(&d, hdr + 16, 4);
+    *ncase = a;
+    *nstep = b;
+    *nst = d;
+    c->state_set = true;
+    return DASHA_OK;
 }
 
 int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <algorithm>
 #include <thread>
+#include <functional>
 
 namespace dasha {
 
@@ -67,6 +68,11 @@ struct Profiler {
     ~Profiler() { for (auto e : pool) cudaEventDestroy(e); }
 };
 
+// Host work on one chunk of a state transfer: field m on z planes k0..k1-1 as (k1-k0)*my rows
+// of mx FP64 values, x fastest; false stops the transfer.
+using ChunkIn = std::function<bool(int m, int k0, int k1, double* rows)>;
+using ChunkOut = std::function<bool(int m, int k0, int k1, const double* rows)>;
+
 struct EngineBase {
     Profiler prof;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
@@ -78,6 +84,8 @@ struct EngineBase {
     virtual Status set_j0(const double* j0) = 0;
     virtual Status set_state(const double* x, long ld1, long ld2) = 0;
     virtual Status get_state(double* x, long ld1, long ld2) = 0;
+    virtual Status state_in(const ChunkIn& fill) = 0;
+    virtual Status state_out(const ChunkOut& take) = 0;
     virtual Status setdt(double* dt, int* blowup) = 0;
     virtual Status stepon(double time, double dt, int nstep) = 0;
     virtual Status current(double* cur, long ld1, long ld2) = 0;
@@ -380,26 +388,26 @@ public:
         }
         for (auto& x : th) x.join();
     }
-    // caller node (i, j, k) of field m: (i+2) + ld1 (j + ld2 ((k+2) + (mz+4) m))
-    Status transfer_in(const double* host, long ld1, long ld2, T* const* dst, int nf, bool sub_eq) {
+    // Chunked host transfers.  z-plane chunks of one field move through the two pinned host
+    // buffers and the two device buffers, so that the host work on one chunk overlaps the DMA
+    // and the conversion kernel of the other.  The host work is the caller's: fill(m, k0, k1,
+    // rows) writes field m on planes k0..k1-1 as (k1-k0)*my rows of mx values (x fastest)
+    // before they go to the device; take(m, k0, k1, rows) reads them after they arrive.  A
+    // false return ends the transfer with DASHA_E_INVALID; the fields moved before it stay.
+    Status stream_in(T* const* dst, int nf, bool sub_eq, const ChunkIn& fill) {
         Status s = xbuf();
         if (s.code) return s;
-        const size_t fld = (size_t)ld1 * ld2 * (mz + 4);
         int q = 0;
         for (int m = 0; m < nf; ++m) {
             const double* prof = sub_eq ? eq_profile(g, m) : nullptr;
             for (int k0 = 0; k0 < mz; k0 += xnk, ++q) {
                 const int k1 = std::min(mz, k0 + xnk), b = q & 1;
                 DASHA_CK(cudaEventSynchronize(xev[b]));        // the DMA out of xh[b] is done
-                const double* src = host + fld * m;
-                double* hb = xh[b];
-                par_rows((long)(k1 - k0) * my, [&](long r0, long r1) {
-                    for (long r = r0; r < r1; ++r) {
-                        const long kk = k0 + r / my, j = r % my;
-                        std::memcpy(hb + r * mx, src + 2 + ld1 * (j + ld2 * (kk + 2)), sizeof(double) * mx);
-                    }
-                });
-                DASHA_CK(cudaMemcpyAsync(xd[b], hb, sizeof(double) * (size_t)mx * my * (k1 - k0), cudaMemcpyHostToDevice, st));
+                if (!fill(m, k0, k1, xh[b])) {
+                    DASHA_CK(cudaStreamSynchronize(st));
+                    return Status::err(DASHA_E_INVALID, "the host side of the transfer failed");
+                }
+                DASHA_CK(cudaMemcpyAsync(xd[b], xh[b], sizeof(double) * (size_t)mx * my * (k1 - k0), cudaMemcpyHostToDevice, st));
                 DASHA_CK(cudaEventRecord(xev[b], st));
                 k_import_chunk<T><<<dim3((mx + blk.x - 1) / blk.x, my, k1 - k0), blk, 0, st>>>(mx, my, k0, xd[b], prof, dst[m]);
                 DASHA_CK(cudaGetLastError());
@@ -409,61 +417,92 @@ public:
         return Status::ok();
     }
 
-    Status transfer_out(double* host, long ld1, long ld2, T* const* src, int nf, bool add_eq,
-                        T* const* comp = nullptr) {
+    Status stream_out(T* const* src, int nf, bool add_eq, T* const* comp, const ChunkOut& take) {
         Status s = xbuf();
         if (s.code) return s;
-        const size_t fld = (size_t)ld1 * ld2 * (mz + 4);
         struct Pend { int m, k0, k1, b; };
         Pend prev{-1, 0, 0, 0};
-        auto scatter = [&](const Pend& c) -> Status {
+        bool ok = true;
+        auto drain = [&](const Pend& c) -> Status {
             DASHA_CK(cudaEventSynchronize(xev[c.b]));       // its D2H has landed
-            double* dstp = host + fld * c.m;
-            const double* hb = xh[c.b];
-            par_rows((long)(c.k1 - c.k0) * my, [&](long r0, long r1) {
-                for (long r = r0; r < r1; ++r) {
-                    const long kk = c.k0 + r / my, j = r % my;
-                    std::memcpy(dstp + 2 + ld1 * (j + ld2 * (kk + 2)), hb + r * mx, sizeof(double) * mx);
-                }
-            });
+            ok = take(c.m, c.k0, c.k1, xh[c.b]);
             return Status::ok();
         };
         int q = 0;
-        for (int m = 0; m < nf; ++m) {
+        for (int m = 0; m < nf && ok; ++m) {
             const double* prof = add_eq ? eq_profile(g, m) : nullptr;
-            for (int k0 = 0; k0 < mz; k0 += xnk, ++q) {
+            for (int k0 = 0; k0 < mz && ok; k0 += xnk, ++q) {
                 const int k1 = std::min(mz, k0 + xnk), b = q & 1;
                 k_export_chunk<T><<<dim3((mx + blk.x - 1) / blk.x, my, k1 - k0), blk, 0, st>>>(
                     mx, my, k0, src[m], comp ? comp[m] : nullptr, prof, xd[b]);
                 DASHA_CK(cudaGetLastError());
                 DASHA_CK(cudaMemcpyAsync(xh[b], xd[b], sizeof(double) * (size_t)mx * my * (k1 - k0), cudaMemcpyDeviceToHost, st));
                 DASHA_CK(cudaEventRecord(xev[b], st));
-                if (prev.m >= 0) {                             // scatter the previous chunk meanwhile
-                    s = scatter(prev);
+                if (prev.m >= 0) {                             // the previous chunk meanwhile
+                    s = drain(prev);
                     if (s.code) return s;
                 }
                 prev = {m, k0, k1, b};
             }
         }
-        if (prev.m >= 0) {
-            s = scatter(prev);
+        if (ok && prev.m >= 0) {
+            s = drain(prev);
             if (s.code) return s;
         }
         DASHA_CK(cudaStreamSynchronize(st));
+        if (!ok) return Status::err(DASHA_E_INVALID, "the host side of the transfer failed");
         return Status::ok();
     }
 
-    Status set_state(const double* x, long ld1, long ld2) override {
-        Status s = transfer_in(x, ld1, ld2, X, 8, true);
+    // The same with the caller's array in the reference layout: node (i, j, k) of field m at
+    // (i+2) + ld1 (j + ld2 ((k+2) + (mz+4) m)); rows are gathered (scattered) by host threads.
+    ChunkIn gather(const double* host, long ld1, long ld2) const {
+        const size_t fld = (size_t)ld1 * ld2 * (mz + 4);
+        const int mx_ = mx, my_ = my;
+        return [=](int m, int k0, int k1, double* rows) {
+            const double* srcp = host + fld * m;
+            par_rows((long)(k1 - k0) * my_, [&](long r0, long r1) {
+                for (long r = r0; r < r1; ++r) {
+                    const long kk = k0 + r / my_, j = r % my_;
+                    std::memcpy(rows + r * mx_, srcp + 2 + ld1 * (j + ld2 * (kk + 2)), sizeof(double) * mx_);
+                }
+            });
+            return true;
+        };
+    }
+    ChunkOut scatter(double* host, long ld1, long ld2) const {
+        const size_t fld = (size_t)ld1 * ld2 * (mz + 4);
+        const int mx_ = mx, my_ = my;
+        return [=](int m, int k0, int k1, const double* rows) {
+            double* dstp = host + fld * m;
+            par_rows((long)(k1 - k0) * my_, [&](long r0, long r1) {
+                for (long r = r0; r < r1; ++r) {
+                    const long kk = k0 + r / my_, j = r % my_;
+                    std::memcpy(dstp + 2 + ld1 * (j + ld2 * (kk + 2)), rows + r * mx_, sizeof(double) * mx_);
+                }
+            });
+            return true;
+        };
+    }
+    Status transfer_in(const double* host, long ld1, long ld2, T* const* dst, int nf, bool sub_eq) {
+        return stream_in(dst, nf, sub_eq, gather(host, ld1, ld2));
+    }
+    Status transfer_out(double* host, long ld1, long ld2, T* const* src, int nf, bool add_eq,
+                        T* const* comp = nullptr) {
+        return stream_out(src, nf, add_eq, comp, scatter(host, ld1, ld2));
+    }
+
+    Status state_in(const ChunkIn& fill) override {
+        Status s = stream_in(X, 8, true, fill);
         if (s.code) return s;
         if (KAHAN) for (int m = 0; m < 8; ++m) DASHA_CK(cudaMemsetAsync(C[m], 0, sizeof(T) * N, st));
         DASHA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
         DASHA_CK(cudaStreamSynchronize(st));
         return Status::ok();
     }
-    Status get_state(double* x, long ld1, long ld2) override {
-        return transfer_out(x, ld1, ld2, X, 8, true, KAHAN ? C : nullptr);
-    }
+    Status state_out(const ChunkOut& take) override { return stream_out(X, 8, true, KAHAN ? C : nullptr, take); }
+    Status set_state(const double* x, long ld1, long ld2) override { return state_in(gather(x, ld1, ld2)); }
+    Status get_state(double* x, long ld1, long ld2) override { return state_out(scatter(x, ld1, ld2)); }
 
     // ---- the RHS chain (right, t3dsdsc.f:1297-1673) ----
     static F8<T> f8(T* const* p) { F8<T> r; for (int m = 0; m < 8; ++m) r.f[m] = p[m]; return r; }

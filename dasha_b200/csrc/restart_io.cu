@@ -22,6 +22,7 @@
 //    reference opens unit 9 on every call and never closes it, so the lines of a run follow
 //    one another in the file.
 #include "dasha_capi.h"
+#include "fortran_records.h"
 
 #include <algorithm>
 #include <cmath>
@@ -35,82 +36,9 @@
 
 namespace {
 
-constexpr long kMaxSub = 2147483639L;   // gfortran's longest subrecord
-
-// Streams one logical record of known length as subrecords of at most maxsub bytes.
-struct RecWriter {
-    FILE* f;
-    long total, maxsub, done = 0, left_in_sub = 0, cur_open_len = 0;
-    bool ok = true, first = true;
-    RecWriter(FILE* f_, long total_, long maxsub_) : f(f_), total(total_), maxsub(maxsub_) {
-        if (total == 0) { open_sub(); close_sub(); }
-    }
-    void marker(int32_t v) { ok = ok && std::fwrite(&v, 4, 1, f) == 1; }
-    void open_sub() {
-        cur_open_len = std::min(total - done, maxsub);
-        left_in_sub = cur_open_len;
-        marker(done + cur_open_len < total ? -(int32_t)cur_open_len : (int32_t)cur_open_len);
-    }
-    void close_sub() {
-        marker(first ? (int32_t)cur_open_len : -(int32_t)cur_open_len);
-        first = false;
-    }
-    void put(const void* data, long n) {
-        const char* p = static_cast<const char*>(data);
-        while (n > 0 && ok) {
-            if (done >= total) { ok = false; break; }   // more data than the record holds
-            if (left_in_sub == 0) open_sub();
-            const long m = std::min(n, left_in_sub);
-            ok = ok && std::fwrite(p, 1, (size_t)m, f) == (size_t)m;
-            p += m; n -= m; done += m; left_in_sub -= m;
-            if (left_in_sub == 0) close_sub();
-        }
-    }
-    bool finish() const { return ok && done == total && left_in_sub == 0; }
-};
-
-// Reads one logical record that must hold exactly `total` bytes, subrecord by subrecord.
-struct RecReader {
-    FILE* f;
-    long total, done = 0, left_in_sub = 0, sub_len = 0;
-    bool ok = true, first = true, more = true;
-    RecReader(FILE* f_, long total_) : f(f_), total(total_) {
-        if (total == 0) { open_sub(); close_sub(); }
-    }
-    int32_t marker() {
-        int32_t v = 0;
-        ok = ok && std::fread(&v, 4, 1, f) == 1;
-        return v;
-    }
-    void open_sub() {
-        if (!more) { ok = false; return; }
-        const int32_t h = marker();
-        more = h < 0;
-        sub_len = more ? -(long)h : (long)h;
-        left_in_sub = sub_len;
-        if (done + sub_len > total) ok = false;
-    }
-    void close_sub() {
-        const int32_t t = marker();
-        if ((first ? (long)t : -(long)t) != sub_len) ok = false;
-        first = false;
-    }
-    void get(void* out, long n) {
-        char* p = static_cast<char*>(out);
-        while (n > 0 && ok) {
-            while (left_in_sub == 0 && ok) {   // zero-length subrecords carry nothing
-                open_sub();
-                if (ok && left_in_sub == 0) close_sub();
-            }
-            if (!ok) break;
-            const long m = std::min(n, left_in_sub);
-            ok = ok && std::fread(p, 1, (size_t)m, f) == (size_t)m;
-            p += m; n -= m; done += m; left_in_sub -= m;
-            if (left_in_sub == 0) close_sub();
-        }
-    }
-    bool finish() const { return ok && done == total && !more && left_in_sub == 0; }
-};
+using dasha::kMaxSubrecord;
+using dasha::RecReader;
+using dasha::RecWriter;
 
 // Powers of ten 1e-300 .. 1e300 as correctly rounded doubles (strtod), exact up to 1e22.
 struct Pow10 {
@@ -276,7 +204,7 @@ extern "C" {
 int dasha_restart_write(const char* path, int ncase, int nstep, double time, int nst, int mx, int my, int mz,
                         const double* x_f, long ld1, long ld2, long max_subrecord) {
     if (!path || !x_f || !dims_ok(mx, my, mz, ld1, ld2) || max_subrecord < 0) return DASHA_E_INVALID;
-    const long maxsub = max_subrecord == 0 ? kMaxSub : std::min(max_subrecord, kMaxSub);
+    const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
     FILE* f = std::fopen(path, "wb");
     if (!f) return DASHA_E_INVALID;
     bool ok = true;

@@ -121,16 +121,32 @@ def write_current_dat(path: str, diag: np.ndarray, time: float, append: bool = T
            f"current.dat write {path}")
 
 
-def checkpoint(d: "capi.Dasha", directory: str, ncase: int, nstep: int, time: float, nst: int) -> str:
-    """recrd for a GPU context: downloads the state and writes <directory>/mhdNNN000."""
+def checkpoint(d: "capi.Dasha", directory: str, ncase: int, nstep: int, time: float, nst: int,
+               max_subrecord: int = 0) -> str:
+    """recrd for a GPU context: streams the state into <directory>/mhdNNN000 (no full host copy)."""
     path = os.path.join(directory, restart_name(nst))
-    write_restart(path, ncase, nstep, time, nst, restart_array(d.get_state()))
+    d._check(d.lib.dasha_checkpoint(d.h, os.fsencode(path), ncase, nstep, float(time), nst, int(max_subrecord)))
     return path
 
 
 def restore(d: "capi.Dasha", directory: str, nst: int):
-    """readin for a GPU context: reads <directory>/mhdNNN000 and uploads its state; returns
+    """readin for a GPU context: streams <directory>/mhdNNN000 into the state; returns
     (ncase, nstep, time, nst) of the file."""
-    a, b, t, n, H = read_restart(os.path.join(directory, restart_name(nst)), d.mx, d.my, d.mz)
+    a, b, n = C.c_int(), C.c_int(), C.c_int()
+    t = C.c_double()
+    path = os.path.join(directory, restart_name(nst))
+    d._check(d.lib.dasha_restore(d.h, os.fsencode(path), C.byref(a), C.byref(b), C.byref(t), C.byref(n)))
+    return a.value, b.value, t.value, n.value
+
+
+def checkpoint_host(d: "capi.Dasha", path: str, ncase: int, nstep: int, time: float, nst: int,
+                    max_subrecord: int = 0):
+    """The same file through a full host copy of the state (dasha_get_state + dasha_restart_write)."""
+    write_restart(path, ncase, nstep, time, nst, restart_array(d.get_state()), max_subrecord)
+
+
+def restore_host(d: "capi.Dasha", path: str):
+    """The same state through a full host copy (dasha_restart_read + dasha_set_state)."""
+    a, b, t, n, H = read_restart(path, d.mx, d.my, d.mz)
     d.set_state(harris.from_halo(H, d.mx, d.my, d.mz))
     return a, b, t, n

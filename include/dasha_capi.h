@@ -95,6 +95,19 @@ int dasha_set_equilibrium_current(dasha_ctx* ctx, const double* j0);
 int dasha_set_state(dasha_ctx* ctx, const double* x_f, long ld1, long ld2);
 int dasha_get_state(dasha_ctx* ctx, double* x_f, long ld1, long ld2);
 
+/* The restart file of recrd / readin (t3dsdsc.f:4814-4861; the format of dasha_restart_write
+ * below) written from, or read into, the context's state without a full host copy: the state
+ * streams through the context's pinned chunk buffers, file I/O overlapped with the DMA.
+ * dasha_checkpoint writes what dasha_restart_write writes for the dasha_get_state array with
+ * the x halo holding the periodic copies and the z halo zeros; max_subrecord as there.
+ * dasha_restore checks the file's records against the grid before it replaces the state
+ * (a mismatch returns DASHA_E_INVALID with the state unchanged); it needs the equilibrium set
+ * and acts as dasha_set_state of the file's interior nodes.  An I/O error during the read
+ * leaves the context without a state (DASHA_E_STATE until the next set_state or restore). */
+int dasha_checkpoint(dasha_ctx* ctx, const char* path, int ncase, int nstep, double time, int nst,
+                     long max_subrecord);
+int dasha_restore(dasha_ctx* ctx, const char* path, int* ncase, int* nstep, double* time, int* nst);
+
 /* CFL time step of the current state (setdt, t3dsdsc.f:4694-4763): synchronises, returns dt.
  * Also reports a latched blow-up (DASHA_E_BLOWUP) and dt collapse (DASHA_E_DT_COLLAPSE,
  * dt < 0.1*dt0 with dt0 the first dt of the context, t3dsdsc.f:142). */

@@ -12,6 +12,9 @@ pytestmark = pytest.mark.gpu
 
 SMALL = harris.RunConfig("small-32x16x32", 32, 16, 32, False, 0.005, 0.5, 4)
 RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 4, dt_whistler=1)
+# 256x128 planes of 256 KB: the 64 MB transfer chunks hold 256 planes, so 300 planes make two
+# chunks per field on the streamed checkpoint and restore
+CHUNKS = harris.RunConfig("chunks-256x128x300", 256, 128, 300, False, 0.005, 0.5, 4)
 
 
 @pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
@@ -59,5 +62,56 @@ def test_restart_continues_the_run(tmp_path, precision, tol):
     xa, xb = a.get_state(), b.get_state()
     err = np.abs(xa - xb).reshape(8, -1).max(axis=1) / scale
     assert err.max() < tol, err
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("maxsub", [0, 1 << 20], ids=["one-subrecord", "1MiB-subrecords"])
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("cfg", [SMALL, CHUNKS], ids=lambda c: c.name)
+def test_streamed_checkpoint_equals_host_path(tmp_path, cfg, precision, maxsub):
+    d = capi.gem_context(cfg, precision)
+    t, _ = d.run(1)
+    p = restart.checkpoint(d, str(tmp_path), 2, 1, t, 5, max_subrecord=maxsub)
+    h = tmp_path / "host"
+    restart.checkpoint_host(d, str(h), 2, 1, t, 5, max_subrecord=maxsub)
+    assert open(p, "rb").read() == h.read_bytes()
+    d.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("cfg", [SMALL, CHUNKS], ids=lambda c: c.name)
+def test_streamed_restore_equals_host_path(tmp_path, cfg, precision):
+    a = capi.gem_context(cfg, precision)
+    t, _ = a.run(1)
+    restart.checkpoint_host(a, str(tmp_path / restart.restart_name(7)), 4, 1, t, 7, max_subrecord=1 << 20)
+    b = capi.gem_context(cfg, precision)
+    b.run(1)                                                   # a different state before the restore
+    assert restart.restore(b, str(tmp_path), 7) == (4, 1, t, 7)
+    c = capi.gem_context(cfg, precision)
+    assert restart.restore_host(c, str(tmp_path / restart.restart_name(7))) == (4, 1, t, 7)
+    assert np.array_equal(b.get_state(), c.get_state())
+    for x in (a, b, c):
+        x.close()
+
+
+def test_restore_rejects_a_mismatched_file_and_keeps_the_state(tmp_path):
+    a = capi.gem_context(SMALL, 0)
+    restart.checkpoint(a, str(tmp_path), 1, 0, 0.0, 1)
+    other = harris.RunConfig("small-64x16x32", 64, 16, 32, False, 0.005, 0.5, 4)
+    b = capi.gem_context(other, 0)
+    before = b.get_state()
+    with pytest.raises(capi.DashaError) as e:
+        restart.restore(b, str(tmp_path), 1)                   # another grid
+    assert e.value.code == capi.E_INVALID
+    assert np.array_equal(b.get_state(), before)
+    p = tmp_path / restart.restart_name(1)
+    p.write_bytes(p.read_bytes()[:-100])                       # truncated
+    before = a.get_state()
+    with pytest.raises(capi.DashaError) as e:
+        restart.restore(a, str(tmp_path), 1)
+    assert e.value.code == capi.E_INVALID
+    assert np.array_equal(a.get_state(), before)
+    a.setdt(0.0)                                               # the context still steps
     a.close()
     b.close()
