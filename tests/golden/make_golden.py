@@ -1,0 +1,60 @@
+"""Writes the golden fixtures of tests/golden/ from the CPU FP64 oracle (test infrastructure).
+
+For each seeded Harris/GEM case: the dt sequence of 4 reference steps (setdt, stepon), the
+diagnostics and the state after them, the smoothed current and one right-hand side of the
+initial state.  Volumes are kept as the mid-y plane (the plane the reference's outputs and
+diagnostics use) plus per-field sums and L2 norms over every node, so the fixtures stay small.
+
+    python tests/golden/make_golden.py          # rewrites tests/golden/*.npz
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from dasha_b200 import harris  # noqa: E402
+
+CASES = [
+    harris.RunConfig("golden-32x16x32-uniform", 32, 16, 32, False, 0.005, 0.5, 4),
+    harris.RunConfig("golden-32x16x40-sinh", 32, 16, 40, True, 0.003, 1.0, 4),
+]
+RHS_T = 0.5
+
+
+def volume_summary(F):
+    """Mid-y plane (nf, mz, mx), per-field sums and L2 norms of (nf, mz, my, mx)."""
+    my = F.shape[2]
+    flat = F.reshape(F.shape[0], -1)
+    return F[:, :, my // 2, :].copy(), flat.sum(axis=1), np.sqrt((flat * flat).sum(axis=1))
+
+
+def make(cfg):
+    from oracle.oracle import gem_oracle
+    o = gem_oracle(cfg)
+    x0 = o.get_state()
+    cur_plane, cur_sum, cur_l2 = volume_summary(o.current())
+    rhs_plane, rhs_sum, rhs_l2 = volume_summary(o.rhs(RHS_T))
+    _, dts = o.run(cfg.steps)
+    st_plane, st_sum, st_l2 = volume_summary(o.get_state())
+    out = dict(grid=np.array([cfg.mx, cfg.my, cfg.mz]), state0_sum=x0.reshape(8, -1).sum(axis=1),
+               current_plane=cur_plane, current_sum=cur_sum, current_l2=cur_l2,
+               rhs_t=np.array(RHS_T), rhs_plane=rhs_plane, rhs_sum=rhs_sum, rhs_l2=rhs_l2,
+               dts=dts, state_plane=st_plane, state_sum=st_sum, state_l2=st_l2, diag=o.diagnostics())
+    o.close()
+    return out
+
+
+def main():
+    for cfg in CASES:
+        path = os.path.join(HERE, cfg.name + ".npz")
+        np.savez_compressed(path, **make(cfg))
+        print(path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()
