@@ -81,6 +81,25 @@ static int from_status(dasha_ctx* c, const Status& s) {
     return fail(c, s.code, s.msg);
 }
 
+// Runs the body of an entry point: a host exception (allocation, thread start) becomes a
+// status, as no exception may cross the C-ABI.
+template <class F>
+static int host_call(dasha_ctx* c, F body) {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return fail(c, DASHA_E_NOMEM, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(c, DASHA_E_INVALID, std::string("host error: ") + e.what());
+    } catch (...) {
+        return fail(c, DASHA_E_INVALID, "host error");
+    }
+}
+template <class F>
+static int engine_call(dasha_ctx* c, F call) {
+    return host_call(c, [&] { return from_status(c, call()); });
+}
+
 extern "C" {
 
 int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_ctx** out) {
@@ -131,7 +150,7 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
                     double hp2 = a.at(i + 2) - x0, hm2 = x0 - a.at(i - 2);
                     double w1[4], w2[4];
                     if (!stencil_weights(hp1, hm1, hp2, hm2, 1, w1) || !stencil_weights(hp1, hm1, hp2, hm2, 2, w2)) {
-                        delete c; return DASHA_E_INVALID;
+                        cudaStreamDestroy(c->st); delete c; return DASHA_E_INVALID;
                     }
                     for (int q = 0; q < 4; ++q) { H.coef[d][q][i] = w1[q]; H.coef[d][4 + q][i] = w2[q]; }
                 }
@@ -197,8 +216,7 @@ int dasha_set_equilibrium_current(dasha_ctx* c, const double* j0) {
     CAPI_GUARD(c);
     if (!j0) return fail(c, DASHA_E_INVALID, "null j0");
     if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium first");
-    try { return from_status(c, c->eng->set_j0(j0)); }
-    catch (...) { return fail(c, DASHA_E_NOMEM, "host allocation failed"); }
+    return engine_call(c, [&] { return c->eng->set_j0(j0); });
 }
 
 static int check_ld(dasha_ctx* c, const void* p, long ld1, long ld2) {
@@ -211,7 +229,7 @@ int dasha_set_state(dasha_ctx* c, const double* x_f, long ld1, long ld2) {
     CAPI_GUARD(c);
     if (int rc = check_ld(c, x_f, ld1, ld2)) return rc;
     if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium before the state");
-    int rc = from_status(c, c->eng->set_state(x_f, ld1, ld2));
+    int rc = engine_call(c, [&] { return c->eng->set_state(x_f, ld1, ld2); });
     if (rc == DASHA_OK) c->state_set = true;
     return rc;
 }
@@ -220,7 +238,7 @@ int dasha_get_state(dasha_ctx* c, double* x_f, long ld1, long ld2) {
     CAPI_GUARD(c);
     if (int rc = check_ld(c, x_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    return from_status(c, c->eng->get_state(x_f, ld1, ld2));
+    return engine_call(c, [&] { return c->eng->get_state(x_f, ld1, ld2); });
 }
 
 // Restart file of recrd / readin (t3dsdsc.f:4814-4861) streamed to or from the device state in
@@ -232,26 +250,21 @@ int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, doubl
     CAPI_GUARD(c);
     if (!path || max_subrecord < 0) return fail(c, DASHA_E_INVALID, "bad checkpoint arguments");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
-    FILE* f = std::fopen(path, "wb");
-    if (!f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
-    const int mx = c->mx, my = c->my, mz = c->mz;
-    const long row = mx + 4;
-    unsigned char hdr[20];
-    const int32_t a = ncase, b = nstep, d = nst;
-    std::memcpy(hdr, &a, 4);
-    std::memcpy(hdr + 4, &b, 4);
-    std::memcpy(hdr + 8, &time, 8);
-    std::memcpy(hdr + 16, &d, 4);
-    RecWriter w1(f, 20, maxsub);
-    w1.put(hdr, 20);
-    bool ok = w1.finish();
-    RecWriter w(f, (long)sizeof(double) * row * my * (mz + 4) * 8, maxsub);
-    std::vector<double> rb(row), zero(row, 0.0);
-    auto zplanes = [&]() { for (long r = 0; r < 2L * my && w.ok; ++r) w.put(zero.data(), (long)sizeof(double) * row); };
-    int rc = DASHA_OK;
-    if (ok) {
-        rc = from_status(c, c->eng->state_out([&](int, int k0, int k1, const double* rows) {
+    return host_call(c, [&]() -> int {
+        const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
+        File f(path, "wb");
+        if (!f.f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
+        const int mx = c->mx, my = c->my, mz = c->mz;
+        const long row = mx + 4;
+        unsigned char hdr[20];
+        pack_restart_header(hdr, ncase, nstep, time, nst);
+        RecWriter w1(f.f, 20, maxsub);
+        w1.put(hdr, 20);
+        if (!w1.finish()) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
+        RecWriter w(f.f, (long)sizeof(double) * row * my * (mz + 4) * 8, maxsub);
+        std::vector<double> rb(row), zero(row, 0.0);
+        auto zplanes = [&]() { for (long r = 0; r < 2L * my && w.ok; ++r) w.put(zero.data(), (long)sizeof(double) * row); };
+        const int rc = from_status(c, c->eng->state_out([&](int, int k0, int k1, const double* rows) {
             if (k0 == 0) zplanes();
             for (long r = 0; r < (long)(k1 - k0) * my && w.ok; ++r) {
                 const double* v = rows + r * mx;
@@ -263,58 +276,50 @@ int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, doubl
             if (k1 == mz) zplanes();
             return w.ok;
         }));
-        ok = w.finish();
-    }
-    const bool closed = std::fclose(f) == 0;
-    if (rc != DASHA_OK) return rc;
-    if (!ok || !closed) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
-    return DASHA_OK;
+        if (rc != DASHA_OK) return rc;
+        const bool ok = w.finish();
+        if (!f.close() || !ok) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
+        return DASHA_OK;
+    });
 }
 
 int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double* time, int* nst) {
     CAPI_GUARD(c);
     if (!path || !ncase || !nstep || !time || !nst) return fail(c, DASHA_E_INVALID, "bad restore arguments");
     if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium before the state");
-    FILE* f = std::fopen(path, "rb");
-    if (!f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
-    const int mx = c->mx, my = c->my, mz = c->mz;
-    const long row = mx + 4, total = (long)sizeof(double) * row * my * (mz + 4) * 8;
-    unsigned char hdr[20];
-    RecReader r1(f, 20);
-    r1.get(hdr, 20);
-    // the markers of record 2 are checked before the device state is touched
-    if (!r1.finish() || !scan_record(f, total)) {
-        std::fclose(f);
-        return fail(c, DASHA_E_INVALID, std::string(path) + " is not a restart file of this grid");
-    }
-    RecReader r(f, total);
-    std::vector<double> rb(row), skip(row);
-    auto zplanes = [&]() { for (long q = 0; q < 2L * my && r.ok; ++q) r.get(skip.data(), (long)sizeof(double) * row); };
-    int rc = from_status(c, c->eng->state_in([&](int, int k0, int k1, double* rows) {
-        if (k0 == 0) zplanes();
-        for (long q = 0; q < (long)(k1 - k0) * my && r.ok; ++q) {
-            r.get(rb.data(), (long)sizeof(double) * row);
-            std::memcpy(rows + q * mx, rb.data() + 2, sizeof(double) * mx);
-        }
-        if (k1 == mz) zplanes();
-        return r.ok;
-    }));
-    const bool ok = rc == DASHA_OK && r.finish();
-    std::fclose(f);
-    if (!ok) {
-        c->state_set = false;   // part of the state may have been replaced
-        return rc != DASHA_OK ? rc : fail(c, DASHA_E_INVALID, std::string("reading ") + path + " failed");
-    }
-    int32_t a, b, d;
-    std::memcpy(&a, hdr, 4);
-    std::memcpy(&b, hdr + 4, 4);
-    std::memcpy(time, hdr + 8, 8);
-    std::memcpy(&d, hdr + 16, 4);
-    *ncase = a;
-    *nstep = b;
-    *nst = d;
-    c->state_set = true;
-    return DASHA_OK;
+    bool touched = false;   // set once the device state starts to change
+    const int rc = host_call(c, [&]() -> int {
+        File f(path, "rb");
+        if (!f.f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
+        const int mx = c->mx, my = c->my, mz = c->mz;
+        const long row = mx + 4, total = (long)sizeof(double) * row * my * (mz + 4) * 8;
+        unsigned char hdr[20];
+        RecReader r1(f.f, 20);
+        r1.get(hdr, 20);
+        // the markers of record 2 are checked before the device state is touched
+        if (!r1.finish() || !scan_record(f.f, total))
+            return fail(c, DASHA_E_INVALID, std::string(path) + " is not a restart file of this grid");
+        RecReader r(f.f, total);
+        std::vector<double> rb(row), skip(row);
+        auto zplanes = [&]() { for (long q = 0; q < 2L * my && r.ok; ++q) r.get(skip.data(), (long)sizeof(double) * row); };
+        touched = true;
+        const int rc2 = from_status(c, c->eng->state_in([&](int, int k0, int k1, double* rows) {
+            if (k0 == 0) zplanes();
+            for (long q = 0; q < (long)(k1 - k0) * my && r.ok; ++q) {
+                r.get(rb.data(), (long)sizeof(double) * row);
+                std::memcpy(rows + q * mx, rb.data() + 2, sizeof(double) * mx);
+            }
+            if (k1 == mz) zplanes();
+            return r.ok;
+        }));
+        if (rc2 != DASHA_OK) return rc2;
+        if (!r.finish()) return fail(c, DASHA_E_INVALID, std::string("reading ") + path + " failed");
+        unpack_restart_header(hdr, ncase, nstep, time, nst);
+        return DASHA_OK;
+    });
+    if (rc == DASHA_OK) c->state_set = true;
+    else if (touched) c->state_set = false;   // part of the state may have been replaced
+    return rc;
 }
 
 int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {
@@ -324,7 +329,7 @@ int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     int blowup = 0;
     double dt = 0.;
-    int rc = from_status(c, c->eng->setdt(&dt, &blowup));
+    int rc = engine_call(c, [&] { return c->eng->setdt(&dt, &blowup); });
     if (rc) return rc;
     *dt_out = dt;
     if (blowup) return fail(c, DASHA_E_BLOWUP, "max Jy on the mid-y plane reached 1e7 (or is not finite)");
@@ -338,35 +343,35 @@ int dasha_stepon(dasha_ctx* c, double time, double dt, int nstep) {
     CAPI_GUARD(c);
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DASHA_E_INVALID, "dt must be positive and finite");
-    return from_status(c, c->eng->stepon(time, dt, nstep));
+    return engine_call(c, [&] { return c->eng->stepon(time, dt, nstep); });
 }
 
 int dasha_current(dasha_ctx* c, double* cur_f, long ld1, long ld2) {
     CAPI_GUARD(c);
     if (int rc = check_ld(c, cur_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    return from_status(c, c->eng->current(cur_f, ld1, ld2));
+    return engine_call(c, [&] { return c->eng->current(cur_f, ld1, ld2); });
 }
 
 int dasha_midplane(dasha_ctx* c, double* plane) {
     CAPI_GUARD(c);
     if (!plane) return fail(c, DASHA_E_INVALID, "null plane");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    return from_status(c, c->eng->midplane(plane));
+    return engine_call(c, [&] { return c->eng->midplane(plane); });
 }
 
 int dasha_rhs(dasha_ctx* c, double t, double* xdif_f, long ld1, long ld2) {
     CAPI_GUARD(c);
     if (int rc = check_ld(c, xdif_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    return from_status(c, c->eng->rhs(t, xdif_f, ld1, ld2));
+    return engine_call(c, [&] { return c->eng->rhs(t, xdif_f, ld1, ld2); });
 }
 
 int dasha_diagnostics(dasha_ctx* c, double* out) {
     CAPI_GUARD(c);
     if (!out) return fail(c, DASHA_E_INVALID, "null out");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    return from_status(c, c->eng->diagnostics(out));
+    return engine_call(c, [&] { return c->eng->diagnostics(out); });
 }
 
 int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int snaps, double* dPhi_deta,
@@ -376,7 +381,7 @@ int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int 
         return fail(c, DASHA_E_INVALID, "bad adjoint arguments");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     if (c->P.precision != 0) return fail(c, DASHA_E_UNSUPPORTED, "the adjoint runs on FP64 contexts only");
-    return from_status(c, c->eng->adjoint_flux_grad(nsteps, dt_seq, snaps, dPhi_deta, dPhi_dpsi));
+    return engine_call(c, [&] { return c->eng->adjoint_flux_grad(nsteps, dt_seq, snaps, dPhi_deta, dPhi_dpsi); });
 }
 
 int dasha_adjoint_rhs(dasha_ctx* c, const double* w_f, double* out_f, long ld1, long ld2) {
@@ -384,7 +389,7 @@ int dasha_adjoint_rhs(dasha_ctx* c, const double* w_f, double* out_f, long ld1, 
     if (int rc = check_ld(c, w_f, ld1, ld2)) return rc;
     if (int rc = check_ld(c, out_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
-    return from_status(c, c->eng->adjoint_rhs(w_f, out_f, ld1, ld2));
+    return engine_call(c, [&] { return c->eng->adjoint_rhs(w_f, out_f, ld1, ld2); });
 }
 
 int dasha_timer(dasha_ctx* c, int op, double* ms) {

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cstring>
 
 namespace dasha {
 
@@ -110,5 +111,39 @@ inline bool scan_record(FILE* f, long total) {
     if (start >= 0) std::fseek(f, start, SEEK_SET);
     return ok;
 }
+
+// Record 1 of the restart file: ncase, nstep (INTEGER*4), time (REAL*8), nst (INTEGER*4).
+inline void pack_restart_header(unsigned char* h, int ncase, int nstep, double time, int nst) {
+    const int32_t a = ncase, b = nstep, d = nst;
+    std::memcpy(h, &a, 4);
+    std::memcpy(h + 4, &b, 4);
+    std::memcpy(h + 8, &time, 8);
+    std::memcpy(h + 16, &d, 4);
+}
+inline void unpack_restart_header(const unsigned char* h, int* ncase, int* nstep, double* time, int* nst) {
+    int32_t a, b, d;
+    std::memcpy(&a, h, 4);
+    std::memcpy(&b, h + 4, 4);
+    std::memcpy(time, h + 8, 8);
+    std::memcpy(&d, h + 16, 4);
+    *ncase = a;
+    *nstep = b;
+    *nst = d;
+}
+
+// A FILE* closed when it leaves scope (also when an exception passes); close() reports whether
+// the buffered data reached the file.
+struct File {
+    FILE* f = nullptr;
+    File(const char* path, const char* mode) : f(std::fopen(path, mode)) {}
+    File(const File&) = delete;
+    File& operator=(const File&) = delete;
+    ~File() { if (f) std::fclose(f); }
+    bool close() {
+        const bool ok = f && !std::ferror(f) && std::fclose(f) == 0;
+        f = nullptr;
+        return ok;
+    }
+};
 
 }  // namespace dasha

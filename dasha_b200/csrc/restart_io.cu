@@ -30,13 +30,17 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
 
 namespace {
 
+using dasha::File;
 using dasha::kMaxSubrecord;
+using dasha::pack_restart_header;
+using dasha::unpack_restart_header;
 using dasha::RecReader;
 using dasha::RecWriter;
 
@@ -199,29 +203,35 @@ bool dims_ok(int mx, int my, int mz, long ld1, long ld2) {
 
 }  // namespace
 
+// Runs the body of an entry point: a host exception (allocation, thread start) becomes a
+// status, as no exception may cross the C-ABI.
+template <class F>
+static int guarded(F body) {
+    try {
+        return body();
+    } catch (const std::bad_alloc&) {
+        return DASHA_E_NOMEM;
+    } catch (...) {
+        return DASHA_E_INVALID;
+    }
+}
+
 extern "C" {
 
 int dasha_restart_write(const char* path, int ncase, int nstep, double time, int nst, int mx, int my, int mz,
                         const double* x_f, long ld1, long ld2, long max_subrecord) {
     if (!path || !x_f || !dims_ok(mx, my, mz, ld1, ld2) || max_subrecord < 0) return DASHA_E_INVALID;
-    const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
-    FILE* f = std::fopen(path, "wb");
-    if (!f) return DASHA_E_INVALID;
-    bool ok = true;
-    {
+    return guarded([&]() -> int {
+        const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
+        File f(path, "wb");
+        if (!f.f) return DASHA_E_INVALID;
         unsigned char hdr[20];
-        const int32_t a = ncase, b = nstep, d = nst;
-        std::memcpy(hdr, &a, 4);
-        std::memcpy(hdr + 4, &b, 4);
-        std::memcpy(hdr + 8, &time, 8);
-        std::memcpy(hdr + 16, &d, 4);
-        RecWriter w(f, 20, maxsub);
-        w.put(hdr, 20);
-        ok = w.finish();
-    }
-    if (ok) {
+        pack_restart_header(hdr, ncase, nstep, time, nst);
+        RecWriter w1(f.f, 20, maxsub);
+        w1.put(hdr, 20);
+        if (!w1.finish()) return DASHA_E_INVALID;
         const long row = mx + 4, nrow = (long)my * (mz + 4) * 8;
-        RecWriter w(f, (long)sizeof(double) * row * nrow, maxsub);
+        RecWriter w(f.f, (long)sizeof(double) * row * nrow, maxsub);
         if (ld1 == row && ld2 == my) {
             w.put(x_f, (long)sizeof(double) * row * nrow);
         } else {
@@ -230,27 +240,23 @@ int dasha_restart_write(const char* path, int ncase, int nstep, double time, int
                     for (int j = 0; j < my; ++j)
                         w.put(x_f + ld1 * ((long)j + ld2 * ((long)kk + (long)(mz + 4) * m)), (long)sizeof(double) * row);
         }
-        ok = w.finish();
-    }
-    const bool closed = std::fclose(f) == 0;
-    return ok && closed ? DASHA_OK : DASHA_E_INVALID;
+        const bool ok = w.finish();
+        return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
+    });
 }
 
 int dasha_restart_read(const char* path, int* ncase, int* nstep, double* time, int* nst, int mx, int my, int mz,
                        double* x_f, long ld1, long ld2) {
     if (!path || !ncase || !nstep || !time || !nst || !x_f || !dims_ok(mx, my, mz, ld1, ld2)) return DASHA_E_INVALID;
-    FILE* f = std::fopen(path, "rb");
-    if (!f) return DASHA_E_INVALID;
-    unsigned char hdr[20];
-    bool ok;
-    {
-        RecReader r(f, 20);
-        r.get(hdr, 20);
-        ok = r.finish();
-    }
-    if (ok) {
+    return guarded([&]() -> int {
+        File f(path, "rb");
+        if (!f.f) return DASHA_E_INVALID;
+        unsigned char hdr[20];
+        RecReader r1(f.f, 20);
+        r1.get(hdr, 20);
+        if (!r1.finish()) return DASHA_E_INVALID;
         const long row = mx + 4, nrow = (long)my * (mz + 4) * 8;
-        RecReader r(f, (long)sizeof(double) * row * nrow);
+        RecReader r(f.f, (long)sizeof(double) * row * nrow);
         if (ld1 == row && ld2 == my) {
             r.get(x_f, (long)sizeof(double) * row * nrow);
         } else {
@@ -259,73 +265,67 @@ int dasha_restart_read(const char* path, int* ncase, int* nstep, double* time, i
                     for (int j = 0; j < my; ++j)
                         r.get(x_f + ld1 * ((long)j + ld2 * ((long)kk + (long)(mz + 4) * m)), (long)sizeof(double) * row);
         }
-        ok = r.finish();
-    }
-    std::fclose(f);
-    if (!ok) return DASHA_E_INVALID;
-    int32_t a, b, d;
-    std::memcpy(&a, hdr, 4);
-    std::memcpy(&b, hdr + 4, 4);
-    std::memcpy(time, hdr + 8, 8);
-    std::memcpy(&d, hdr + 16, 4);
-    *ncase = a;
-    *nstep = b;
-    *nst = d;
-    return DASHA_OK;
+        if (!r.finish()) return DASHA_E_INVALID;
+        unpack_restart_header(hdr, ncase, nstep, time, nst);
+        return DASHA_OK;
+    });
 }
 
 int dasha_m2d_write(const char* path, int mx, int mz, double time, const double* xc, const double* zc,
                     const double* plane) {
     if (!path || mx <= 0 || mz <= 0 || !xc || !zc || !plane) return DASHA_E_INVALID;
-    FILE* f = std::fopen(path, "w");
-    if (!f) return DASHA_E_INVALID;
-    const int hdr[3] = {2, mx, mz};
-    ld_ints(f, hdr, 3);
-    ld_real(f, time);
-    bool ok = write_list(f, (long)mx + mz, 5, 14, 5, 3, [&](long n) { return n < mx ? xc[n] : zc[n - mx]; });
-    const long np = (long)mx * mz;
-    for (int q = 0; q < 11 && ok; ++q) {
-        const int iq = q + 1;
-        ld_ints(f, &iq, 1);
-        const double* p = plane + (size_t)q * np;
-        ok = write_list(f, np, 5, 14, 5, 3, [&](long n) { return p[n]; });
-    }
-    ok = ok && !std::ferror(f);
-    return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
+    return guarded([&]() -> int {
+        File f(path, "w");
+        if (!f.f) return DASHA_E_INVALID;
+        const int hdr[3] = {2, mx, mz};
+        ld_ints(f.f, hdr, 3);
+        ld_real(f.f, time);
+        bool ok = write_list(f.f, (long)mx + mz, 5, 14, 5, 3, [&](long n) { return n < mx ? xc[n] : zc[n - mx]; });
+        const long np = (long)mx * mz;
+        for (int q = 0; q < 11 && ok; ++q) {
+            const int iq = q + 1;
+            ld_ints(f.f, &iq, 1);
+            const double* p = plane + (size_t)q * np;
+            ok = write_list(f.f, np, 5, 14, 5, 3, [&](long n) { return p[n]; });
+        }
+        return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
+    });
 }
 
 int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const double* xc, const double* yc,
                     const double* zc, const double* x_f, const double* cur_f, long ld1, long ld2) {
     if (!path || !xc || !yc || !zc || !x_f || !cur_f || !dims_ok(mx, my, mz, ld1, ld2)) return DASHA_E_INVALID;
-    FILE* f = std::fopen(path, "w");
-    if (!f) return DASHA_E_INVALID;
-    const int hdr[4] = {3, mx, my, mz};
-    ld_ints(f, hdr, 4);
-    ld_real(f, time);
-    bool ok = write_list(f, (long)mx + my + mz, 11, 10, 4, 0, [&](long n) {
-        return n < mx ? xc[n] : (n < (long)mx + my ? yc[n - mx] : zc[n - mx - my]);
-    });
-    const long mxy = (long)mx * my, nv = mxy * mz;
-    for (int q = 0; q < 11 && ok; ++q) {
-        const int iq = q + 1;
-        ld_ints(f, &iq, 1);
-        ok = write_list(f, nv, 11, 10, 4, 0, [&](long n) {
-            const int i = (int)(n % mx), j = (int)((n / mx) % my), k = (int)(n / mxy);
-            return out_field(x_f, cur_f, ld1, ld2, mz, q, i, j, k);
+    return guarded([&]() -> int {
+        File f(path, "w");
+        if (!f.f) return DASHA_E_INVALID;
+        const int hdr[4] = {3, mx, my, mz};
+        ld_ints(f.f, hdr, 4);
+        ld_real(f.f, time);
+        bool ok = write_list(f.f, (long)mx + my + mz, 11, 10, 4, 0, [&](long n) {
+            return n < mx ? xc[n] : (n < (long)mx + my ? yc[n - mx] : zc[n - mx - my]);
         });
-    }
-    ok = ok && !std::ferror(f);
-    return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
+        const long mxy = (long)mx * my, nv = mxy * mz;
+        for (int q = 0; q < 11 && ok; ++q) {
+            const int iq = q + 1;
+            ld_ints(f.f, &iq, 1);
+            ok = write_list(f.f, nv, 11, 10, 4, 0, [&](long n) {
+                const int i = (int)(n % mx), j = (int)((n / mx) % my), k = (int)(n / mxy);
+                return out_field(x_f, cur_f, ld1, ld2, mz, q, i, j, k);
+            });
+        }
+        return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
+    });
 }
 
 int dasha_current_dat_write(const char* path, const double* diag, double time, int append) {
     if (!path || !diag) return DASHA_E_INVALID;
-    FILE* f = std::fopen(path, append ? "a" : "w");
-    if (!f) return DASHA_E_INVALID;
-    const double v[7] = {diag[3], diag[4], diag[5], diag[6], diag[7], diag[8], time};
-    bool ok = write_list(f, 7, 7, 13, 4, 0, [&](long n) { return v[n]; });
-    ok = ok && !std::ferror(f);
-    return std::fclose(f) == 0 && ok ? DASHA_OK : DASHA_E_INVALID;
+    return guarded([&]() -> int {
+        File f(path, append ? "a" : "w");
+        if (!f.f) return DASHA_E_INVALID;
+        const double v[7] = {diag[3], diag[4], diag[5], diag[6], diag[7], diag[8], time};
+        const bool ok = write_list(f.f, 7, 7, 13, 4, 0, [&](long n) { return v[n]; });
+        return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
+    });
 }
 
 int dasha_midplane_host(int mx, int my, int mz, const double* x_f, const double* cur_f, long ld1, long ld2,
