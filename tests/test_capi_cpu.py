@@ -30,6 +30,27 @@ def test_library_exports_every_declared_symbol():
         assert n in capi.SIGNATURES, n
 
 
+def test_product_never_uses_the_oracle():
+    """The package neither imports nor loads the oracle (only tests/, __graft_entry__.smoke()
+    and bench.py's CPU legs may), and the built library carries none of its symbols."""
+    import ast
+    import glob
+    for path in glob.glob(os.path.join(ROOT, "dasha_b200", "**", "*.py"), recursive=True):
+        for node in ast.walk(ast.parse(open(path).read())):
+            if isinstance(node, ast.Import):
+                names = [a.name for a in node.names]
+            elif isinstance(node, ast.ImportFrom):
+                names = [node.module or ""]
+            else:
+                continue
+            assert not any(n.split(".")[0] == "oracle" for n in names), path
+    for path in glob.glob(os.path.join(ROOT, "dasha_b200", "csrc", "*")):
+        assert "liboracle" not in open(path, errors="ignore").read(), path
+    lib = capi.load()
+    for sym in ("oracle_create", "oracle_stepon", "oracle_setdt"):
+        assert not hasattr(lib, sym), sym
+
+
 def test_missing_library_fails_loudly(tmp_path):
     saved = capi._lib
     capi._lib = None
