@@ -17,6 +17,9 @@
 //    11(1X,E10.4) (m3d), a new line after every 5 or 11 numbers and at the end of each list.
 //    Fields: 1 rho, 2-4 v = (rho v)/rho, 5-7 B, 8 p (totals), 9-11 the current density; m2d
 //    holds the plane j = my/2 (0-based; nyh = my/2+1 in the reference).
+//  - The main loop's step logs (t3dsdsc.f:157-181): ./data/stepnm, one list-directed line
+//    "nstep time dt" appended before each step, and unit 20 (fort.20), one line
+//    2(1X,F10.5),1X,I5 of dt, time and nstep after it.
 //  - current.dat of diagn (t3dsdsc.f:1226-1232): one line per call, the mid-y-plane extrema
 //    Jx max, Jx min, Jy max, Jy min, Jz max, Jz min and time in the format 7(1X,E13.4).  The
 //    reference opens unit 9 on every call and never closes it, so the lines of a run follow
@@ -138,6 +141,31 @@ void fmt_e(char* out, double v, int w, int d, int edig) {
     n += nex;
     std::memset(out, ' ', w - n);
     std::memcpy(out + w - n, body, n);
+}
+
+// Fortran Fw.d output editing of v: correctly rounded to d decimals (snprintf), right-justified;
+// the optional zero before the point is dropped only when the field would not fit otherwise;
+// a field that does not fit is w asterisks.  Writes exactly w characters, no terminator.
+void fmt_f(char* out, double v, int w, int d) {
+    char s[512];
+    int n = std::snprintf(s, sizeof s, "%.*f", d, v);
+    const char* p = s;
+    if (n > w && (std::strncmp(s, "0.", 2) == 0 || std::strncmp(s, "-0.", 3) == 0)) {
+        if (s[0] == '-') { s[1] = '-'; p = s + 1; } else p = s + 1;
+        --n;
+    }
+    if (n > w || n < 0 || !std::isfinite(v)) { std::memset(out, '*', w); return; }
+    std::memset(out, ' ', w - n);
+    std::memcpy(out + w - n, p, n);
+}
+
+// Fortran Iw output editing: right-justified, w asterisks when it does not fit.
+void fmt_i(char* out, long v, int w) {
+    char s[32];
+    const int n = std::snprintf(s, sizeof s, "%ld", v);
+    if (n > w) { std::memset(out, '*', w); return; }
+    std::memset(out, ' ', w - n);
+    std::memcpy(out + w - n, s, n);
 }
 
 // One output list under the format r(1X,Ew.d[Ee]): records of r items; `value(n)` gives item n.
@@ -324,6 +352,34 @@ int dasha_current_dat_write(const char* path, const double* diag, double time, i
         if (!f.f) return DASHA_E_INVALID;
         const double v[7] = {diag[3], diag[4], diag[5], diag[6], diag[7], diag[8], time};
         const bool ok = write_list(f.f, 7, 7, 13, 4, 0, [&](long n) { return v[n]; });
+        return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
+    });
+}
+
+int dasha_stepnm_write(const char* path, int nstep, double time, double dt) {
+    if (!path) return DASHA_E_INVALID;
+    return guarded([&]() -> int {
+        File f(path, "a");
+        if (!f.f) return DASHA_E_INVALID;
+        std::fprintf(f.f, " %11d %24.16E %24.16E\n", nstep, time, dt);
+        return f.close() ? DASHA_OK : DASHA_E_INVALID;
+    });
+}
+
+int dasha_dtlog_write(const char* path, double dt, double time, int nstep) {
+    if (!path) return DASHA_E_INVALID;
+    return guarded([&]() -> int {
+        File f(path, "a");
+        if (!f.f) return DASHA_E_INVALID;
+        char line[40];
+        line[0] = ' ';
+        fmt_f(line + 1, dt, 10, 5);
+        line[11] = ' ';
+        fmt_f(line + 12, time, 10, 5);
+        line[22] = ' ';
+        fmt_i(line + 23, nstep, 5);
+        line[28] = '\n';
+        const bool ok = std::fwrite(line, 1, 29, f.f) == 29;
         return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
     });
 }

@@ -8,6 +8,7 @@
 * `write_m2d` / `write_m3d`: the ASCII files data/m2dNNN.dat and data/m3dNNN of recrd2 / recrd3
   (t3dsdsc.f:4965-5412); `Dasha.midplane()` gives the eleven mid-plane fields from the GPU.
 * `write_current_dat`: the line diagn appends to current.dat (t3dsdsc.f:1226-1232).
+* `write_step_logs`: the main loop's stepnm and unit-20 lines (t3dsdsc.f:157-181).
 
 Arrays follow `harris.to_halo`: C-order (nf, mz+4, ld2, ld1) == Fortran x(ld1, ld2, mz+4, nf).
 Everything goes through the C library; without it every call raises.
@@ -119,6 +120,14 @@ def write_current_dat(path: str, diag: np.ndarray, time: float, append: bool = T
     assert diag.size >= capi.NDIAG
     _check(lib.dasha_current_dat_write(os.fsencode(path), capi._dp(diag), float(time), 1 if append else 0),
            f"current.dat write {path}")
+
+
+def write_step_logs(stepnm_path: str, dtlog_path: str, nstep: int, time: float, dt: float):
+    """The main loop's two per-step lines (t3dsdsc.f:157-181): stepnm gets (nstep, time, dt) as
+    before the step, the unit-20 log (dt, time + dt, nstep + 1) as after it."""
+    lib = capi.load()
+    _check(lib.dasha_stepnm_write(os.fsencode(stepnm_path), nstep, float(time), float(dt)), "stepnm write")
+    _check(lib.dasha_dtlog_write(os.fsencode(dtlog_path), float(dt), float(time + dt), nstep + 1), "dt log write")
 
 
 def checkpoint(d: "capi.Dasha", directory: str, ncase: int, nstep: int, time: float, nst: int,

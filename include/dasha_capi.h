@@ -227,6 +227,13 @@ int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const
  * call of a run), 1 adds the line at its end. */
 int dasha_current_dat_write(const char* path, const double* diag, double time, int append);
 
+/* The main loop's step logs (t3dsdsc.f:157-181), each call appending one line:
+ * dasha_stepnm_write: ./data/stepnm, "nstep time dt" before the step (list-directed; integers in
+ * 12 columns, reals with 17 significant digits); dasha_dtlog_write: unit 20 (fort.20), dt, time
+ * and nstep after the step in the format 2(1X,F10.5),1X,I5. */
+int dasha_stepnm_write(const char* path, int nstep, double time, double dt);
+int dasha_dtlog_write(const char* path, double dt, double time, int nstep);
+
 const char* dasha_last_error(dasha_ctx* ctx);
 void dasha_destroy(dasha_ctx* ctx);
 

@@ -11,6 +11,8 @@ unformatted records and for E editing, and gfortran's published record layout.
   lines (written here as the library writes them: integers in 12 columns, the time with 17
   significant digits), then lists under 5(1X,E14.5E3) or 11(1X,E10.4).
 * current.dat (diagn, t3dsdsc.f:1226-1232): 7(1X,E13.4) per line.
+* the main loop's step logs (t3dsdsc.f:157-181): stepnm (list-directed) and unit 20,
+  2(1X,F10.5),1X,I5.
 * the eleven output fields (t3dsdsc.f:5009-5110): bl 1..8 = x at the plane nyh = my/2+1,
   bl 2..4 divided by bl 1, bl 9..11 = cur.
 """
@@ -104,6 +106,38 @@ def e_edit(v: float, w: int, d: int, e: int | None = None) -> str:
     if len(body) + 1 <= w:
         body = ("-" if neg else "") + "0." + digits + exs
     return body.rjust(w)
+
+
+def f_edit(v: float, w: int, d: int) -> str:
+    """Fortran Fw.d output of v: rounded half-even on the exact value to d decimals, the zero
+    before the point dropped only when the field would not fit otherwise, else asterisks."""
+    v = float(v)
+    if v != v or v in (float("inf"), float("-inf")):
+        return "*" * w
+    with localcontext() as ctx:
+        ctx.prec = 1200
+        q = Decimal(v).quantize(Decimal(1).scaleb(-d), rounding=ROUND_HALF_EVEN)
+    s = f"{q:f}"
+    if np.signbit(v) and not s.startswith("-"):
+        s = "-" + s                       # -0.0 and negatives that round to zero keep the sign
+    if len(s) > w and (s.startswith("0.") or s.startswith("-0.")):
+        s = s.replace("0.", ".", 1)
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def i_edit(v: int, w: int) -> str:
+    s = str(int(v))
+    return s.rjust(w) if len(s) <= w else "*" * w
+
+
+def stepnm_line(nstep: int, time: float, dt: float) -> str:
+    """write(16,*) nstep, time, dt (t3dsdsc.f:167), in the library's list-directed form."""
+    return f" {nstep:11d} {time:24.16E} {dt:24.16E}\n"
+
+
+def dtlog_line(dt: float, time: float, nstep: int) -> str:
+    """write(20,10) dt, time, nstep with 10 format(2(1x,f10.5),1x,i5) (t3dsdsc.f:177-178)."""
+    return " " + f_edit(dt, 10, 5) + " " + f_edit(time, 10, 5) + " " + i_edit(nstep, 5) + "\n"
 
 
 def format_list(values, per_line: int, w: int, d: int, e: int | None = None) -> str:

@@ -241,6 +241,29 @@ def test_formatting_matches_exact_decimal_conversion(tmp_path):
     assert "\n".join(got) + "\n" == fio.format_list(list(vals) + [0.0, 0.0], 11, 10, 4)
 
 
+def test_step_logs(tmp_path):
+    """The main loop's stepnm and unit-20 lines against the oracle, over a run whose step count
+    passes 99999 (I5 turns to asterisks there) and whose time passes 99999.99999 (F10.5 does)."""
+    KAT_F10_5 = [(0.123456, "   0.12346"), (1234.5, "1234.50000"), (-1234.5, "**********"), (-0.0, "  -0.00000"),
+                 (99999.999996, "**********"), (-0.5, "  -0.50000")]
+    for v, ref in KAT_F10_5:
+        assert fio.f_edit(v, 10, 5) == ref, v
+    assert fio.f_edit(0.5, 6, 5) == ".50000" and fio.i_edit(100000, 5) == "*****"
+    rng = np.random.default_rng(12)
+    sp, dp = tmp_path / "stepnm", tmp_path / "fort.20"
+    want_s, want_d = [], []
+    steps = list(rng.integers(0, 99998, 40)) + [99998, 99999, 100000, 123456]
+    for nstep in steps:
+        dt = float(10.0 ** rng.uniform(-6, 0))
+        time = float(rng.uniform(0, 2e5)) if nstep > 50000 else float(rng.uniform(0, 100))
+        restart.write_step_logs(str(sp), str(dp), int(nstep), time, dt)
+        want_s.append(fio.stepnm_line(int(nstep), time, dt))
+        want_d.append(fio.dtlog_line(dt, time + dt, int(nstep) + 1))
+    assert sp.read_text() == "".join(want_s)
+    assert dp.read_text() == "".join(want_d)
+    assert "*****" in dp.read_text() and "**********" in dp.read_text()
+
+
 def test_bad_arguments_rejected(tmp_path):
     lib = capi.load()
     assert lib.dasha_restart_write(None, 0, 0, 0.0, 0, 4, 4, 4, None, 8, 4, 0) == capi.E_INVALID
