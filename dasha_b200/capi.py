@@ -63,6 +63,8 @@ SIGNATURES = {
     "dasha_current_noalloc": ([C.POINTER(GridC), C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "dasha_midplane": ([_P, _D], C.c_int),
     "dasha_checkpoint": ([_P, C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_long], C.c_int),
+    "dasha_stream_out": ([_P, C.c_int, C.c_void_p, C.c_void_p], C.c_int),
+    "dasha_m3d_write_ctx": ([_P, C.c_char_p, C.c_double], C.c_int),
     "dasha_restore": ([_P, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, C.POINTER(C.c_int)], C.c_int),
     "dasha_restart_write": ([C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                              _D, C.c_long, C.c_long, C.c_long], C.c_int),
@@ -78,6 +80,9 @@ SIGNATURES = {
     "dasha_last_error": ([_P], C.c_char_p),
     "dasha_destroy": ([_P], None),
 }
+
+# dasha_chunk_fn: int (*)(void* user, int m, int k0, int k1, const double* rows)
+CHUNK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_double))
 
 _lib = None
 
@@ -195,6 +200,18 @@ class Dasha:
         out = np.zeros((11, self.mz, self.mx))
         self._check(self.lib.dasha_midplane(self.h, _dp(out)))
         return out
+
+    def stream_out(self, what: int, fn):
+        """dasha_stream_out: fn(m, k0, k1, rows) per chunk, rows a (k1-k0, my, mx) view valid
+        during the call; a true return value stops the transfer."""
+        mx, my = self.mx, self.my
+
+        def tramp(user, m, k0, k1, rows):
+            a = np.ctypeslib.as_array(rows, shape=((k1 - k0) * my * mx,)).reshape(k1 - k0, my, mx)
+            return 1 if fn(m, k0, k1, a) else 0
+
+        cb = CHUNK_FN(tramp)
+        self._check(self.lib.dasha_stream_out(self.h, int(what), C.cast(cb, C.c_void_p), None))
 
     def rhs(self, t: float) -> np.ndarray:
         H = harris.to_halo(np.zeros((8, self.mz, self.my, self.mx)))

@@ -3,6 +3,7 @@
 #include "dasha_capi.h"
 #include "mhd_kernels.cuh"
 #include "engine.cuh"
+#include "fortran_format.h"
 #include "fortran_records.h"
 
 #include <cmath>
@@ -320,6 +321,65 @@ int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double
     if (rc == DASHA_OK) c->state_set = true;
     else if (touched) c->state_set = false;   // part of the state may have been replaced
     return rc;
+}
+
+int dasha_stream_out(dasha_ctx* c, int what, dasha_chunk_fn fn, void* user) {
+    CAPI_GUARD(c);
+    if (!fn || (what != 0 && what != 1)) return fail(c, DASHA_E_INVALID, "bad stream arguments");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return engine_call(c, [&] {
+        const ChunkOut take = [&](int m, int k0, int k1, const double* rows) { return fn(user, m, k0, k1, rows) == 0; };
+        return what == 0 ? c->eng->state_out(take) : c->eng->current_out(take);
+    });
+}
+
+// m3d of recrd3 (t3dsdsc.f:5365-5402) from the context: the state's fields stream in order
+// (rho kept on the host for v = (rho v)/rho), then the current's, each list formatted while the
+// next chunk's transfer runs; the text equals dasha_m3d_write of the get_state / current arrays.
+int dasha_m3d_write_ctx(dasha_ctx* c, const char* path, double time) {
+    CAPI_GUARD(c);
+    if (!path) return fail(c, DASHA_E_INVALID, "null path");
+    if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
+    return host_call(c, [&]() -> int {
+        File f(path, "w");
+        if (!f.f) return fail(c, DASHA_E_INVALID, std::string("cannot open ") + path);
+        const int mx = c->mx, my = c->my, mz = c->mz;
+        const int hdr[4] = {3, mx, my, mz};
+        ld_ints(f.f, hdr, 4);
+        ld_real(f.f, time);
+        bool ok = write_list(f.f, (long)mx + my + mz, 11, 10, 4, 0, [&](long n) {
+            return n < mx ? c->ax.c[n] : (n < (long)mx + my ? c->ay.c[n - mx] : c->az.c[n - mx - my]);
+        });
+        if (!ok) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
+        std::vector<double> rho((size_t)c->N);
+        ListWriter lw(f.f, 11, 10, 4, 0);
+        int open_q = -1;
+        auto list = [&](int q, int k0, int k1, const double* rows) {
+            if (q != open_q) {               // a new field: close the last list, number the next
+                if (open_q >= 0) lw.end();
+                const int iq = q + 1;
+                ld_ints(f.f, &iq, 1);
+                open_q = q;
+            }
+            const long cnt = (long)(k1 - k0) * mx * my;
+            const size_t off = (size_t)k0 * mx * my;
+            if (q == 0) std::memcpy(rho.data() + off, rows, sizeof(double) * cnt);
+            if (q >= 1 && q <= 3) lw.put(cnt, [&](long n) { return rows[n] / rho[off + n]; });
+            else lw.put(cnt, [&](long n) { return rows[n]; });
+            return lw.ok;
+        };
+        int rc = from_status(c, c->eng->state_out([&](int m, int k0, int k1, const double* rows) {
+            return list(m, k0, k1, rows);
+        }));
+        if (rc == DASHA_OK)
+            rc = from_status(c, c->eng->current_out([&](int m, int k0, int k1, const double* rows) {
+                return list(8 + m, k0, k1, rows);
+            }));
+        if (rc != DASHA_OK) return rc;
+        ok = lw.end();
+        if (!f.close() || !ok) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
+        return DASHA_OK;
+    });
 }
 
 int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {

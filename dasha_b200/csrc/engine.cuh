@@ -86,6 +86,7 @@ struct EngineBase {
     virtual Status get_state(double* x, long ld1, long ld2) = 0;
     virtual Status state_in(const ChunkIn& fill) = 0;
     virtual Status state_out(const ChunkOut& take) = 0;
+    virtual Status current_out(const ChunkOut& take) = 0;
     virtual Status setdt(double* dt, int* blowup) = 0;
     virtual Status stepon(double time, double dt, int nstep) = 0;
     virtual Status current(double* cur, long ld1, long ld2) = 0;
@@ -897,6 +898,12 @@ public:
         DASHA_CK(cudaMemcpyAsync(outh, mpd, sizeof(double) * 11 * (size_t)mx * mz, cudaMemcpyDeviceToHost, st));
         DASHA_CK(cudaStreamSynchronize(st));
         return Status::ok();
+    }
+
+    Status current_out(const ChunkOut& take) override {
+        launch_current(X);
+        DASHA_CK(cudaGetLastError());
+        return stream_out(curF, 3, false, nullptr, take);
     }
 
     Status rhs(double t, double* xdif, long ld1, long ld2) override {

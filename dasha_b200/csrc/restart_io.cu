@@ -25,6 +25,7 @@
 //    reference opens unit 9 on every call and never closes it, so the lines of a run follow
 //    one another in the file.
 #include "dasha_capi.h"
+#include "fortran_format.h"
 #include "fortran_records.h"
 
 #include <algorithm>
@@ -41,177 +42,17 @@
 namespace {
 
 using dasha::File;
+using dasha::ld_ints;
+using dasha::ld_real;
+using dasha::ListWriter;
+using dasha::fmt_f;
+using dasha::fmt_i;
+using dasha::write_list;
 using dasha::kMaxSubrecord;
 using dasha::pack_restart_header;
 using dasha::unpack_restart_header;
 using dasha::RecReader;
 using dasha::RecWriter;
-
-// Powers of ten 1e-300 .. 1e300 as correctly rounded doubles (strtod), exact up to 1e22.
-struct Pow10 {
-    double p[601];
-    Pow10() {
-        for (int k = -300; k <= 300; ++k) p[k + 300] = std::strtod(("1e" + std::to_string(k)).c_str(), nullptr);
-    }
-};
-const Pow10& pow10_table() {
-    static const Pow10 t;
-    return t;
-}
-
-// The d (<= 6) significant decimal digits of a > 0, correctly rounded, and the exponent e of
-// a ~ 0.d1..dd x 10^e, by scaling in double: m = a * 10^(d-1-e10) lies in [10^(d-1), 10^d)
-// with a relative error below 3e-16 (two roundings), so below 3e-10 in absolute terms, and
-// rounding m to the nearest integer gives the exact result unless m lies within 1e-6 of a
-// tie (xxx.5) or of either end of the interval, where the function declines (returns false)
-// and the caller uses the exact conversion of snprintf.
-bool fast_digits(double a, int d, char* digits, int* e) {
-    if (d < 1 || d > 6 || !(a >= 1e-280 && a <= 1e280)) return false;
-    static const double P[7] = {1, 10, 100, 1000, 10000, 100000, 1000000};
-    int e10 = (int)std::floor(std::log10(a));
-    const int sc = d - 1 - e10;
-    if (sc < -300 || sc > 300) return false;
-    const double m = a * pow10_table().p[sc + 300];
-    const double lo = P[d - 1], hi = P[d];
-    if (!(m >= lo + 1e-6 && m <= hi - 1e-6)) return false;   // exponent near a power of ten
-    const double fl = std::floor(m), fr = m - fl;            // exact: m < 1e6
-    if (std::fabs(fr - 0.5) < 1e-6) return false;            // near a decimal tie
-    long r = (long)fl + (fr > 0.5 ? 1 : 0);
-    if (r >= (long)hi) { r = (long)lo; ++e10; }              // 9..9.7 rounds up to 10..0
-    for (int q = d - 1; q >= 0; --q) { digits[q] = char('0' + r % 10); r /= 10; }
-    *e = e10 + 1;
-    return true;
-}
-
-// Fortran Ew.d (edig = 0) or Ew.dEe output editing of v at scale factor 0, as gfortran writes it:
-// [-][0].d1..dd followed by E+xx (Ew.d, |exponent| <= 99), +xxx (Ew.d, 99 < |exponent| <= 999)
-// or E+ and edig digits; the optional zero before the point is written when the width has
-// room; a field that does not fit is w asterisks.  Writes exactly w characters, no terminator.
-void fmt_e(char* out, double v, int w, int d, int edig) {
-    char body[64];
-    const bool neg = std::signbit(v);
-    if (std::isnan(v) || std::isinf(v)) {
-        const char* s = std::isnan(v) ? "NaN" : (neg ? (w >= 9 ? "-Infinity" : "-Inf") : (w >= 8 ? "Infinity" : "Inf"));
-        const int n = (int)std::strlen(s);
-        if (n > w) { std::memset(out, '*', w); return; }
-        std::memset(out, ' ', w - n);
-        std::memcpy(out + w - n, s, n);
-        return;
-    }
-    char digits[32];
-    int e = 0;
-    if (v == 0.0) {
-        std::memset(digits, '0', d);
-    } else if (!fast_digits(std::fabs(v), d, digits, &e)) {
-        char s[48];
-        std::snprintf(s, sizeof s, "%.*e", d - 1, std::fabs(v));   // d.dd..de+XX: d significant digits
-        digits[0] = s[0];
-        if (d > 1) std::memcpy(digits + 1, s + 2, d - 1);
-        e = std::atoi(std::strchr(s, 'e') + 1) + 1;                 // 0.d1..dd x 10^e
-    }
-    const int ae = e < 0 ? -e : e;
-    // exponent field: E, sign and nd digits (Ew.d with |e| <= 99, Ew.dEe), or sign and 3 digits
-    int nd;
-    bool with_e = true;
-    if (edig == 0) {
-        if (ae <= 99) nd = 2;
-        else if (ae <= 999) { nd = 3; with_e = false; }
-        else { std::memset(out, '*', w); return; }
-    } else {
-        int lim = 1;
-        for (int q = 0; q < edig; ++q) lim *= 10;
-        if (ae >= lim) { std::memset(out, '*', w); return; }
-        nd = edig;
-    }
-    char ex[16];
-    int nex = 0;
-    if (with_e) ex[nex++] = 'E';
-    ex[nex++] = e < 0 ? '-' : '+';
-    for (int q = nd - 1, a = ae; q >= 0; --q, a /= 10) ex[nex + q] = char('0' + a % 10);
-    nex += nd;
-    const int need = (neg ? 1 : 0) + 1 + d + nex;   // without the optional zero
-    if (need > w) { std::memset(out, '*', w); return; }
-    int n = 0;
-    if (neg) body[n++] = '-';
-    if (need + 1 <= w) body[n++] = '0';
-    body[n++] = '.';
-    std::memcpy(body + n, digits, d);
-    n += d;
-    std::memcpy(body + n, ex, nex);
-    n += nex;
-    std::memset(out, ' ', w - n);
-    std::memcpy(out + w - n, body, n);
-}
-
-// Fortran Fw.d output editing of v: correctly rounded to d decimals (snprintf), right-justified;
-// the optional zero before the point is dropped only when the field would not fit otherwise;
-// a field that does not fit is w asterisks.  Writes exactly w characters, no terminator.
-void fmt_f(char* out, double v, int w, int d) {
-    char s[512];
-    int n = std::snprintf(s, sizeof s, "%.*f", d, v);
-    const char* p = s;
-    if (n > w && (std::strncmp(s, "0.", 2) == 0 || std::strncmp(s, "-0.", 3) == 0)) {
-        if (s[0] == '-') { s[1] = '-'; p = s + 1; } else p = s + 1;
-        --n;
-    }
-    if (n > w || n < 0 || !std::isfinite(v)) { std::memset(out, '*', w); return; }
-    std::memset(out, ' ', w - n);
-    std::memcpy(out + w - n, p, n);
-}
-
-// Fortran Iw output editing: right-justified, w asterisks when it does not fit.
-void fmt_i(char* out, long v, int w) {
-    char s[32];
-    const int n = std::snprintf(s, sizeof s, "%ld", v);
-    if (n > w) { std::memset(out, '*', w); return; }
-    std::memset(out, ' ', w - n);
-    std::memcpy(out + w - n, s, n);
-}
-
-// One output list under the format r(1X,Ew.d[Ee]): records of r items; `value(n)` gives item n.
-// Blocks of lines are formatted in parallel and written in order.
-template <class F>
-bool write_list(FILE* f, long count, int per_line, int w, int d, int edig, F value) {
-    const long nlines = (count + per_line - 1) / per_line;
-    const int lw = per_line * (w + 1) + 1;
-    const long block = 1L << 14;   // lines per block
-    const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    std::vector<std::string> buf(nt);
-    for (long l0 = 0; l0 < nlines; l0 += block * nt) {
-        std::vector<std::thread> th;
-        for (unsigned t = 0; t < nt; ++t) {
-            th.emplace_back([&, t]() {
-                std::string& s = buf[t];
-                s.clear();
-                const long a = l0 + (long)t * block, b = std::min(nlines, a + block);
-                if (a >= b) return;
-                s.resize((size_t)(b - a) * lw);
-                char* p = &s[0];
-                for (long l = a; l < b; ++l) {
-                    const long n0 = l * per_line, n1 = std::min(count, n0 + per_line);
-                    for (long n = n0; n < n1; ++n) {
-                        *p++ = ' ';
-                        fmt_e(p, value(n), w, d, edig);
-                        p += w;
-                    }
-                    *p++ = '\n';
-                }
-                s.resize((size_t)(p - &s[0]));
-            });
-        }
-        for (auto& x : th) x.join();
-        for (unsigned t = 0; t < nt; ++t)
-            if (!buf[t].empty() && std::fwrite(buf[t].data(), 1, buf[t].size(), f) != buf[t].size()) return false;
-    }
-    return true;
-}
-
-// list-directed lines: integers in 12 columns, a REAL*8 as " " + 17 significant digits
-void ld_ints(FILE* f, const int* v, int n) {
-    for (int q = 0; q < n; ++q) std::fprintf(f, " %11d", v[q]);
-    std::fputc('\n', f);
-}
-void ld_real(FILE* f, double v) { std::fprintf(f, " %24.16E\n", v); }
 
 inline long hidx(long ld1, long ld2, int mz, int i, int j, int k, int m) {
     return (long)(i + 2) + ld1 * ((long)j + ld2 * ((long)(k + 2) + (long)(mz + 4) * m));
@@ -332,14 +173,14 @@ int dasha_m3d_write(const char* path, int mx, int my, int mz, double time, const
         bool ok = write_list(f.f, (long)mx + my + mz, 11, 10, 4, 0, [&](long n) {
             return n < mx ? xc[n] : (n < (long)mx + my ? yc[n - mx] : zc[n - mx - my]);
         });
-        const long mxy = (long)mx * my, nv = mxy * mz;
+        const long mxy = (long)mx * my;
         for (int q = 0; q < 11 && ok; ++q) {
             const int iq = q + 1;
             ld_ints(f.f, &iq, 1);
-            ok = write_list(f.f, nv, 11, 10, 4, 0, [&](long n) {
-                const int i = (int)(n % mx), j = (int)((n / mx) % my), k = (int)(n / mxy);
-                return out_field(x_f, cur_f, ld1, ld2, mz, q, i, j, k);
-            });
+            ListWriter lw(f.f, 11, 10, 4, 0);   // one plane per put: records run across planes
+            for (int k = 0; k < mz && lw.ok; ++k)
+                lw.put(mxy, [&](long n) { return out_field(x_f, cur_f, ld1, ld2, mz, q, (int)(n % mx), (int)(n / mx), k); });
+            ok = lw.end();
         }
         return f.close() && ok ? DASHA_OK : DASHA_E_INVALID;
     });

@@ -6,7 +6,8 @@
   (t3dsdsc.f:4814-4861), record 1 (ncase, nstep, time, nst), record 2 the array
   x(mx+4, my, mz+4, 8).
 * `write_m2d` / `write_m3d`: the ASCII files data/m2dNNN.dat and data/m3dNNN of recrd2 / recrd3
-  (t3dsdsc.f:4965-5412); `Dasha.midplane()` gives the eleven mid-plane fields from the GPU.
+  (t3dsdsc.f:4965-5412); `Dasha.midplane()` gives the eleven mid-plane fields from the GPU and
+  `write_m3d_ctx` streams the 3-D file from a context.
 * `write_current_dat`: the line diagn appends to current.dat (t3dsdsc.f:1226-1232).
 * `write_step_logs`: the main loop's stepnm and unit-20 lines (t3dsdsc.f:157-181).
 
@@ -111,6 +112,11 @@ def write_m3d(path: str, time: float, x: np.ndarray, y: np.ndarray, z: np.ndarra
     assert Hcur.shape[1:] == H.shape[1:] and (x.size, y.size, z.size) == (ld1 - 4, ld2, mz4 - 4)
     _check(lib.dasha_m3d_write(os.fsencode(path), x.size, y.size, z.size, float(time), capi._dp(x), capi._dp(y),
                                capi._dp(z), capi._dp(H), capi._dp(Hcur), ld1, ld2), f"m3d write {path}")
+
+
+def write_m3d_ctx(d: "capi.Dasha", path: str, time: float):
+    """recrd3's data/m3dNNN from a GPU context, streamed (no host copy of the volume)."""
+    d._check(d.lib.dasha_m3d_write_ctx(d.h, os.fsencode(path), float(time)))
 
 
 def write_current_dat(path: str, diag: np.ndarray, time: float, append: bool = True):

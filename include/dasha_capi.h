@@ -108,6 +108,22 @@ int dasha_checkpoint(dasha_ctx* ctx, const char* path, int ncase, int nstep, dou
                      long max_subrecord);
 int dasha_restore(dasha_ctx* ctx, const char* path, int* ncase, int* nstep, double* time, int* nst);
 
+/* Chunked download, for callers that write their own files without a host copy of the
+ * volume: what = 0 streams the state (the 8 fields of dasha_get_state), what = 1 the smoothed
+ * current (the 3 fields of dasha_current).  fn(user, m, k0, k1, rows) is called once per chunk,
+ * fields in order and z planes in order within a field, rows holding field m on planes
+ * k0..k1-1 as (k1-k0)*my rows of mx FP64 values (x fastest, no halo), valid during the call
+ * only; the next chunk's transfer runs meanwhile.  A non-zero return stops the transfer
+ * (DASHA_E_INVALID).  No counterpart in the reference. */
+typedef int (*dasha_chunk_fn)(void* user, int m, int k0, int k1, const double* rows);
+int dasha_stream_out(dasha_ctx* ctx, int what, dasha_chunk_fn fn, void* user);
+
+/* The m3d file of recrd3 (the format of dasha_m3d_write below) written from the context through
+ * dasha_stream_out: no host copy of the state or the current, only of rho (mx*my*mz values) for
+ * v = (rho v)/rho; the coordinates are the grid's.  The text equals dasha_m3d_write of the
+ * dasha_get_state and dasha_current arrays. */
+int dasha_m3d_write_ctx(dasha_ctx* ctx, const char* path, double time);
+
 /* CFL time step of the current state (setdt, t3dsdsc.f:4694-4763): synchronises, returns dt.
  * Also reports a latched blow-up (DASHA_E_BLOWUP) and dt collapse (DASHA_E_DT_COLLAPSE,
  * dt < 0.1*dt0 with dt0 the first dt of the context, t3dsdsc.f:142). */

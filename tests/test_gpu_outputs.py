@@ -115,3 +115,49 @@ def test_restore_rejects_a_mismatched_file_and_keeps_the_state(tmp_path):
     a.setdt(0.0)                                               # the context still steps
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("cfg", [SMALL, CHUNKS], ids=lambda c: c.name)
+def test_stream_out_equals_get_state_and_current(cfg):
+    """dasha_stream_out delivers every plane of every field once, fields and planes in order,
+    with the values of dasha_get_state / dasha_current (two chunks per field on CHUNKS)."""
+    d = capi.gem_context(cfg, 1)
+    d.run(1)
+    for what, nf, ref in ((0, 8, d.get_state()), (1, 3, d.current())):
+        got = np.full((nf, cfg.mz, cfg.my, cfg.mx), np.nan)
+        order = []
+
+        def take(m, k0, k1, rows):
+            order.append((m, k0, k1))
+            got[m, k0:k1] = rows
+            return False
+
+        d.stream_out(what, take)
+        assert np.array_equal(got, ref)
+        assert [o[0] for o in order] == sorted(o[0] for o in order)
+        for m in range(nf):
+            ks = [(k0, k1) for mm, k0, k1 in order if mm == m]
+            assert ks[0][0] == 0 and ks[-1][1] == cfg.mz and all(a[1] == b[0] for a, b in zip(ks, ks[1:]))
+    d.close()
+
+
+def test_stream_out_stops_when_asked():
+    d = capi.gem_context(CHUNKS, 0)
+    seen = []
+    with pytest.raises(capi.DashaError) as e:
+        d.stream_out(0, lambda m, k0, k1, rows: seen.append(m) or True)
+    assert e.value.code == capi.E_INVALID and seen == [0]
+    assert np.isfinite(d.get_state()).all()                     # the context is still usable
+    d.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("cfg", [SMALL, RAGGED], ids=lambda c: c.name)
+def test_m3d_from_context_equals_host_path(tmp_path, cfg, precision):
+    d = capi.gem_context(cfg, precision)
+    t, _ = d.run(1)
+    a, b = tmp_path / "m3d_ctx", tmp_path / "m3d_host"
+    restart.write_m3d_ctx(d, str(a), t)
+    restart.write_m3d(str(b), t, d.x, d.y, d.z, harris.to_halo(d.get_state()), harris.to_halo(d.current()))
+    assert a.read_text() == b.read_text()
+    d.close()

@@ -273,6 +273,8 @@ def test_bad_arguments_rejected(tmp_path):
     assert lib.dasha_m2d_write(str(tmp_path / "m").encode(), 0, 4, 0.0, None, None, None) == capi.E_INVALID
     assert lib.dasha_midplane(None, None) == capi.E_INVALID
     assert lib.dasha_checkpoint(None, b"x", 0, 0, 0.0, 0, 0) == capi.E_INVALID
+    assert lib.dasha_stream_out(None, 0, None, None) == capi.E_INVALID
+    assert lib.dasha_m3d_write_ctx(None, b"x", 0.0) == capi.E_INVALID
     i, t = ctypes.c_int(), ctypes.c_double()
     assert lib.dasha_restore(None, b"x", ctypes.byref(i), ctypes.byref(i), ctypes.byref(t), ctypes.byref(i)) == capi.E_INVALID
     assert lib.dasha_restart_write(str(tmp_path / "no" / "dir").encode(), 0, 0, 0.0, 0, 4, 4, 4, capi._dp(H), 8, 4, 0) == capi.E_INVALID
