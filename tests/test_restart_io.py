@@ -168,6 +168,17 @@ def test_m3d_matches_oracle(tmp_path):
     assert p.read_text() == fio.m3d_text(3.5, x, y, z, X, cur)
 
 
+@pytest.mark.parametrize("mx,my,mz", [(1, 1, 12), (11, 1, 3), (3, 1, 5), (2, 2, 9), (13, 7, 2)])
+def test_m3d_records_run_across_planes(tmp_path, mx, my, mz):
+    """The 3-D writer formats one z plane per piece; records of 11 numbers continue across
+    planes of 1, 11, 3, 4 and 91 nodes exactly as in one list."""
+    X, cur = _state(mx, my, mz, seed=mx * my + mz)
+    x, y, z = np.arange(mx) * 0.5, np.arange(my) - 1.0, np.linspace(-1, 1, mz)
+    p = tmp_path / "m3d"
+    restart.write_m3d(str(p), 2.0, x, y, z, harris.to_halo(X), harris.to_halo(cur))
+    assert p.read_text() == fio.m3d_text(2.0, x, y, z, X, cur)
+
+
 def test_large_list_parallel_formatting(tmp_path):
     """Lists longer than one formatting block of the library (2^14 lines per thread)."""
     mx, mz = 512, 200
