@@ -71,6 +71,11 @@ SIGNATURES = {
     "dasha_restart_read": ([C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), _D, C.POINTER(C.c_int),
                             C.c_int, C.c_int, C.c_int, _D, C.c_long, C.c_long], C.c_int),
     "dasha_m2d_write": ([C.c_char_p, C.c_int, C.c_int, C.c_double, _D, _D, _D], C.c_int),
+    "dasha_restart_read_ranks": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                  _D, C.POINTER(C.c_int), C.c_int, C.c_int, C.c_int, _D, C.c_long, C.c_long],
+                                 C.c_int),
+    "dasha_restart_write_ranks": ([C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_int, C.c_int, _D, C.c_long, C.c_long, C.c_long], C.c_int),
     "dasha_midplane_host": ([C.c_int, C.c_int, C.c_int, _D, _D, C.c_long, C.c_long, _D], C.c_int),
     "dasha_current_dat_write": ([C.c_char_p, _D, C.c_double, C.c_int], C.c_int),
     "dasha_stepnm_write": ([C.c_char_p, C.c_int, C.c_double, C.c_double], C.c_int),

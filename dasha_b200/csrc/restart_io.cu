@@ -140,6 +140,103 @@ int dasha_restart_read(const char* path, int* ncase, int* nstep, double* time, i
     });
 }
 
+// The restart files of an nprx x nprz MPI run of the reference (t3dsdsc.f:36-67, 4814-4861):
+// rank r (mepx = r mod nprx, mepz = r / nprx) holds x(mxpr, my, mzpr, 8) with mxpr = mx/nprx + 4
+// and mzpr = mz/nprz + 4; its interior columns jx = 3 .. mxpr-2 (1-based; the last rank in x
+// also mxpr-1 when mod(mx, nprx) = 1) are the global columns mepx*(mxpr-4) + jx - 2, and the
+// same in z.  The reference allows mod(mx, nprx) <= 1 and mod(mz, nprz) <= 1 only (T:44-47).
+struct RankGrid {
+    int mx, my, mz, nprx, nprz, mxpr, mzpr;
+    bool ok() const {
+        return nprx > 0 && nprz > 0 && nprx * nprz <= 1000 && mx % nprx <= 1 && mz % nprz <= 1 && mx / nprx >= 1 &&
+               mz / nprz >= 1;
+    }
+    // local 0-based column range [lo, hi] of rank coordinate p holding global nodes
+    void interior(int p, int npr, int mpr, int m, int* lo, int* hi) const {
+        *lo = 2;
+        *hi = mpr - 3 + (p == npr - 1 ? m % npr : 0);
+    }
+    std::string path(const char* dir, int nst, int rank) const {
+        char name[16];
+        std::snprintf(name, sizeof name, "mhd%03d%03d", nst, rank);
+        return std::string(dir) + "/" + name;
+    }
+};
+
+int dasha_restart_read_ranks(const char* dir, int nst_file, int nprx, int nprz, int* ncase, int* nstep, double* time,
+                             int* nst, int mx, int my, int mz, double* x_f, long ld1, long ld2) {
+    if (!dir || !ncase || !nstep || !time || !nst || !x_f || !dims_ok(mx, my, mz, ld1, ld2)) return DASHA_E_INVALID;
+    RankGrid G{mx, my, mz, nprx, nprz, mx / std::max(nprx, 1) + 4, mz / std::max(nprz, 1) + 4};
+    if (!G.ok() || nst_file < 0 || nst_file > 999) return DASHA_E_INVALID;
+    return guarded([&]() -> int {
+        const long nloc = (long)G.mxpr * my * G.mzpr * 8;
+        std::vector<double> loc((size_t)nloc);
+        unsigned char hdr0[20] = {0};
+        for (int r = 0; r < nprx * nprz; ++r) {
+            File f(G.path(dir, nst_file, r).c_str(), "rb");
+            if (!f.f) return DASHA_E_INVALID;
+            unsigned char hdr[20];
+            RecReader r1(f.f, 20);
+            r1.get(hdr, 20);
+            RecReader r2(f.f, (long)sizeof(double) * nloc);
+            if (r1.finish()) r2.get(loc.data(), (long)sizeof(double) * nloc);
+            if (!r1.finish() || !r2.finish()) return DASHA_E_INVALID;
+            if (r == 0) std::memcpy(hdr0, hdr, 20);
+            else if (std::memcmp(hdr0, hdr, 20) != 0) return DASHA_E_INVALID;   // ranks of different runs
+            const int px = r % nprx, pz = r / nprx;
+            int xlo, xhi, zlo, zhi;
+            G.interior(px, nprx, G.mxpr, mx, &xlo, &xhi);
+            G.interior(pz, nprz, G.mzpr, mz, &zlo, &zhi);
+            for (int m = 0; m < 8; ++m)
+                for (int lz = zlo; lz <= zhi; ++lz)
+                    for (int j = 0; j < my; ++j) {
+                        const int gk = pz * (G.mzpr - 4) + lz - 2, gi0 = px * (G.mxpr - 4) + xlo - 2;
+                        const double* src = loc.data() + xlo + (long)G.mxpr * (j + (long)my * (lz + (long)G.mzpr * m));
+                        std::memcpy(x_f + hidx(ld1, ld2, mz, gi0, j, gk, m), src, sizeof(double) * (xhi - xlo + 1));
+                    }
+        }
+        unpack_restart_header(hdr0, ncase, nstep, time, nst);
+        return DASHA_OK;
+    });
+}
+
+int dasha_restart_write_ranks(const char* dir, int ncase, int nstep, double time, int nst, int nprx, int nprz, int mx,
+                              int my, int mz, const double* x_f, long ld1, long ld2, long max_subrecord) {
+    if (!dir || !x_f || !dims_ok(mx, my, mz, ld1, ld2) || max_subrecord < 0) return DASHA_E_INVALID;
+    RankGrid G{mx, my, mz, nprx, nprz, mx / std::max(nprx, 1) + 4, mz / std::max(nprz, 1) + 4};
+    if (!G.ok() || nst < 0 || nst > 999) return DASHA_E_INVALID;
+    return guarded([&]() -> int {
+        const long maxsub = max_subrecord == 0 ? kMaxSubrecord : std::min(max_subrecord, kMaxSubrecord);
+        const long nloc = (long)G.mxpr * my * G.mzpr * 8;
+        std::vector<double> loc((size_t)nloc);
+        unsigned char hdr[20];
+        pack_restart_header(hdr, ncase, nstep, time, nst);
+        for (int r = 0; r < nprx * nprz; ++r) {
+            const int px = r % nprx, pz = r / nprx;
+            // every local entry from the global node it stands for: x wraps (periodic), z
+            // beyond the walls is zero
+            for (int m = 0; m < 8; ++m)
+                for (int lz = 0; lz < G.mzpr; ++lz)
+                    for (int j = 0; j < my; ++j)
+                        for (int lx = 0; lx < G.mxpr; ++lx) {
+                            const int gk = pz * (G.mzpr - 4) + lz - 2;
+                            int gi = px * (G.mxpr - 4) + lx - 2;
+                            gi = ((gi % mx) + mx) % mx;
+                            loc[lx + (size_t)G.mxpr * (j + (size_t)my * (lz + (size_t)G.mzpr * m))] =
+                                (gk >= 0 && gk < mz) ? x_f[hidx(ld1, ld2, mz, gi, j, gk, m)] : 0.0;
+                        }
+            File f(G.path(dir, nst, r).c_str(), "wb");
+            if (!f.f) return DASHA_E_INVALID;
+            RecWriter w1(f.f, 20, maxsub);
+            w1.put(hdr, 20);
+            RecWriter w2(f.f, (long)sizeof(double) * nloc, maxsub);
+            if (w1.finish()) w2.put(loc.data(), (long)sizeof(double) * nloc);
+            if (!w1.finish() || !w2.finish() || !f.close()) return DASHA_E_INVALID;
+        }
+        return DASHA_OK;
+    });
+}
+
 int dasha_m2d_write(const char* path, int mx, int mz, double time, const double* xc, const double* zc,
                     const double* plane) {
     if (!path || mx <= 0 || mz <= 0 || !xc || !zc || !plane) return DASHA_E_INVALID;

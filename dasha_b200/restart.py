@@ -76,6 +76,30 @@ def read_restart(path: str, mx: int, my: int, mz: int):
     return a.value, b.value, t.value, d.value, H
 
 
+def read_restart_ranks(directory: str, nst: int, nprx: int, nprz: int, mx: int, my: int, mz: int):
+    """readin of an nprx x nprz MPI run: the rank files mhdNNN000 .. assembled into one global
+    state; returns (ncase, nstep, time, nst, H) with H (8, mz+4, my, mx+4) (interior filled)."""
+    lib = capi.load()
+    H = np.zeros((8, mz + 4, my, mx + 4))
+    a, b, d = C.c_int(), C.c_int(), C.c_int()
+    t = C.c_double()
+    _check(lib.dasha_restart_read_ranks(os.fsencode(directory), nst, nprx, nprz, C.byref(a), C.byref(b), C.byref(t),
+                                        C.byref(d), mx, my, mz, capi._dp(H), mx + 4, my), f"rank restart read {directory}")
+    return a.value, b.value, t.value, d.value, H
+
+
+def write_restart_ranks(directory: str, ncase: int, nstep: int, time: float, nst: int, nprx: int, nprz: int,
+                        H: np.ndarray, max_subrecord: int = 0):
+    """recrd of an nprx x nprz MPI run: the global state H (8, mz+4, my, mx+4) split into the
+    rank files mhdNNNRRR of `directory`."""
+    lib = capi.load()
+    H = np.ascontiguousarray(H, np.float64)
+    _, mz4, ld2, ld1 = H.shape
+    _check(lib.dasha_restart_write_ranks(os.fsencode(directory), ncase, nstep, float(time), nst, nprx, nprz, ld1 - 4,
+                                         ld2, mz4 - 4, capi._dp(H), ld1, ld2, int(max_subrecord)),
+           f"rank restart write {directory}")
+
+
 def midplane_host(H: np.ndarray, Hcur: np.ndarray) -> np.ndarray:
     """The eleven output fields on the plane j = my/2 from a state and a current array in the
     halo layout; (11, mz, mx)."""

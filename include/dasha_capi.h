@@ -218,6 +218,21 @@ int dasha_restart_write(const char* path, int ncase, int nstep, double time, int
 int dasha_restart_read(const char* path, int* ncase, int* nstep, double* time, int* nst, int mx, int my, int mz,
                        double* x_f, long ld1, long ld2);
 
+/* The restart files of an nprx x nprz MPI run of the reference, one per rank:
+ * <dir>/mhdNNNRRR, RRR = rank (t3dsdsc.f:36-67, 4814-4861), each the rank's x(mxpr, my, mzpr, 8)
+ * with mxpr = mx/nprx + 4, mzpr = mz/nprz + 4 (mhd01.for:5-6), rank r at process coordinates
+ * (r mod nprx, r / nprx), the last rank of each direction holding the one extra node when
+ * mx mod nprx (mz mod nprz) is 1; the reference allows no larger remainder.
+ * dasha_restart_read_ranks assembles the global state (interior nodes of every rank) into the
+ * dasha_set_state layout, checking that all ranks carry the same record 1;
+ * dasha_restart_write_ranks splits a global state into the rank files, each local entry taken
+ * from the global node it stands for (x periodic, zeros beyond the z walls), which readin
+ * then refreshes between ranks (message4).  Records as in dasha_restart_write. */
+int dasha_restart_read_ranks(const char* dir, int nst_file, int nprx, int nprz, int* ncase, int* nstep, double* time,
+                             int* nst, int mx, int my, int mz, double* x_f, long ld1, long ld2);
+int dasha_restart_write_ranks(const char* dir, int ncase, int nstep, double time, int nst, int nprx, int nprz, int mx,
+                              int my, int mz, const double* x_f, long ld1, long ld2, long max_subrecord);
+
 /* ASCII mid-plane file m2dNNN.dat of recrd2 (t3dsdsc.f:5116-5154): list-directed lines
  * "2 mx mz" and time, the coordinates x[mx] then z[mz] as one list, then for q = 1..11 a line
  * "q" and plane field q-1 (the layout dasha_midplane returns), all lists in the format

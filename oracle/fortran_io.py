@@ -10,6 +10,8 @@ unformatted records and for E editing, and gfortran's published record layout.
 * m2d / m3d (recrd2 t3dsdsc.f:5116-5154, recrd3 t3dsdsc.f:5365-5402): list-directed header
   lines (written here as the library writes them: integers in 12 columns, the time with 17
   significant digits), then lists under 5(1X,E14.5E3) or 11(1X,E10.4).
+* rank files of an nprx x nprz run (t3dsdsc.f:36-67): the local arrays and the gather rule
+  of recrd2 (t3dsdsc.f:5034-5068).
 * current.dat (diagn, t3dsdsc.f:1226-1232): 7(1X,E13.4) per line.
 * the main loop's step logs (t3dsdsc.f:157-181): stepnm (list-directed) and unit 20,
   2(1X,F10.5),1X,I5.
@@ -63,6 +65,37 @@ def restart_bytes(ncase: int, nstep: int, time: float, nst: int, x_fortran: np.n
     """x_fortran: C-order (8, mz+4, my, mx+4) == Fortran x(mx+4, my, mz+4, 8)."""
     hdr = struct.pack("<iidi", ncase, nstep, time, nst)
     return write_record(hdr, maxsub) + write_record(np.ascontiguousarray(x_fortran, "<f8").tobytes(), maxsub)
+
+
+def rank_layout(mx: int, mz: int, nprx: int, nprz: int):
+    """mxpr, mzpr of the reference's decomposition (mhd01.for:5-6)."""
+    return mx // nprx + 4, mz // nprz + 4
+
+
+def rank_local(X: np.ndarray, rank: int, nprx: int, nprz: int) -> np.ndarray:
+    """The local array x(mxpr, my, mzpr, 8) of `rank` as C-order (8, mzpr, my, mxpr) from the
+    compact global state (8, mz, my, mx): local node (lx, lz) (0-based) stands for global
+    column mepx*(mxpr-4) + lx - 2 and row mepz*(mzpr-4) + lz - 2, the gather rule of recrd2
+    (t3dsdsc.f:5034-5068) run backwards; x wraps, z beyond the walls is zero."""
+    _, mz, my, mx = X.shape
+    mxpr, mzpr = rank_layout(mx, mz, nprx, nprz)
+    px, pz = rank % nprx, rank // nprx
+    gi = (px * (mxpr - 4) + np.arange(mxpr) - 2) % mx
+    gk = pz * (mzpr - 4) + np.arange(mzpr) - 2
+    inside = (gk >= 0) & (gk < mz)
+    L = np.zeros((8, mzpr, my, mxpr))
+    L[:, inside] = X[:, gk[inside]][:, :, :, gi]
+    return L
+
+
+def rank_interior(rank: int, mx: int, mz: int, nprx: int, nprz: int):
+    """(local x slice, global x slice, local z slice, global z slice) that rank owns."""
+    mxpr, mzpr = rank_layout(mx, mz, nprx, nprz)
+    px, pz = rank % nprx, rank // nprx
+    xn = mxpr - 4 + (mx % nprx if px == nprx - 1 else 0)
+    zn = mzpr - 4 + (mz % nprz if pz == nprz - 1 else 0)
+    return (slice(2, 2 + xn), slice(px * (mxpr - 4), px * (mxpr - 4) + xn),
+            slice(2, 2 + zn), slice(pz * (mzpr - 4), pz * (mzpr - 4) + zn))
 
 
 def e_edit(v: float, w: int, d: int, e: int | None = None) -> str:

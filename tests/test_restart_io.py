@@ -127,6 +127,48 @@ def test_restart_reader_accepts_any_split_and_rejects_mismatches(tmp_path):
         restart.read_restart(str(tmp_path / "missing"), mx, my, mz)
 
 
+@pytest.mark.parametrize("mx,my,mz,nprx,nprz", [(10, 4, 9, 3, 2), (9, 3, 8, 3, 2), (13, 2, 7, 4, 3), (8, 3, 6, 1, 1)])
+def test_rank_files_match_oracle(tmp_path, mx, my, mz, nprx, nprz):
+    """A global state split into the rank files of an nprx x nprz run byte for byte as the
+    oracle forms them, and the files assembled back into the same interior; the last rank of a
+    direction holds the extra node when mx mod nprx (mz mod nprz) is 1."""
+    X, _ = _state(mx, my, mz, seed=mx + 10 * mz)
+    H = harris.to_halo(X)                                     # NaN halo: it must not be read
+    restart.write_restart_ranks(str(tmp_path), 1, 30, 2.5, 4, nprx, nprz, H, max_subrecord=1000)
+    for r in range(nprx * nprz):
+        ref = fio.restart_bytes(1, 30, 2.5, 4, fio.rank_local(X, r, nprx, nprz), 1000)
+        assert (tmp_path / restart.restart_name(4, r)).read_bytes() == ref, r
+    ncase, nstep, t, nst, G = restart.read_restart_ranks(str(tmp_path), 4, nprx, nprz, mx, my, mz)
+    assert (ncase, nstep, t, nst) == (1, 30, 2.5, 4)
+    assert np.array_equal(harris.from_halo(G, mx, my, mz), X)
+    # the oracle's gather rule covers every global node exactly once
+    hits = np.zeros((mz, mx), int)
+    for r in range(nprx * nprz):
+        _, gx, _, gz = fio.rank_interior(r, mx, mz, nprx, nprz)
+        hits[gz, gx] += 1
+    assert (hits == 1).all()
+
+
+def test_rank_files_read_from_oracle_and_rejected(tmp_path):
+    mx, my, mz, nprx, nprz = 10, 3, 9, 3, 2
+    X, _ = _state(mx, my, mz, seed=3)
+    for r in range(nprx * nprz):                              # files made by the oracle alone
+        L = fio.rank_local(X, r, nprx, nprz)
+        lx, gx, lz, gz = fio.rank_interior(r, mx, mz, nprx, nprz)
+        assert np.array_equal(L[:, lz, :, lx], X[:, gz, :, gx])
+        (tmp_path / restart.restart_name(2, r)).write_bytes(fio.restart_bytes(5, 6, 7.0, 2, L, 97))
+    G = restart.read_restart_ranks(str(tmp_path), 2, nprx, nprz, mx, my, mz)[4]
+    assert np.array_equal(harris.from_halo(G, mx, my, mz), X)
+    with pytest.raises(capi.DashaError):
+        restart.read_restart_ranks(str(tmp_path), 2, 3, 3, mx, my, mz)     # other process grid: records differ
+    with pytest.raises(capi.DashaError):
+        restart.read_restart_ranks(str(tmp_path), 2, 4, 2, mx, my, mz)     # mod(10, 4) = 2
+    p = tmp_path / restart.restart_name(2, 4)
+    p.write_bytes(fio.restart_bytes(5, 6, 7.5, 2, fio.rank_local(X, 4, nprx, nprz)))
+    with pytest.raises(capi.DashaError):
+        restart.read_restart_ranks(str(tmp_path), 2, nprx, nprz, mx, my, mz)   # another time in one rank
+
+
 def test_restart_names():
     assert restart.restart_name(7) == "mhd007000"
     assert restart.restart_name(123, 45) == "mhd123045"
