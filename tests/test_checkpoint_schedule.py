@@ -96,10 +96,10 @@ def test_schedule_is_valid_and_optimal(driver, n, s):
 
 
 def test_large_cases_closed_form(driver):
-    """500 steps: with 4 states on the device (slot 0 and 3 more; a 1024x512x1024 FP64 state
-    is 34 GB) the schedule takes 3213 forward steps, 6.4 runs, where two-level checkpointing
-    needs about 45 states; with 11 states 1545; with every state kept (499 more slots) one
-    sweep, 499 steps; with 46 states, the memory of two-level checkpointing, 952."""
+    """500 steps: with 11 states (slot 0 and 10 more, what fits beside the adjoint's scratch on
+    a 512x256x512 FP64 grid) the schedule takes 1545 forward steps, 3.1 runs, where two-level
+    checkpointing needs about 45 states; with 4 states 3213; with every state kept (499 more
+    slots) one sweep, 499 steps; with 46 states, the memory of two-level checkpointing, 952."""
     assert cost(driver, 500, 3) == 3213
     assert cost(driver, 500, 10) == 1545
     assert cost(driver, 500, 499) == 499
