@@ -41,9 +41,10 @@ def write_record(data: bytes, maxsub: int = GFORTRAN_MAX_SUBRECORD) -> bytes:
     return b"".join(parts)
 
 
-def read_records(buf: bytes) -> list[bytes]:
+def read_records(buf: bytes, count: int | None = None) -> list[bytes]:
+    """The records of `buf` (the first `count` of them, as a READ of that many does)."""
     out, pos = [], 0
-    while pos < len(buf):
+    while pos < len(buf) and (count is None or len(out) < count):
         rec, first = [], True
         while True:
             (head,) = struct.unpack_from("<i", buf, pos)

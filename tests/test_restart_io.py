@@ -169,6 +169,44 @@ def test_rank_files_read_from_oracle_and_rejected(tmp_path):
         restart.read_restart_ranks(str(tmp_path), 2, nprx, nprz, mx, my, mz)   # another time in one rank
 
 
+def test_restart_reader_survives_corrupt_files(tmp_path):
+    """Random damage to a restart file (bytes flipped in the markers or the data, the file cut
+    or extended, markers replaced by extreme lengths): the reader returns the data only when
+    the records still hold exactly the grid's bytes, else a status; it never reads past them."""
+    mx, my, mz = 6, 3, 5
+    X, _ = _state(mx, my, mz, seed=31)
+    H = restart.restart_array(X)
+    good = fio.restart_bytes(1, 2, 3.0, 4, H, 64)
+    rng = np.random.default_rng(99)
+    p = tmp_path / "f"
+    outcomes = {"ok": 0, "error": 0}
+    for trial in range(300):
+        b = bytearray(good)
+        kind = trial % 4
+        if kind == 0:                                     # flip a few bytes anywhere
+            for q in rng.integers(0, len(b), rng.integers(1, 4)):
+                b[q] ^= int(rng.integers(1, 256))
+        elif kind == 1:                                   # cut
+            b = b[:int(rng.integers(0, len(b)))]
+        elif kind == 2:                                   # extend
+            b += bytes(rng.integers(0, 256, int(rng.integers(1, 40))).astype(np.uint8))
+        else:                                             # an extreme marker at a marker position
+            pos = [0, 4 + 20, 4 + 20 + 4][int(rng.integers(0, 3))]
+            b[pos:pos + 4] = int(rng.choice([-2**31, 2**31 - 1, -1, 0, 1 << 30])).to_bytes(4, "little", signed=True)
+        p.write_bytes(bytes(b))
+        try:
+            got = restart.read_restart(str(p), mx, my, mz)
+        except capi.DashaError:
+            outcomes["error"] += 1
+            continue
+        outcomes["ok"] += 1
+        # accepted only if the records are intact; a flipped data byte changes the values
+        recs = fio.read_records(bytes(b), count=2)       # bytes after record 2 are not read
+        assert len(recs) >= 2 and len(recs[1]) == H.nbytes
+        assert np.ascontiguousarray(got[4]).tobytes() == recs[1]   # bit for bit (a flip may make a NaN)
+    assert outcomes["error"] > 100 and outcomes["ok"] > 0
+
+
 def test_restart_names():
     assert restart.restart_name(7) == "mhd007000"
     assert restart.restart_name(123, 45) == "mhd123045"
