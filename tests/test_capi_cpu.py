@@ -51,6 +51,41 @@ def test_product_never_uses_the_oracle():
         assert not hasattr(lib, sym), sym
 
 
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/dasha_capi.h as a C99 caller sees it (the Fortran ISO_C_BINDING module binds the
+    same symbols): compiled with -Wall -Werror -pedantic, every declared function taken by
+    address, linked against the built library, and run through the host-only file calls."""
+    names = declared_functions()
+    src = tmp_path / "caller.c"
+    body = "\n".join(f"    p[{i}] = (void (*)(void)){n};" for i, n in enumerate(names))
+    src.write_text(f"""#include "dasha_capi.h"
+#include <stdio.h>
+#include <string.h>
+int main(void) {{
+    void (*p[{len(names)}])(void);
+{body}
+    double x[16 * 4 * 8 * 8];
+    int ncase = 0, nstep = 0, nst = 0;
+    double t = 0.0;
+    for (int q = 0; q < 16 * 4 * 8 * 8; ++q) x[q] = 0.25 * q;
+    if (dasha_restart_write("{tmp_path}/mhd001000", 3, 40, 1.5, 1, 12, 4, 4, x, 16, 4, 0) != DASHA_OK) return 1;
+    memset(x, 0, sizeof x);
+    if (dasha_restart_read("{tmp_path}/mhd001000", &ncase, &nstep, &t, &nst, 12, 4, 4, x, 16, 4) != DASHA_OK) return 2;
+    if (ncase != 3 || nstep != 40 || t != 1.5 || nst != 1 || x[100] != 25.0) return 3;
+    if (dasha_setdt(NULL, 0.0, &t) != DASHA_E_INVALID) return 4;
+    printf("%d\\n", (int)(sizeof p / sizeof p[0]));
+    return 0;
+}}
+""")
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(capi.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", str(exe), "-L" + libdir, "-ldasha", "-Wl,-rpath," + libdir], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert out.returncode == 0, out
+    assert int(out.stdout) == len(names)
+
+
 def test_missing_library_fails_loudly(tmp_path):
     saved = capi._lib
     capi._lib = None
