@@ -12,7 +12,9 @@ to them are the reference's boundary treatment, not the equations).
     for B (E is smoothed 4 times: c h^2 del^2 E).
   * "full": B = B0 + curl A, eta = 0.01, di = 0.5.  J and the Hall field are smoothed too, so
     every field converges at least at 2nd order.
-Both on a uniform and on the sinh-stretched z grid."""
+Both on a uniform and on the sinh-stretched z grid.  And in time: the step (stepon,
+t3dsdsc.f:1063-1185, classical RK4) converges at 4th order in dt over a fixed time, the
+post-step filter off (it acts once per step, so it is not a discretization of the ODE)."""
 import numpy as np
 import pytest
 import sympy as sp
@@ -101,3 +103,26 @@ def test_full_rhs_with_current_resistivity_and_hall_converges(stretch):
     assert np.all(fine < 5e-2), fine
     assert np.all(ratio > 3.3), ratio                                      # at least 2nd order
     assert ratio[0] > 13.0 and ratio[7] > 8.0, ratio   # rho has no J term; |J|^2 heats p little
+
+
+def test_rk4_step_converges_at_4th_order_in_time():
+    from oracle.oracle import gem_oracle
+    cfg = harris.RunConfig("rk-32x16x32", 32, 16, 32, False, 0.005, 0.5, 4, filter_every=10 ** 9)
+    o = gem_oracle(cfg)
+    T = 2 * o.setdt()
+    o.close()
+
+    def run(n):
+        o = gem_oracle(cfg)
+        for k in range(n):                  # nstep from 1: nstep % filter_every is never 0
+            o.stepon(k * T / n, T / n, 1 + k)
+        X = o.get_state()
+        o.close()
+        return X
+
+    ref = run(64)
+    scale = np.abs(ref).reshape(8, -1).max(axis=1)
+    err = {n: np.abs(run(n) - ref).reshape(8, -1).max(axis=1) / scale for n in (4, 8, 16)}
+    assert np.all(err[4] / err[8] > 13.0), err[4] / err[8]
+    r = err[8] / err[16]
+    assert np.all((r > 14.0) & (r < 18.0)), r
