@@ -40,3 +40,34 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = _bench("--impl", "reference", "--steps", "1", "--warmup", "0",
                env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_roofline_peak_is_the_measured_one_when_present(tmp_path, monkeypatch):
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.peaks() == (6650.0, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6531.5, "bf16_tflops": 1590.0}))
+    assert bench.peaks() == (6531.5, "measured")
+
+
+def test_clock_samples_give_median_max_and_active_reasons(tmp_path):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class Proc:
+        def terminate(self):
+            pass
+
+        def wait(self, timeout=None):
+            return 0
+
+    c = bench.Clocks()
+    c.path = str(tmp_path / "clocks.csv")
+    c.f = open(c.path, "w")
+    c.f.write("0, 1770, 1965, 998.1, 0x4, Not Active, Not Active, Not Active, Active\n"
+              "0, 1860, 1965, 990.0, 0x0, Not Active, Not Active, Not Active, Not Active\n"
+              "garbage line\n"
+              "0, 1800, 1965, 995.0, 0x4, Not Active, Not Active, Not Active, Active\n")
+    c.p = Proc()
+    assert c.stop() == {"sm_mhz": 1800.0, "sm_max_mhz": 1965.0, "reasons": ["sw_power_cap"], "samples": 3}
