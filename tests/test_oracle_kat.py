@@ -63,6 +63,47 @@ def test_difc_uniform_is_second_difference():
     np.testing.assert_array_equal(g[:2], f[:2])
 
 
+def _difc(fm, f0, fp, xm, x0, xp):
+    """The reference's active three-point difference, its "zero order diffusion" (t3dsdsc.f:
+    5618-5619, and the same statement in every smoothing routine):
+    2 ((fp - f0)(xp - x0) - (f0 - fm)(x0 - xm)) / (xp - xm).  The line after it, commented out,
+    is the "second-order" variant with the spacings the other way round; the two agree on a
+    uniform grid only, so the stretched case below tells them apart."""
+    return 2.0 * ((fp - f0) * (xp - x0) - (f0 - fm) * (x0 - xm)) / (xp - xm)
+
+
+@pytest.mark.parametrize("stretch", [False, True], ids=["uniform", "sinh-z"])
+@pytest.mark.parametrize("kind", [0, 2], ids=["radial", "x-profile"])
+def test_smoothing_pass_coefficients(kind, stretch):
+    """One pass f + c (difc_x + difc_y + difc_z) on the interior rows with the reference's
+    coefficients: c = 1/32 + (1/8 - 1/32) (1 + tanh((r - 3)/3)) / 2 for J, E and the non-B
+    fields of avrg / avrgtt (t3dsdsc.f:5659-5661, 5981-5983); c = (1/32)(1 - tanh((x + 3)/8))
+    for B in avrg / avrgtt (t3dsdsc.f:5636-5642, caf0 = 0 at T:1148).  x and y wrap with the
+    coordinates continued by one period."""
+    x, y, z = harris.make_grid(16, 8, 14, stretch)
+    o = _oracle(x, y, z)
+    f = np.random.default_rng(kind + 2 * stretch).standard_normal((z.size, y.size, x.size))
+    g = o.smooth_pass(f, kind)
+    Lx, Ly = harris.LX, harris.LY
+    xm, xp = np.roll(x, 1), np.roll(x, -1)
+    xm[0] -= Lx
+    xp[-1] += Lx
+    ym, yp = np.roll(y, 1), np.roll(y, -1)
+    ym[0] -= Ly
+    yp[-1] += Ly
+    s = (_difc(np.roll(f, 1, 2), f, np.roll(f, -1, 2), xm[None, None, :], x[None, None, :], xp[None, None, :])
+         + _difc(np.roll(f, 1, 1), f, np.roll(f, -1, 1), ym[None, :, None], y[None, :, None], yp[None, :, None]))
+    sz = np.zeros_like(f)
+    sz[1:-1] = _difc(f[:-2], f[1:-1], f[2:], z[:-2, None, None], z[1:-1, None, None], z[2:, None, None])
+    s += sz
+    Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+    if kind == 0:
+        c = 1 / 32 + (1 / 8 - 1 / 32) * 0.5 * (1 + np.tanh((np.sqrt(X ** 2 + Y ** 2 + Z ** 2) - 3.0) / 3.0))
+    else:
+        c = (1 / 32) * (1 - np.tanh((X + 3.0) / 8.0))
+    np.testing.assert_allclose(g[2:-2], (f + c * s)[2:-2], rtol=0, atol=1e-13)
+
+
 def test_equilibrium_is_steady():
     """x = eq: J1 = 0, v = 0, p - p0 = 0, so every RHS term vanishes (LITERAL equations)."""
     cfg = harris.RunConfig("eq", 16, 8, 24, True, 0.005, 0.5, 1)
