@@ -2,7 +2,9 @@
 
 For each seeded Harris/GEM case: the dt sequence of 4 reference steps (setdt, stepon), the
 diagnostics and the state after them, the smoothed current and one right-hand side of the
-initial state.  Volumes are kept as the mid-y plane (the plane the reference's outputs and
+initial state.  And the reference gradient of the reconnected flux on the adjoint's test
+configuration: d Phi / d eta and d Phi along two psi directions by central differences of
+two oracle runs each, with the dt sequence fixed.  Volumes are kept as the mid-y plane (the plane the reference's outputs and
 diagnostics use) plus per-field sums and L2 norms over every node, so the fixtures stay small.
 
     python tests/golden/make_golden.py          # rewrites tests/golden/*.npz
@@ -49,11 +51,39 @@ def make(cfg):
     return out
 
 
+# the reference gradient of the reconnected flux (central differences of two oracle runs per
+# parameter) on the adjoint's test configuration: eta and two psi directions
+ADJOINT_CFG = harris.RunConfig("adj-32x16x32", 32, 16, 32, False, 0.005, 0.5, 6)
+ADJOINT_BASIS_SEED = 10
+
+
+def adjoint_basis(k=2):
+    rng = np.random.default_rng(ADJOINT_BASIS_SEED)
+    return rng.standard_normal((k, ADJOINT_CFG.mz, ADJOINT_CFG.mx))
+
+
+def make_adjoint():
+    sys.path.insert(0, os.path.dirname(HERE))
+    from adjoint_torch import OracleModel
+    from oracle.oracle import gem_oracle
+    o = gem_oracle(ADJOINT_CFG)
+    _, dts = o.run(ADJOINT_CFG.steps)
+    o.close()
+    m = OracleModel(ADJOINT_CFG, adjoint_basis(), dts)
+    a0 = np.zeros(2)
+    g_eta, g_a = m.grad(ADJOINT_CFG.eta, a0)
+    return dict(dts=dts, phi=np.array(m.value(ADJOINT_CFG.eta, a0)), g_eta=np.array(g_eta), g_a=g_a,
+                h_eta=np.array(m.h_eta), h_a=np.array(m.h_a))
+
+
 def main():
     for cfg in CASES:
         path = os.path.join(HERE, cfg.name + ".npz")
         np.savez_compressed(path, **make(cfg))
         print(path, os.path.getsize(path), "bytes")
+    path = os.path.join(HERE, "reference-gradient-" + ADJOINT_CFG.name + ".npz")
+    np.savez_compressed(path, **make_adjoint())
+    print(path, os.path.getsize(path), "bytes")
 
 
 if __name__ == "__main__":

@@ -92,3 +92,15 @@ def test_gpu_fp32_close_to_fixture(cfg):
     err = [np.linalg.norm(plane[m] - r[m]) / np.linalg.norm(r[m]) for m in range(8)]
     assert max(err) < 2e-6, err
     d.close()
+
+
+def test_oracle_reproduces_the_reference_gradient():
+    """The reference gradient of the reconnected flux (central differences of two FP64 oracle
+    runs per parameter, dt sequence fixed) on the adjoint's test configuration."""
+    ref = dict(np.load(os.path.join(HERE, "reference-gradient-" + make_golden.ADJOINT_CFG.name + ".npz")))
+    got = make_golden.make_adjoint()
+    np.testing.assert_allclose(got["dts"], ref["dts"], rtol=1e-13, atol=0)
+    assert float(got["phi"]) == pytest.approx(float(ref["phi"]), rel=1e-13)
+    assert float(got["g_eta"]) == pytest.approx(float(ref["g_eta"]), rel=1e-6)
+    np.testing.assert_allclose(got["g_a"], ref["g_a"], rtol=1e-5)
+    assert abs(float(ref["g_eta"])) > 0 and np.all(np.abs(ref["g_a"]) > 0)
