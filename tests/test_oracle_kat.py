@@ -104,6 +104,38 @@ def test_smoothing_pass_coefficients(kind, stretch):
     np.testing.assert_allclose(g[2:-2], (f + c * s)[2:-2], rtol=0, atol=1e-13)
 
 
+@pytest.mark.parametrize("mz", [15, 16], ids=["odd-mz", "even-mz"])
+def test_diagnostics_follow_their_definitions(mz):
+    """The FP64 diagnostics as the C-ABI defines them (dasha_diagnostics): mass and energy
+    integrated with trapezoid weights (x, y periodic), the reconnected flux
+    (1/my) sum_y sum_x sqrt(Bz(z=0)^2 + 1e-20) dx with Bz(z=0) the central plane (odd mz) or
+    the mean of the two central planes (even mz), and the current's extrema on the plane
+    j = my/2 (diagn, t3dsdsc.f:1199-1214)."""
+    x, y, z = harris.make_grid(16, 8, mz, True)
+    o = _oracle(x, y, z)
+    rng = np.random.default_rng(mz)
+    X = rng.standard_normal((8, mz, 8, 16))
+    X[0] = 1.0 + 0.5 * rng.random(X[0].shape)
+    X[7] = 1.0 + 0.5 * rng.random(X[7].shape)
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    o.set_equilibrium(rho0, b0, p0)
+    o.set_state(X)
+    out = o.diagnostics()
+    cur = o.current()
+    dx, dy = harris.LX / 16, harris.LY / 8
+    wz = 0.5 * (z[np.minimum(np.arange(mz) + 1, mz - 1)] - z[np.maximum(np.arange(mz) - 1, 0)])
+    dV = wz[:, None, None] * dy * dx
+    mass = np.sum(X[0] * dV)
+    e = 0.5 * (X[1] ** 2 + X[2] ** 2 + X[3] ** 2) / X[0] + X[7] / (5.0 / 3.0 - 1.0) + 0.5 * (X[4] ** 2 + X[5] ** 2 + X[6] ** 2)
+    energy = np.sum(e * dV)
+    bz = X[6, mz // 2] if mz % 2 else 0.5 * (X[6, mz // 2 - 1] + X[6, mz // 2])
+    flux = np.sum(np.sqrt(bz ** 2 + 1e-20) * dx) / 8
+    plane = cur[:, :, 4, :]
+    ext = [plane[0].max(), plane[0].min(), plane[1].max(), plane[1].min(), plane[2].max(), plane[2].min()]
+    np.testing.assert_allclose(out[:3], [mass, energy, flux], rtol=1e-12)
+    np.testing.assert_array_equal(out[3:], ext)
+
+
 def test_equilibrium_is_steady():
     """x = eq: J1 = 0, v = 0, p - p0 = 0, so every RHS term vanishes (LITERAL equations)."""
     cfg = harris.RunConfig("eq", 16, 8, 24, True, 0.005, 0.5, 1)
