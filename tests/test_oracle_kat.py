@@ -136,6 +136,32 @@ def test_diagnostics_follow_their_definitions(mz):
     np.testing.assert_array_equal(out[3:], ext)
 
 
+def test_wall_rows():
+    """The fixed z rows: the right-hand side is 0 on the wall row and half its inner neighbour
+    on the next (bndry, t3dsdsc.f:1825-1826 and the upper wall), with and without the xdif
+    smoothing (t != 0: the rows are set again after each pass); after a step with the filter,
+    the perturbation x - eq follows the same rule (bndrytt, t3dsdsc.f:2135-2136)."""
+    from oracle.oracle import gem_oracle
+    cfg = harris.RunConfig("walls-32x16x24-sinh", 32, 16, 24, True, 0.005, 0.5, 1)
+    o = gem_oracle(cfg)
+    for t in (0.0, 0.5):
+        r = o.rhs(t)
+        assert np.abs(r).max() > 1e-3
+        assert (r[:, 0] == 0).all() and (r[:, -1] == 0).all()
+        assert (r[:, 1] == 0.5 * r[:, 2]).all() and (r[:, -2] == 0.5 * r[:, -3]).all()
+    o.stepon(0.0, o.setdt(), 0)
+    X = o.get_state()
+    rho0, b0, p0, _ = harris.harris_profiles(o.z)
+    eq = np.zeros_like(X)
+    for m, prof in ((0, rho0), (4, b0[0]), (5, b0[1]), (6, b0[2]), (7, p0)):
+        eq[m] = prof[:, None, None]
+    P = X - eq                                   # the state is held as totals: one rounding
+    scale = np.abs(P).max()
+    assert np.abs(P[:, 0]).max() <= 1e-14 * scale and np.abs(P[:, -1]).max() <= 1e-14 * scale
+    assert np.abs(P[:, 1] - 0.5 * P[:, 2]).max() <= 1e-14 * scale
+    assert np.abs(P[:, -2] - 0.5 * P[:, -3]).max() <= 1e-14 * scale
+
+
 def test_equilibrium_is_steady():
     """x = eq: J1 = 0, v = 0, p - p0 = 0, so every RHS term vanishes (LITERAL equations)."""
     cfg = harris.RunConfig("eq", 16, 8, 24, True, 0.005, 0.5, 1)
