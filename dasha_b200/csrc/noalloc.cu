@@ -86,6 +86,11 @@ extern "C" int dasha_current_noalloc(const dasha_grid_c* grid, const double* db_
     if (mx < 5 || my < 5 || mz < 7) return DASHA_E_INVALID;
     if (!(grid->periodic[0] == 1 && grid->periodic[1] == 1 && grid->periodic[2] == 0)) return DASHA_E_UNSUPPORTED;
     if ((long)mx * my * mz > kMaxCells || mx > kAxisMax || my > kAxisMax || mz > kAxisMax) return DASHA_E_NOSCRATCH;
+    {   // the curl reads neighbours of B while it writes J: the two ranges must be disjoint
+        const uintptr_t nb = 3u * sizeof(double) * (uintptr_t)mx * my * mz;
+        const uintptr_t a = reinterpret_cast<uintptr_t>(db_dev), b = reinterpret_cast<uintptr_t>(cur_dev);
+        if (a < b + nb && b < a + nb) return DASHA_E_INVALID;
+    }
     const double* coords[3] = {grid->x, grid->y, grid->z};
     const int n[3] = {mx, my, mz};
     for (int d = 0; d < 3; ++d)

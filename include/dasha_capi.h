@@ -188,7 +188,8 @@ int dasha_profile_read(dasha_ctx* ctx, int* n, char* names, double* ms, long* la
  * budget, or the allocator must not be called at that point).  Computes what dasha_current
  * computes for j0_mode LITERAL, J = S^4(curl(B - B0)) with the wall rows, from caller device
  * arrays: db_dev = B - B0 and cur_dev = J, each 3 fields of mx*my*mz FP64 values, node
- * (i,j,k) at i + mx*(j + my*k), field stride mx*my*mz.  Work is enqueued on `stream` (a
+ * (i,j,k) at i + mx*(j + my*k), field stride mx*my*mz; the two 3-field ranges must not
+ * overlap (an in-place call returns DASHA_E_INVALID).  Work is enqueued on `stream` (a
  * cudaStream_t, NULL for the default stream).  The ping-pong buffer and the stencil tables
  * live in one static device array of DASHA_NOALLOC_SCRATCH_DOUBLES doubles (about 26 MB) that
  * every GPU loading the library holds until exit; grids above DASHA_NOALLOC_MAX_CELLS nodes

@@ -115,6 +115,14 @@ def test_argument_checks_need_no_device():
     big = np.arange(2048.0)
     gb = capi.GridC(2048, 1024, 8, capi._dp(big), capi._dp(big), capi._dp(big), (ctypes.c_int * 3)(1, 1, 0))
     assert lib.dasha_current_noalloc(ctypes.byref(gb), ctypes.c_void_p(1), ctypes.c_void_p(1), None) == capi.E_NOSCRATCH
+    # ... and an in-place call (B - B0 and J overlapping), which the curl would read while it
+    # writes, also before any device call
+    z8 = np.arange(8.0)
+    gs = capi.GridC(8, 8, 8, capi._dp(z8), capi._dp(z8), capi._dp(z8), (ctypes.c_int * 3)(1, 1, 0))
+    nb = 3 * 8 * 8 * 8 * 8
+    for off in (0, 8, nb - 8):
+        assert lib.dasha_current_noalloc(ctypes.byref(gs), ctypes.c_void_p(1 << 20), ctypes.c_void_p((1 << 20) + off),
+                                         None) == capi.E_INVALID
 
 
 def test_library_stencil_weights_match_reference_closed_forms(tmp_path):
