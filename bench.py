@@ -155,14 +155,17 @@ def cpu_port_rate(steps=2, grid=(256, 128, 256), warm=0):
     return cfg.cells * steps / el, el
 
 
+CPU_GRID = (256, 128, 256)     # the reduced grid of the 1024x512x1024 comparison, scaled per cell
+
+
 def run_reference(args, rank, world):
-    """The reference's CPU path on the host cores: the oracle restatement (the Fortran
-    reference cannot be built here), each step a bounded sample grid."""
+    """The reference's CPU path on the host cores: the oracle restatement of the reference's
+    FP64 algorithm (the Fortran reference cannot be built here), all host threads, on the
+    256x128x256 grid with the driver's warm-up and timed steps."""
     if rank != 0:
         return
     from dasha_b200 import harris
-    kw = args.steps + args.warmup
-    grid = (256, 128, 256) if kw <= 16 else ((128, 64, 128) if kw <= 120 else (64, 32, 64))
+    grid = CPU_GRID
     rate, el = cpu_port_rate(steps=args.steps, grid=grid, warm=args.warmup)
     cfg = harris.CONFIGS[args.config]
     cores = os.cpu_count() or 1
@@ -176,6 +179,97 @@ def run_reference(args, rank, world):
                              "sample": sample},
             "e2e": {"value": rate, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# Profiler tags -> the __global__ instantiation they launch (several tags share one kernel:
+# the current and E chains both run the 3-field radial-coefficient smoothing pass).
+KERNEL_OF = {
+    "k_zpv_J": "k_zpv<3 fields, radial coef, store>", "k_zpv_E": "k_zpv<3 fields, radial coef, store>",
+    "k_zpv_H": "k_zpv2<3 fields, 1/8, two passes>", "k_zpv_EH": "k_zpv<6 fields, E + Hall sum>",
+    "k_zpv_X": "k_zpv<4 fields, store>", "k_zpv_F": "k_zpv<4 fields, store>",
+    "k_zpv_X_rk1": "k_zpv<4 fields, RK stage update>", "k_zpv_X_rk2": "k_zpv<4 fields, RK stage update>",
+    "k_zpv_X_rk3": "k_zpv<4 fields, RK stage update>", "k_zpv_X_rk4": "k_zpv<4 fields, RK stage update>",
+    "k_zpv_F1": "k_zpv<field pairs, compensated filter pass 1>",
+    "k_zpv_F2": "k_zpv<4 fields, compensated filter pass 2>",
+    "k_rhs_hydro": "k_zhydro", "k_efield_hall": "k_zeh", "k_curl": "k_zcurl<+1>",
+    "k_rhs_induction": "k_zcurl<-1>", "k_cfl": "k_cfl_rate",
+}
+
+
+def by_kernel(prof):
+    """Group the per-tag profile {tag: (ms, launches, bytes_per_launch)} by __global__:
+    {kernel: {"ms", "launches", "bytes", "tags"}} with bytes the algorithmic total."""
+    out = {}
+    for tag, (ms, n, b) in prof.items():
+        k = KERNEL_OF.get(tag, tag)
+        e = out.setdefault(k, {"ms": 0.0, "launches": 0, "bytes": 0.0, "tags": []})
+        e["ms"] += ms
+        e["launches"] += n
+        e["bytes"] += b * n
+        e["tags"].append(tag)
+    return out
+
+
+def accuracy_c2(steps: int):
+    """FP32 perturbation path against the FP64 path on the 512x256x512 sinh grid (d_i = 1,
+    whistler CFL): the FP64 run takes its CFL steps, the FP32 run replays them; per field the
+    relative L2 and max error of the total state, and the reconnected flux.  Then 10 timed
+    steps (setdt + stepon, CUDA events) of each path for their cell-updates/s."""
+    from dasha_b200 import accuracy, capi, harris
+    cfg = harris.CONFIGS["c2"]
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    eq = np.zeros((8, cfg.mz, 1, 1))
+    eq[0, :, 0, 0] = rho0
+    eq[4:7, :, 0, 0] = b0
+    eq[7, :, 0, 0] = p0
+    H = harris.gem_state_halo(x, y, z, threads=os.cpu_count() or 8)
+    ctx = {}
+    for prec in (0, 1):
+        d = capi.Dasha(x, y, z, capi.make_params(cfg, prec))
+        d.set_equilibrium(rho0, b0, p0)
+        d.set_state_halo(H)
+        ctx[prec] = d
+    del H
+    t, dts = 0.0, []
+    for n in range(steps):
+        dt = ctx[0].setdt(t)
+        ctx[0].stepon(t, dt, n)
+        dts.append(dt)
+        t += dt
+    tt = 0.0
+    for n, dt in enumerate(dts):
+        ctx[1].stepon(tt, dt, n)
+        tt += dt
+    s64, s32 = ctx[0].get_state(), ctx[1].get_state()
+    d64, d32 = ctx[0].diagnostics(), ctx[1].diagnostics()
+    fields = accuracy.compare(s32, s64, eq)
+    del s64, s32
+    rate = {}
+    for prec, name in ((0, "fp64"), (1, "fp32")):
+        d = ctx[prec]
+        tk, nk = t, steps
+        for _ in range(3):
+            dt = d.setdt(tk)
+            d.stepon(tk, dt, nk)
+            tk += dt
+            nk += 1
+        d.setdt(tk)
+        d.timer_start()
+        for _ in range(10):
+            dt = d.setdt(tk)
+            d.stepon(tk, dt, nk)
+            tk += dt
+            nk += 1
+        rate[name] = cfg.cells * 10 / (d.timer_stop() / 1e3)
+    for d in ctx.values():
+        d.close()
+    return {"workload": cfg.name, "steps": steps, "dt": "FP64 run's CFL steps replayed by the FP32 run",
+            "max_rel_l2": max(v["rel_l2_total"] for v in fields.values()),
+            "max_rel_max": max(v["rel_max_total"] for v in fields.values()),
+            "fields": {k: {"rel_l2": v["rel_l2_total"], "rel_max": v["rel_max_total"]} for k, v in fields.items()},
+            "flux_rel_err": float(abs(d32[2] - d64[2]) / abs(d64[2])),
+            "cell_updates_per_s": rate, "fp32_over_fp64": rate["fp32"] / rate["fp64"]}
 
 
 def run_dasha(args, rank, world):
@@ -215,13 +309,14 @@ def run_dasha(args, rank, world):
     d.profile(True)
     dt = d.setdt(t)
     d.stepon(t, dt, n)
-    d.setdt(t + dt)
     prof = d.profile_read()
     d.profile(False)
     launches_per_step = sum(v[1] for v in prof.values())
     tot = sum(v[0] for v in prof.values())
-    dom = max(prof.items(), key=lambda kv: kv[1][0])
-    dom_name, (dom_ms, dom_n, dom_bytes) = dom
+    kern = by_kernel(prof)
+    dom_name, dom = max(kern.items(), key=lambda kv: kv[1]["ms"])
+    dom_ms, dom_n = dom["ms"], dom["launches"]
+    dom_bytes = dom["bytes"] / dom_n
     peak, peak_kind = peaks()
     ach = dom_bytes / (dom_ms / dom_n / 1e3) / 1e9
     traffic = None
@@ -229,7 +324,7 @@ def run_dasha(args, rank, world):
     if os.path.exists(tpath):
         try:
             tr = json.load(open(tpath))
-            key = f"{dom_name}.{prec}"
+            key = f"{dom['tags'][0]}.{prec}"
             if key in tr:
                 traffic = tr[key] * cells
         except Exception:
@@ -268,26 +363,37 @@ def run_dasha(args, rank, world):
             "config": {"workload": cfg.name, "grid": [cfg.mx, cfg.my, cfg.mz], "precision": prec,
                        "state": "FP32 perturbation + Kahan RK4" if prec == "fp32" else "FP64",
                        "hall": cfg.hall, "filter_every": cfg.filter_every, "eta": cfg.eta, "di": cfg.di,
+                       "dt_whistler": cfg.dt_whistler,
+                       "cfl": "reference setdt + whistler speed d_i pi |B|/(rho h)" if cfg.dt_whistler
+                              else "reference setdt",
                        "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas{world}"},
             "e2e": e2e,
             "gpu_launches": int(launches_per_step * args.steps),
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "bytes_per_launch": dom_bytes, "avg_launch_ms": dom_ms / dom_n,
-                         "share_of_step": dom_ms / tot},
+                         "launches_per_step": dom_n, "share_of_step": dom_ms / tot},
             "step_roofline": {"algorithmic_bytes_per_cell_update": a_step, "achieved": step_ach,
                               "peak": peak, "unit": "GB/s", "frac": step_ach / peak},
-            "kernels": {k: {"ms_per_step": v[0], "launches": v[1], "GBps": v[2] * v[1] / (v[0] / 1e3) / 1e9}
-                        for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+            "kernels": {k: {"ms_per_step": v["ms"], "launches": v["launches"],
+                            "GBps": v["bytes"] / (v["ms"] / 1e3) / 1e9,
+                            "frac": v["bytes"] / (v["ms"] / 1e3) / 1e9 / peak}
+                        for k, v in sorted(kern.items(), key=lambda kv: -kv[1]["ms"])},
+            "tags": {k: {"ms_per_step": v[0], "launches": v[1], "GBps": v[2] * v[1] / (v[0] / 1e3) / 1e9}
+                     for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
             "clocks": ck}
     d.close()
     del H
+    if rank == 0 and world == 1 and args.acc_steps > 0 and prec == "fp32":
+        # outside every timed region: the FP32 path's error against FP64, and the FP64 path's rate
+        line["accuracy"] = accuracy_c2(args.acc_steps)
     if rank == 0 and world == 1 and not args.no_cpu:
-        rate, el = cpu_port_rate(steps=2)
+        rate, el = cpu_port_rate(steps=3, grid=CPU_GRID, warm=1)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-updates/s", "cores": os.cpu_count() or 1,
                                 "kind": "port",
-                                "sample": f"256x128x256 Harris/GEM grid, 2 RK4 steps ({el:.1f} s), "
-                                          "CPU FP64 oracle with OpenMP, scaled per cell"}
+                                "sample": f"{CPU_GRID[0]}x{CPU_GRID[1]}x{CPU_GRID[2]} Harris/GEM grid, 1 warm-up + "
+                                          f"3 timed RK4 steps ({el:.1f} s), CPU FP64 oracle with OpenMP, "
+                                          "scaled per cell"}
     if dist:
         dist.destroy_process_group()
     if rank == 0:
@@ -303,6 +409,8 @@ def main():
     ap.add_argument("--config", default="c4", choices=["c0", "c1", "c2", "c3", "c4"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--acc-steps", type=int, default=100,
+                    help="steps of the 512x256x512 FP32-vs-FP64 check after the timed region (0: skip)")
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.impl == "reference":

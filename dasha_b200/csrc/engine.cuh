@@ -10,6 +10,7 @@
 #include "zhydro.cuh"
 #include "zeh.cuh"
 #include "adjoint.cuh"
+#include "checkpoint_schedule.h"
 #include <cuda_runtime.h>
 #include <type_traits>
 #include <string>
@@ -1088,6 +1089,47 @@ public:
         }
     }
 
+    // Reverse sweep of one step j: the stage states of step j are in s1..s3, Xn is state j;
+    // lambda (in lam) goes from dPhi/dX_{j+1} to dPhi/dX_j.
+    // mu = F^T lambda (the post-step filter when step j filtered), then the RK4 stages in reverse:
+    // kappa4 = dt/6 mu, sigma3 = G'(S3)^T kappa4, kappa3 = dt/3 mu + dt sigma3, ...,
+    // lambda = mu + sigma0 + sigma1 + sigma2 + sigma3.
+    struct AdjVec { T *lam[8], *mu[8], *kap[8], *sig[8], *tot[8], *ta[8], *tb[8]; };
+    void adj_step(T* const* Xn, T* const* s1, T* const* s2, T* const* s3, double dt, bool filtered, AdjVec& v,
+                  AdjScratch& w) {
+        if (filtered) {
+            copy8(v.ta, v.lam);
+            T** r = adj_passes(v.ta, v.tb, 8, 2, 0u, false);
+            copy8(v.mu, r);
+        } else {
+            copy8(v.mu, v.lam);
+        }
+        copy8(v.tot, v.mu);                                    // lambda_X = mu + sum sigma
+        copy8(v.kap, v.mu);
+        axpby8(v.kap, dt / 6.0, v.mu, 0.0);                    // kappa4 = dt/6 mu
+        adj_rhs(s3, v.kap, v.sig, w);                          // sigma3
+        axpby8(v.tot, 1.0, v.sig, 1.0);
+        axpby8(v.kap, 0.0, v.mu, dt / 3.0);                    // kappa3 = dt/3 mu + dt sigma3
+        axpby8(v.kap, 1.0, v.sig, dt);
+        adj_rhs(s2, v.kap, v.sig, w);                          // sigma2
+        axpby8(v.tot, 1.0, v.sig, 1.0);
+        axpby8(v.kap, 0.0, v.mu, dt / 3.0);                    // kappa2 = dt/3 mu + dt/2 sigma2
+        axpby8(v.kap, 1.0, v.sig, dt / 2.0);
+        adj_rhs(s1, v.kap, v.sig, w);                          // sigma1
+        axpby8(v.tot, 1.0, v.sig, 1.0);
+        axpby8(v.kap, 0.0, v.mu, dt / 6.0);                    // kappa1 = dt/6 mu + dt/2 sigma1
+        axpby8(v.kap, 1.0, v.sig, dt / 2.0);
+        adj_rhs(Xn, v.kap, v.sig, w);                          // sigma0
+        axpby8(v.tot, 1.0, v.sig, 1.0);
+        copy8(v.lam, v.tot);
+    }
+    // the seed lambda = dPhi/dX_N of the reconnected flux of the final state X_N
+    void adj_seed(T* const* XN, T* const* lam) {
+        zero8(lam);
+        dim3 g2((mx + blk.x - 1) / blk.x, my, 1);
+        k_adj_flux_seed<<<g2, blk, 0, st>>>(g, XN[6], wx, lam[6]);
+    }
+
     Status adjoint_flux_grad(int nsteps, const double* dts, int snaps, double* deta, double* dpsi) override {
         if constexpr (!std::is_same<T, double>::value) {
             (void)nsteps; (void)dts; (void)snaps; (void)deta; (void)dpsi;
@@ -1097,117 +1139,85 @@ public:
             const int every = P.filter_every > 0 ? P.filter_every : 1;
             AdjBufs B;
             AdjScratch w;
-            // fields: scratch 60, 13 work vectors of 8, snapshots, segment states, stage states
+            // fields: scratch 60, 13 work vectors of 8, then either every step and stage state
+            // of the run (keep-all) or the binomial plan's state slots
             size_t freeb = 0, totb = 0;
             cudaMemGetInfo(&freeb, &totb);
             const size_t fb = adj_field_bytes(N);
             const size_t extra = adj_field_bytes(w_netap_max()) + adj_field_bytes((long)mx * mz) + 8192;
             const double budget = 0.85 * (double)freeb;
-            // snaps == 0: keep every step and stage state of the forward sweep when they fit
-            // (one segment, nothing recomputed), else sqrt(nsteps) segments
-            const size_t all_fields = 60 + 13 * 8 + 8 + (size_t)(nsteps + 1) * 8 + 24 * (size_t)nsteps;
+            const size_t fixed_fields = 60 + 13 * 8;
+            // snaps == 0: keep every step and stage state of the forward sweep when they fit (one
+            // forward sweep, nothing recomputed), else the binomial plan with as many state slots
+            // as fit; snaps > 0: the binomial plan with `snaps` free state slots
+            const size_t all_fields = fixed_fields + (size_t)(nsteps + 1) * 8 + 24 * (size_t)nsteps;
             const bool keep_all = snaps == 0 && (double)(all_fields * fb + extra) < budget;
-            if (snaps == 0 && !keep_all) snaps = std::max(1, (int)std::lround(std::sqrt((double)nsteps)));
-            const int seg = keep_all ? std::max(1, nsteps) : std::max(1, (nsteps + snaps - 1) / std::max(1, snaps));
-            const int nseg = (nsteps + seg - 1) / seg;
-            const size_t base_fields = 60 + 13 * 8 + (size_t)std::max(nseg, 1) * 8 + (size_t)(seg + 1) * 8;
-            const size_t with_stages = (base_fields + 24 * (size_t)seg) * fb + extra;
-            const bool keep_stages = keep_all || (double)with_stages < budget;
-            if (!B.reserve(keep_stages ? with_stages : base_fields * fb + extra))
-                return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
+            if (snaps == 0 && !keep_all) {
+                const double room = (budget - (double)(extra + (fixed_fields + 16) * fb)) / (8.0 * (double)fb);
+                if (room < 1.0) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
+                snaps = (int)std::min<double>(room, std::max(1, nsteps - 1));
+            }
+            if (!keep_all) snaps = std::max(1, std::min(snaps, std::max(1, nsteps - 1)));
+            const size_t want = keep_all ? all_fields * fb + extra : (fixed_fields + 16 + 8 * (size_t)snaps) * fb + extra;
+            if (!B.reserve(want)) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
             if (!adj_scratch(B, w)) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
             auto take8 = [&](T** a) { for (int m = 0; m < 8; ++m) if (!(a[m] = (T*)B.take(N))) return false; return true; };
-            std::vector<std::vector<T*>> snap(std::max(nseg, 1), std::vector<T*>(8));
-            std::vector<std::vector<T*>> sst(seg + 1, std::vector<T*>(8));
-            // stage states of every step of a segment, kept from the segment recompute when
-            // they fit (else each reverse step recomputes its own)
-            std::vector<std::vector<T*>> stg;
-            T *X0[8], *S1[8], *S2[8], *S3[8], *Xo[8], *Ac[8], *lam[8], *mu[8], *kap[8], *sig[8], *tot[8], *ta[8], *tb[8];
-            bool ok = take8(X0) && take8(S1) && take8(S2) && take8(S3) && take8(Xo) && take8(Ac) && take8(lam) && take8(mu) &&
-                      take8(kap) && take8(sig) && take8(tot) && take8(ta) && take8(tb);
-            for (auto& v : snap) ok = ok && take8(v.data());
-            for (auto& v : sst) ok = ok && take8(v.data());
+            T *X0[8], *S1[8], *S2[8], *S3[8], *Xo[8], *Ac[8];
+            AdjVec v;
+            bool ok = take8(X0) && take8(S1) && take8(S2) && take8(S3) && take8(Xo) && take8(Ac) && take8(v.lam) &&
+                      take8(v.mu) && take8(v.kap) && take8(v.sig) && take8(v.tot) && take8(v.ta) && take8(v.tb);
             if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
-            if (keep_stages) {
-                stg.assign(3L * seg, std::vector<T*>(8));
-                for (auto& v : stg) ok = ok && take8(v.data());
-                if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint stage states");
-            }
             copy8(X0, X);
-            // forward sweep with segment snapshots (keep_all: every step state into sst and its
-            // stage states into stg, so the reverse sweep recomputes nothing)
-            T *cur8[8], *nxt8[8];
             if (keep_all) {
+                // every step state and its stage states from one forward sweep
+                std::vector<std::vector<T*>> sst(nsteps + 1, std::vector<T*>(8)), stg(3L * nsteps, std::vector<T*>(8));
+                for (auto& q : sst) ok = ok && take8(q.data());
+                for (auto& q : stg) ok = ok && take8(q.data());
+                if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint stage states");
                 copy8(sst[0].data(), X0);
                 for (int n = 0; n < nsteps; ++n)
                     fwd_step(sst[n].data(), dts[n], n % every == 0, stg[3 * n].data(), stg[3 * n + 1].data(),
                              stg[3 * n + 2].data(), sst[n + 1].data(), Ac);
-                k8(cur8, sst[nsteps].data());
+                adj_seed(sst[nsteps].data(), v.lam);
+                for (int n = nsteps - 1; n >= 0; --n)
+                    adj_step(sst[n].data(), stg[3 * n].data(), stg[3 * n + 1].data(), stg[3 * n + 2].data(), dts[n],
+                             n % every == 0, v, w);
             } else {
-                copy8(ta, X0);
-                k8(cur8, ta);
-                k8(nxt8, tb);
-                for (int n = 0; n < nsteps; ++n) {
-                    if (n % seg == 0) copy8(snap[n / seg].data(), cur8);
-                    fwd_step(cur8, dts[n], n % every == 0, S1, S2, S3, nxt8, Ac);
-                    std::swap_ranges(cur8, cur8 + 8, nxt8);
-                }
-            }
-            // seed: dPhi/dX_N
-            zero8(lam);
-            {
-                dim3 g2((mx + blk.x - 1) / blk.x, my, 1);
-                k_adj_flux_seed<<<g2, blk, 0, st>>>(g, cur8[6], wx, lam[6]);
-            }
-            // reverse sweep, one segment at a time
-            for (int sgi = nseg - 1; sgi >= 0; --sgi) {
-                const int n0 = sgi * seg, n1 = std::min(nsteps, n0 + seg);
-                const bool keep = !stg.empty();
-                if (!keep_all) copy8(sst[0].data(), snap[sgi].data());
-                for (int n = n0; n < n1 - 1 && !keep_all; ++n) {
-                    const int q = n - n0;
-                    fwd_step(sst[q].data(), dts[n], n % every == 0, keep ? stg[3 * q].data() : S1,
-                             keep ? stg[3 * q + 1].data() : S2, keep ? stg[3 * q + 2].data() : S3, sst[q + 1].data(), Ac);
-                }
-                for (int n = n1 - 1; n >= n0; --n) {
-                    const int q = n - n0;
-                    T* const* Xn = sst[q].data();
-                    const double dt = dts[n];
-                    T *const *s1 = S1, *const *s2 = S2, *const *s3 = S3;
-                    if (keep && (keep_all || n < n1 - 1)) { s1 = stg[3 * q].data(); s2 = stg[3 * q + 1].data(); s3 = stg[3 * q + 2].data(); }
-                    else fwd_step(Xn, dt, false, S1, S2, S3, Xo, Ac);  // stage states of step n
-                    // mu = F^T lambda
-                    if (n % every == 0) {
-                        copy8(ta, lam);
-                        T** r = adj_passes(ta, tb, 8, 2, 0u, false);
-                        copy8(mu, r);
-                    } else {
-                        copy8(mu, lam);
+                // binomial checkpointing (checkpoint_schedule.h): slot 0 holds state 0, slots
+                // 1..snaps are free; reversing step j re-runs step j from state j for its stage
+                // states (the last step's run also gives the final state, and with it the seed)
+                std::vector<std::vector<T*>> slot(snaps + 1, std::vector<T*>(8));
+                T *cur[8], *nxt[8];
+                ok = take8(cur) && take8(nxt);
+                for (int q = 1; q <= snaps; ++q) ok = ok && take8(slot[q].data());
+                if (!ok) return Status::err(DASHA_E_NOMEM, "adjoint checkpoints do not fit in device memory");
+                for (int m = 0; m < 8; ++m) slot[0][m] = X0[m];
+                copy8(cur, X0);
+                for (const CkptAction& a : binomial_schedule(nsteps, snaps)) {
+                    switch (a.kind) {
+                        case CkptAction::Restore: copy8(cur, slot[a.a].data()); break;
+                        case CkptAction::Store: copy8(slot[a.a].data(), cur); break;
+                        case CkptAction::Release: break;
+                        case CkptAction::Advance:
+                            for (int j = a.a; j < a.b; ++j) {
+                                fwd_step(cur, dts[j], j % every == 0, S1, S2, S3, nxt, Ac);
+                                std::swap_ranges(cur, cur + 8, nxt);
+                            }
+                            break;
+                        case CkptAction::Reverse: {
+                            const int j = a.a;
+                            fwd_step(cur, dts[j], j % every == 0, S1, S2, S3, Xo, Ac);
+                            if (j == nsteps - 1) adj_seed(Xo, v.lam);
+                            adj_step(cur, S1, S2, S3, dts[j], j % every == 0, v, w);
+                            break;
+                        }
                     }
-                    copy8(tot, mu);                                    // lambda_X = mu + sum sigma
-                    copy8(kap, mu);
-                    axpby8(kap, dt / 6.0, mu, 0.0);                    // kappa4 = dt/6 mu
-                    adj_rhs(s3, kap, sig, w);                          // sigma3
-                    axpby8(tot, 1.0, sig, 1.0);
-                    axpby8(kap, 0.0, mu, dt / 3.0);                    // kappa3 = dt/3 mu + dt sigma3
-                    axpby8(kap, 1.0, sig, dt);
-                    adj_rhs(s2, kap, sig, w);                          // sigma2
-                    axpby8(tot, 1.0, sig, 1.0);
-                    axpby8(kap, 0.0, mu, dt / 3.0);                    // kappa2 = dt/3 mu + dt/2 sigma2
-                    axpby8(kap, 1.0, sig, dt / 2.0);
-                    adj_rhs(s1, kap, sig, w);                          // sigma1
-                    axpby8(tot, 1.0, sig, 1.0);
-                    axpby8(kap, 0.0, mu, dt / 6.0);                    // kappa1 = dt/6 mu + dt/2 sigma1
-                    axpby8(kap, 1.0, sig, dt / 2.0);
-                    adj_rhs(Xn, kap, sig, w);                          // sigma0
-                    axpby8(tot, 1.0, sig, 1.0);
-                    copy8(lam, tot);
                 }
             }
             // gradients: eta, and psi through dBx = -Dz psi, dBz = Dx psi
             double* dpsi_d = B.take((size_t)mx * mz);
             if (!dpsi_d) return Status::err(DASHA_E_NOMEM, "adjoint scratch");
-            k_adj_psi<<<dim3((mx + blk.x - 1) / blk.x, mz, 1), blk, 0, st>>>(g, lam[4], lam[6], dpsi_d);
+            k_adj_psi<<<dim3((mx + blk.x - 1) / blk.x, mz, 1), blk, 0, st>>>(g, v.lam[4], v.lam[6], dpsi_d);
             DASHA_CK(cudaGetLastError());
             std::vector<double> hp((size_t)mx * mz);
             DASHA_CK(cudaMemcpyAsync(hp.data(), dpsi_d, sizeof(double) * mx * mz, cudaMemcpyDeviceToHost, st));

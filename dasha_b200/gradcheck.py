@@ -49,6 +49,51 @@ def phi(cfg, x, y, z, X, dts, **over):
     return v
 
 
+def check(cfg, steps, snaps=0, dirs=10, log=None):
+    """The forward run, its adjoint gradient and the central-difference checks; returns the
+    report (errors, device times of the forward and the adjoint, their ratio)."""
+    x, y, z, X0 = initial_state(cfg)
+    d = ctx(cfg, x, y, z, X0)
+    d.timer_start()
+    _, dts = d.run(steps)
+    fwd_ms = d.timer_stop()
+    phi0 = d.diagnostics()[2]
+    d.close()
+    d = ctx(cfg, x, y, z, X0)
+    t0 = time.perf_counter()
+    d.timer_start()
+    g_eta, g_psi = d.adjoint_flux_grad(dts, snaps=snaps)
+    adj_ms = d.timer_stop()
+    adj_wall = time.perf_counter() - t0
+    d.close()
+    res = {"config": cfg.name, "steps": steps, "snaps": snaps, "phi": float(phi0),
+           "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_wall_s": adj_wall,
+           "adjoint_over_forward": adj_ms / fwd_ms, "dt_first_last": [float(dts[0]), float(dts[-1])]}
+    h = 1e-6
+    fd = (phi(cfg, x, y, z, X0, dts, eta=cfg.eta + h) - phi(cfg, x, y, z, X0, dts, eta=cfg.eta - h)) / (2 * h)
+    res["eta"] = {"adjoint": g_eta, "fd": fd, "rel_err": abs(g_eta - fd) / max(abs(fd), 1e-300)}
+    rng = np.random.default_rng(1)
+    out = []
+    for q in range(dirs):
+        dpsi = rng.standard_normal((cfg.mz, cfg.mx))
+        dpsi /= np.linalg.norm(dpsi)
+        dbx, dbz = harris.psi_to_dB(dpsi, x, z)
+        e = 1e-6
+        Xp, Xm = X0.copy(), X0.copy()
+        Xp[4] += e * dbx[:, None, :]
+        Xp[6] += e * dbz[:, None, :]
+        Xm[4] -= e * dbx[:, None, :]
+        Xm[6] -= e * dbz[:, None, :]
+        f = (phi(cfg, x, y, z, Xp, dts) - phi(cfg, x, y, z, Xm, dts)) / (2 * e)
+        ad = float(np.sum(g_psi * dpsi))
+        out.append({"adjoint": ad, "fd": f, "rel_err": abs(ad - f) / max(abs(f), 1e-300)})
+        if log:
+            log(json.dumps({"dir": q, **out[-1]}))
+    res["psi_dirs"] = out
+    res["max_rel_err"] = max([res["eta"]["rel_err"]] + [q["rel_err"] for q in out])
+    return res, dts, (g_eta, g_psi)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="c3")
@@ -61,45 +106,7 @@ def main(argv=None):
     cfg = harris.CONFIGS[a.config]
     if a.whistler is not None:
         cfg = dataclasses.replace(cfg, dt_whistler=a.whistler)
-    steps = a.steps or cfg.steps
-    x, y, z, X0 = initial_state(cfg)
-    d = ctx(cfg, x, y, z, X0)
-    d.timer_start()
-    _, dts = d.run(steps)
-    fwd_ms = d.timer_stop()
-    phi0 = d.diagnostics()[2]
-    d.close()
-    d = ctx(cfg, x, y, z, X0)
-    t0 = time.perf_counter()
-    d.timer_start()
-    g_eta, g_psi = d.adjoint_flux_grad(dts, snaps=a.snaps)
-    adj_ms = d.timer_stop()
-    adj_wall = time.perf_counter() - t0
-    d.close()
-    res = {"config": cfg.name, "steps": steps, "snaps": a.snaps, "phi": float(phi0),
-           "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "adjoint_wall_s": adj_wall,
-           "adjoint_over_forward": adj_ms / fwd_ms, "dt_first_last": [float(dts[0]), float(dts[-1])]}
-    h = 1e-6
-    fd = (phi(cfg, x, y, z, X0, dts, eta=cfg.eta + h) - phi(cfg, x, y, z, X0, dts, eta=cfg.eta - h)) / (2 * h)
-    res["eta"] = {"adjoint": g_eta, "fd": fd, "rel_err": abs(g_eta - fd) / max(abs(fd), 1e-300)}
-    rng = np.random.default_rng(1)
-    dirs = []
-    for q in range(a.dirs):
-        dpsi = rng.standard_normal((cfg.mz, cfg.mx))
-        dpsi /= np.linalg.norm(dpsi)
-        dbx, dbz = harris.psi_to_dB(dpsi, x, z)
-        e = 1e-6
-        Xp, Xm = X0.copy(), X0.copy()
-        Xp[4] += e * dbx[:, None, :]
-        Xp[6] += e * dbz[:, None, :]
-        Xm[4] -= e * dbx[:, None, :]
-        Xm[6] -= e * dbz[:, None, :]
-        f = (phi(cfg, x, y, z, Xp, dts) - phi(cfg, x, y, z, Xm, dts)) / (2 * e)
-        ad = float(np.sum(g_psi * dpsi))
-        dirs.append({"adjoint": ad, "fd": f, "rel_err": abs(ad - f) / max(abs(f), 1e-300)})
-        print(json.dumps({"dir": q, **dirs[-1]}), flush=True)
-    res["psi_dirs"] = dirs
-    res["max_rel_err"] = max([res["eta"]["rel_err"]] + [q["rel_err"] for q in dirs])
+    res, _, _ = check(cfg, a.steps or cfg.steps, a.snaps, a.dirs, log=lambda s: print(s, flush=True))
     txt = json.dumps(res, indent=1)
     if a.out:
         with open(a.out, "w") as f:

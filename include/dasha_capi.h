@@ -159,10 +159,13 @@ int dasha_diagnostics(dasha_ctx* ctx, double* out);
  * steps with the recorded dt sequence dt_seq[nsteps], starting from the current state, with
  * respect to eta (*dPhi_deta) and to a psi perturbation on the (x,z) nodes (dPhi_dpsi[mx*mz],
  * x fastest), where the perturbation enters the initial B as dBx = -Dz psi, dBz = Dx psi.
- * snaps > 0: two-level checkpointing with snaps stored step snapshots, each segment re-run
- * before its reverse sweep; snaps == 0: every step and stage state of the forward sweep is kept
- * when they fit in 85 % of the free device memory (no recomputation), else sqrt(nsteps)
- * snapshots.  FP64 contexts only.  The state of the context is left unchanged. */
+ * snaps > 0: binomial checkpointing (the revolve strategy of Griewank and Walther) with
+ * `snaps` free state slots besides the initial state: binomial_cost(nsteps, snaps) forward steps
+ * to reach the states the schedule stores (the fewest possible with that many slots), plus one
+ * re-run of every step for its stage states as it is reversed; snaps == 0: every step and stage
+ * state of one forward sweep is kept when they fit in 85 % of the free device memory (nothing is
+ * recomputed), else the binomial plan with as many slots as fit there.  FP64 contexts only.
+ * The state of the context is left unchanged. */
 int dasha_adjoint_flux_grad(dasha_ctx* ctx, int nsteps, const double* dt_seq, int snaps,
                             double* dPhi_deta, double* dPhi_dpsi);
 

@@ -7,7 +7,10 @@ configuration: d Phi / d eta and d Phi along two psi directions by central diffe
 two oracle runs each, with the dt sequence fixed.  Volumes are kept as the mid-y plane (the plane the reference's outputs and
 diagnostics use) plus per-field sums and L2 norms over every node, so the fixtures stay small.
 
-    python tests/golden/make_golden.py          # rewrites tests/golden/*.npz
+    python tests/golden/make_golden.py [cases] [adjoint] [c1]   # rewrites tests/golden/*.npz
+
+The c1 fixture (20 steps of the 256x128x256 configuration with the filter every 10 steps)
+takes a few minutes of oracle time on 8 cores.
 """
 import os
 import sys
@@ -76,15 +79,41 @@ def make_adjoint():
                 h_eta=np.array(m.h_eta), h_a=np.array(m.h_a))
 
 
-def main():
-    for cfg in CASES:
+# config c1 (256x128x256 sinh, eta 0.003, d_i 0.5) with the post-step filter every 10 steps:
+# 20 steps, so that the filter runs after steps 0 and 10 and is skipped after the others
+C1_STEPS = 20
+
+
+def make_c1():
+    from oracle.oracle import gem_oracle
+    cfg = harris.CONFIGS["c1"]
+    assert cfg.filter_every == 10
+    o = gem_oracle(cfg)
+    _, dts = o.run(C1_STEPS)
+    st_plane, st_sum, st_l2 = volume_summary(o.get_state())
+    out = dict(grid=np.array([cfg.mx, cfg.my, cfg.mz]), filter_every=np.array(cfg.filter_every), dts=dts,
+               state_plane=st_plane, state_sum=st_sum, state_l2=st_l2, diag=o.diagnostics())
+    o.close()
+    return out
+
+
+C1_FIXTURE = "oracle-c1-256x128x256-sinh-filter10-20steps"
+
+
+def main(which=("cases", "adjoint", "c1")):
+    if "c1" in which:
+        path = os.path.join(HERE, C1_FIXTURE + ".npz")
+        np.savez_compressed(path, **make_c1())
+        print(path, os.path.getsize(path), "bytes")
+    for cfg in CASES if "cases" in which else ():
         path = os.path.join(HERE, cfg.name + ".npz")
         np.savez_compressed(path, **make(cfg))
         print(path, os.path.getsize(path), "bytes")
-    path = os.path.join(HERE, "reference-gradient-" + ADJOINT_CFG.name + ".npz")
-    np.savez_compressed(path, **make_adjoint())
-    print(path, os.path.getsize(path), "bytes")
+    if "adjoint" in which:
+        path = os.path.join(HERE, "reference-gradient-" + ADJOINT_CFG.name + ".npz")
+        np.savez_compressed(path, **make_adjoint())
+        print(path, os.path.getsize(path), "bytes")
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]) or ("cases", "adjoint", "c1"))

@@ -115,8 +115,9 @@ def test_adjoint_gradient_matches_finite_differences():
 
 
 def test_adjoint_plans_agree():
-    """snaps=0 keeps every forward state (no recompute); snaps>0 re-runs segments: the same
-    arithmetic, so the gradients agree to rounding."""
+    """snaps=0 keeps every forward state (no recompute); snaps>0 follows the binomial schedule,
+    re-running steps from stored states: the same arithmetic, so the gradients agree to
+    rounding."""
     d = _ctx(CFG)
     _, dts = _ctx(CFG).run(CFG.steps)
     e0, p0 = d.adjoint_flux_grad(dts, snaps=0)
