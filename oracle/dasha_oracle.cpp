@@ -7,11 +7,17 @@
  * the CUDA library in dasha_b200/ with: only tests/, __graft_entry__.smoke() and the cpu_baseline /
  * reference leg of bench.py may load it.  The product never links or calls it.
  *
- * PARITY UNPINNED.  The reference ships no tests, golden vectors or fixtures, and it cannot
- * be built here (it needs a Fortran compiler and MPI; neither exists on these machines).
- * The restatement is therefore pinned only by known-answer tests derived from the
- * reference's own formulas (polynomial exactness of the stencil coefficients, difc on
- * uniform grids, equilibrium preservation, conservation, symmetry) in tests/.
+ * PINNED AGAINST THE REFERENCE ITSELF.  The reference ships no tests, golden vectors or
+ * fixtures, and no Fortran compiler exists on these machines; its own source is instead
+ * translated to C (oracle/f77c.py) and built under oracle/_ref/ (oracle/refmodel.py), and
+ * tests/test_reference_pin.py runs the reference's input, right, current, setdt and stepon
+ * beside this restatement on the same nodes and state: stencil coefficients, one right-hand
+ * side (Hall on and off, uniform and stretched z), the smoothed current, dt, and one RK4 step
+ * with the post-step filter agree to 1e-13..1e-16 of each field's scale on every node that the
+ * two codes' different x/y boundary handling cannot reach (the reference's periodic branches
+ * are defective, so it runs with its x/y walls there).  Known-answer tests derived from the
+ * reference's formulas (polynomial exactness of the stencil coefficients, difc on uniform
+ * grids, equilibrium preservation, conservation, symmetry) in tests/ pin the rest.
  *
  * Semantics of the one-domain build (the reference's 1x1 process grid):
  *   node (i,j,k), 0-based, x fastest, is the reference's (jx,jy,jz) = (i+3, j+1, k+3);

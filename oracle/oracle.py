@@ -1,6 +1,7 @@
 """ctypes wrapper of the CPU FP64 oracle (dasha_oracle.cpp).  TEST INFRASTRUCTURE ONLY:
 imported by tests/, __graft_entry__.smoke() and bench.py's CPU legs, never by the product.
-Parity unpinned (see dasha_oracle.cpp)."""
+Pinned against the reference program itself, translated and run on the host
+(tests/test_reference_pin.py; see dasha_oracle.cpp)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -62,13 +63,15 @@ class Oracle:
 
     def __init__(self, x, y, z, gamma=5.0 / 3.0, eta=0.005, di=0.5, cfl=0.4, hall=1, j0_mode=0,
                  filter_every=1, mu=0.0, drho=0.0, dp=0.0, viscos=1, diffu=1, threads=0, variant="",
-                 dt_whistler=0):
+                 dt_whistler=0, rcr=0.0):
+        """rcr: setdt takes cells with r >= rcr only (the reference's fixed threshold r >= 1,
+        t3dsdsc.f:4712, is rcr = 1; 0 takes every cell, the build's Harris runs)."""
         self.lib = load(variant)
         if threads:
             self.lib.oracle_set_threads(threads)
         self.x, self.y, self.z = (np.ascontiguousarray(a, np.float64) for a in (x, y, z))
         self.mx, self.my, self.mz = self.x.size, self.y.size, self.z.size
-        p = OracleParams(gamma=gamma, eta=eta, di=di, mu=mu, drho=drho, dp=dp, cfl=cfl, rcr=0.0, hall=hall,
+        p = OracleParams(gamma=gamma, eta=eta, di=di, mu=mu, drho=drho, dp=dp, cfl=cfl, rcr=rcr, hall=hall,
                          viscos=viscos, diffu=diffu, total_e=1, j0_mode=j0_mode, filter_every=filter_every,
                          precision=0, dt_whistler=dt_whistler)
         self.h = self.lib.oracle_create(self.mx, self.my, self.mz, _dp(self.x), _dp(self.y), _dp(self.z),
