@@ -151,6 +151,8 @@ public:
     double* red = nullptr;       // reduction scratch
     double* cfltab = nullptr;    // CFL rate tables: ich[mx+my+mz], vv[..], ih[..]
     int* flag = nullptr;         // blow-up flag
+    unsigned long long* rate_bits = nullptr;   // max CFL rate of the state, from the fused tap
+    bool rate_ok = false;        // rate_bits belongs to the current state (set by stepon)
     double* hpin = nullptr;      // pinned host scratch
     double* mpd = nullptr;       // the 11 mid-plane output fields (allocated on first use)
     Geo<T> g{};
@@ -170,6 +172,7 @@ public:
         if (red) cudaFree(red);
         if (cfltab) cudaFree(cfltab);
         if (flag) cudaFree(flag);
+        if (rate_bits) cudaFree(rate_bits);
         if (hpin) cudaFreeHost(hpin);
         if (mpd) cudaFree(mpd);
     }
@@ -278,6 +281,7 @@ public:
         nred = 2L * my * mz + my + 6L * mz + 64;
         DASHA_CK(cudaMalloc(&red, sizeof(double) * (nred + 16)));
         DASHA_CK(cudaMalloc(&flag, sizeof(int)));
+        DASHA_CK(cudaMalloc(&rate_bits, sizeof(unsigned long long)));
         DASHA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
         DASHA_CK(cudaMallocHost(&hpin, sizeof(double) * 16));
 
@@ -299,6 +303,7 @@ public:
     }
 
     Status upload_eq() {
+        rate_ok = false;   // the CFL rate is of the totals: a new equilibrium invalidates it
         std::vector<double> h(16L * mz, 0.0);
         for (int k = 0; k < mz; ++k) {
             h[k] = rho0h[k]; h[mz + k] = b0h[0][k]; h[2 * mz + k] = b0h[1][k]; h[3 * mz + k] = b0h[2][k];
@@ -495,6 +500,7 @@ public:
     }
 
     Status state_in(const ChunkIn& fill) override {
+        rate_ok = false;
         Status s = stream_in(X, 8, true, fill);
         if (s.code) return s;
         if (KAHAN) for (int m = 0; m < 8; ++m) DASHA_CK(cudaMemsetAsync(C[m], 0, sizeof(T) * N, st));
@@ -604,6 +610,7 @@ public:
         if ((e = zp_attr1<4, KIND_B4, St4>())) return e;
         if ((e = zp_attr1<4, 0u, RK4>())) return e;
         if ((e = zp_attr1<4, KIND_B4, RK4>())) return e;
+        if ((e = zp_attr1<4, KIND_B4, WithCfl<St4, T, ZVX>>())) return e;
         if ((e = zp2_attr1<3, KIND_H, St3>())) return e;
         if constexpr (KAHAN) {
             if ((e = zp_attr1<4, 0u, VStore<T, 2, ZVX>, 1>())) return e;
@@ -611,6 +618,7 @@ public:
             if ((e = zp_attr1<4, KIND_P67, VStore<T, 2, ZVX>, 1>())) return e;
             if ((e = zp_attr1<4, 0u, VKF<T, 4, ZVX>, 2>())) return e;
             if ((e = zp_attr1<4, KIND_B4, VKF<T, 4, ZVX>, 2>())) return e;
+            if ((e = zp_attr1<4, KIND_B4, WithCfl<VKF<T, 4, ZVX>, T, ZVX>, 2>())) return e;
         }
         if ((e = cudaFuncSetAttribute(k_zst2<T, 5, ZTX, 8, HMINB, OpHydro<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZS2<T, 5, ZTX, 8>::smem(true))))
@@ -652,6 +660,36 @@ public:
     // both xdif avrg passes of the raw RHS k, the second ending in the RK stage update: x =
     // stage state (or the step result at stage 4), base, acc, comp (FP32 Kahan compensation or
     // null)
+    // The fused CFL tap (CflTap, mhd_kernels.cuh) reading back the final state f, its maximum
+    // into rate_bits (cleared here, on the stream, before the tapped launch)
+    CflTap<T> cfl_tap(T* const* f) {
+        CflTap<T> c;
+        for (int m = 0; m < 8; ++m) c.x.f[m] = f[m];
+        const long nt = (long)mx + my + mz;
+        c.ich = cfltab; c.vv = cfltab + nt; c.ih = cfltab + 2 * nt;
+        c.rho0 = g.rho0; c.bx0 = g.bx0; c.by0 = g.by0; c.bz0 = g.bz0; c.p0 = g.p0;
+        c.gamma = P.gamma;
+        c.whistler = (P.dt_whistler && P.hall) ? P.di * 3.141592653589793 : 0.0;
+        c.mx = mx; c.my = my; c.mz = mz; c.sy = (unsigned)mx; c.sz = (unsigned)((long)mx * my);
+        c.out = rate_bits;
+        cudaMemsetAsync(rate_bits, 0, sizeof(unsigned long long), st);
+        return c;
+    }
+    template <class E>
+    WithCfl<E, T, ZVX> with_cfl(const E& e, T* const* f) {
+        WithCfl<E, T, ZVX> w;
+        static_cast<E&>(w) = e;
+        w.tap = cfl_tap(f);
+        w.best = 0.0;
+        return w;
+    }
+    // the tap reads 8 fields back per node: 4 finished by the launch before (DRAM), 4 just
+    // stored (L2)
+    double tap_bytes() const { return 4.0 * sizeof(T) * N; }
+
+    // both xdif avrg passes of the raw RHS k, the second ending in the RK stage update: x =
+    // stage state (or the step result at stage 4), base, acc, comp (FP32 Kahan compensation or
+    // null)
     void rk_passes(int stage, double dt, T* const* k, T* const* base, T* const* x, T* const* acc, T* const* comp) {
         static const char* names[4] = {"k_zpv_X_rk1", "k_zpv_X_rk2", "k_zpv_X_rk3", "k_zpv_X_rk4"};
         T* t[8];
@@ -672,7 +710,7 @@ public:
 
     // avrgtt on the compensated FP32 state (X, C): pass 1 writes its increment of X - C into
     // t, pass 2 adds the two-pass increment to (X, C) in place with a Kahan step
-    void filter_compensated(T* const* t) {
+    void filter_compensated(T* const* t, bool tap = false) {
         for (int lo = 0; lo < 8; lo += 2) {   // pass 1 by field pairs: ring (x_a, x_b, comp_a, comp_b)
             SrcFields<T, 4> a;
             VStore<T, 2, ZVX> o;
@@ -687,7 +725,8 @@ public:
             VKF<T, 4, ZVX> e;
             for (int q = 0; q < 4; ++q) { d.f[q] = t[lo + q]; e.x[q] = X[lo + q]; e.comp[q] = C[lo + q]; }
             if (lo == 0) zp<4, 0u, 2>("k_zpv_F2", 20.0 * N * sizeof(T), d, e);
-            else zp<4, KIND_B4, 2>("k_zpv_F2", 20.0 * N * sizeof(T), d, e);
+            else if (!tap) zp<4, KIND_B4, 2>("k_zpv_F2", 20.0 * N * sizeof(T), d, e);
+            else zp<4, KIND_B4, 2>("k_zpv_F2", 20.0 * N * sizeof(T) + tap_bytes(), d, with_cfl(e, X));
         }
     }
 
@@ -811,21 +850,30 @@ public:
     Status stepon(double time, double dt, int nstep) override {
         (void)time;
         // stages 1..4: base = X, stage state in S, accumulator in A; both xdif smoothing
-        // passes run in one k_zpv2 launch per field pair that ends in the RK stage update
+        // passes run in one k_zpv2 launch per field pair that ends in the RK stage update.  When
+        // the post-step filter runs, its last launch (fields B, p) also takes the CFL rate of the
+        // new state for the next setdt (the tap leaves that launch's registers unchanged; on the
+        // RK stage-4 launch it would lower occupancy, so a step without the filter leaves setdt
+        // its own sweep).
+        const int every = P.filter_every > 0 ? P.filter_every : 1;
+        const bool filt = nstep % every == 0;
+        rate_ok = false;
         for (int stage = 1; stage <= 4; ++stage) {
             launch_rhs_raw(stage == 1 ? X : S);
             rk_passes(stage, dt, K, X, S, A, KAHAN ? C : nullptr);
         }
         for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
-        int every = P.filter_every > 0 ? P.filter_every : 1;
-        if (nstep % every == 0) {   // avrgtt on the perturbation (t3dsdsc.f:1135-1165)
+        if (filt) {   // avrgtt on the perturbation (t3dsdsc.f:1135-1165)
             T* t[8];
             tmp8(t);
             if constexpr (KAHAN) {
-                filter_compensated(t);
+                filter_compensated(t, true);
             } else {
                 pass8("k_zpv_F", 16.0, X, [&](int lo) { return st4(t, lo); });
-                pass8("k_zpv_F", 16.0, t, [&](int lo) { return st4(S, lo); });
+                SrcFields<T, 4> a, b;
+                for (int q = 0; q < 4; ++q) { a.f[q] = t[q]; b.f[q] = t[4 + q]; }
+                zp<4, 0u>("k_zpv_F", 8.0 * N * sizeof(T), a, st4(S, 0));
+                zp<4, KIND_B4>("k_zpv_F", 8.0 * N * sizeof(T) + tap_bytes(), b, with_cfl(st4(S, 4), S));
                 for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
             }
         }
@@ -834,6 +882,7 @@ public:
             if (s.code) return s;
         }
         DASHA_CK(cudaGetLastError());
+        rate_ok = filt;
         return Status::ok();
     }
 
@@ -863,6 +912,17 @@ public:
     }
 
     Status setdt(double* dt, int* blowup) override {
+        if (rate_ok) {   // the rate of this state was taken by the last stepon's final launch
+            DASHA_CK(cudaMemcpyAsync(hpin + 12, rate_bits, sizeof(double), cudaMemcpyDeviceToHost, st));
+            DASHA_CK(cudaMemcpyAsync(hpin + 13, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+            DASHA_CK(cudaStreamSynchronize(st));
+            const double v = hpin[12];
+            int fl = 0;
+            std::memcpy(&fl, hpin + 13, sizeof(int));
+            *dt = (v != v) ? v : std::fmin(100.0, 1.0 / v);   // as k_reduce_rate
+            *blowup = fl;
+            return Status::ok();
+        }
         dim3 g2(1, my, mz);
         const long nt = (long)mx + my + mz;
         DASHA_LAUNCH("k_cfl", 8.0 * N * sizeof(T),
@@ -1224,6 +1284,7 @@ public:
             double he = 0.0;
             DASHA_CK(cudaMemcpyAsync(&he, w.eta_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
             copy8(X, X0);                                              // the context state is unchanged
+            rate_ok = false;
             DASHA_CK(cudaStreamSynchronize(st));
             *deta = he;
             std::memcpy(dpsi, hp.data(), sizeof(double) * mx * mz);

@@ -185,6 +185,95 @@ __device__ __forceinline__ double warp_sum(double v) {
 // row; NaN wins so that a corrupted state is reported.
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a != a ? a : b) : fmax(a, b); }
 
+// The CFL rate of node c (totals = equilibrium profile at the node's plane + stored
+// perturbation), max over the three directions; shared by k_cfl_rate and the fused tap.
+template <class T>
+__device__ __forceinline__ double cfl_node_rate(const F8<T>& x, long c, double r0, double bx0, double by0, double bz0,
+                                                double p0, double gamma, double whistler, double cx, double vx_,
+                                                double hx, double cy, double vy_, double hy, double cz, double vz_,
+                                                double hz) {
+    double rinv = 1.0 / (r0 + (double)x.f[0][c]);
+    double vx = (double)x.f[1][c] * rinv, vy = (double)x.f[2][c] * rinv, vz = (double)x.f[3][c] * rinv;
+    double b1 = bx0 + (double)x.f[4][c], b2 = by0 + (double)x.f[5][c], b3 = bz0 + (double)x.f[6][c];
+    double bb = b1 * b1 + b2 * b2 + b3 * b3;
+    double vf = sqrt(fabs((bb + gamma * (p0 + (double)x.f[7][c])) * rinv));
+    double w = whistler != 0.0 ? whistler * sqrt(bb) * rinv : 0.0;
+    double rx = (fabs(vx) + vf + w * hx) * cx + vx_;
+    double ry = (fabs(vy) + vf + w * hy) * cy + vy_;
+    double rz = (fabs(vz) + vf + w * hz) * cz + vz_;
+    return nanmax(rx, nanmax(ry, rz));
+}
+
+// The fused form of setdt's sweep (survey row f3): the step's last launch, after it stores the
+// final B and p of a node (rho and rho v of the node were finished by the launch before it),
+// reads the node's 8 fields back and folds its CFL rate into a running maximum; at the end of
+// the launch each CTA adds its maximum with one atomicMax on the bits of a double (rates are
+// >= 0, so their bit patterns order as unsigned integers, and a NaN pattern lies above every
+// finite one: NaN wins as in k_cfl_rate).  The next dasha_setdt then needs no pass over the
+// state.  Region and formula as k_cfl_rate.
+template <class T>
+struct CflTap {
+    F8<T> x;
+    const double *ich, *vv, *ih;   // per-axis tables, x | y | z concatenated
+    const double *rho0, *bx0, *by0, *bz0, *p0;
+    double gamma, whistler;
+    int mx, my, mz;
+    unsigned sy, sz;
+    unsigned long long* out;
+    __device__ __forceinline__ double rate(long i) const {
+        const unsigned n = (unsigned)i, k = n / sz, r = n - k * sz, j = r / sy, ix = r - j * sy;
+        if ((int)k > mz - 3 || (int)j > my - 2 || (int)ix > mx - 3) return 0.0;
+        const double *iy = ich + mx, *iz = ich + mx + my, *wy = vv + mx, *wz = vv + mx + my;
+        const double *hy = ih + mx, *hz = ih + mx + my;
+        return cfl_node_rate(x, i, rho0[k], bx0[k], by0[k], bz0[k], p0[k], gamma, whistler, ich[ix], vv[ix], ih[ix],
+                             iy[j], wy[j], hy[j], iz[k], wz[k], hz[k]);
+    }
+};
+
+// An epilogue with the tap: stores through Inner, then takes the rate of each stored node
+template <class Inner, class T, int VX>
+struct WithCfl : Inner {
+    CflTap<T> tap;
+    mutable double best;
+    using Pre = typename Inner::Pre;
+    __device__ __forceinline__ void take(long i) const {
+#pragma unroll
+        for (int e = 0; e < VX; ++e) best = nanmax(best, tap.rate(i + e));
+    }
+    template <class V>
+    __device__ __forceinline__ void store(long i, const V& v, const Pre& p) const { Inner::store(i, v, p); take(i); }
+    template <class V>
+    __device__ __forceinline__ void wall(long i, const V& v) const { Inner::wall(i, v); take(i); }
+    template <class V>
+    __device__ __forceinline__ void store_rows(long i, bool wall, long ih, long iz, const V& v, const Pre& p) const {
+        Inner::store_rows(i, wall, ih, iz, v, p);
+        take(i);
+        if (wall) { take(ih); take(iz); }
+    }
+    // every thread of the CTA, after its last store
+    __device__ __forceinline__ void finish() const {
+        __shared__ double sh[32];
+        double v = best;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (lane == 0) sh[wid] = v;
+        __syncthreads();
+        if (wid == 0) {
+            const int nw = (blockDim.x + 31) >> 5;
+            v = lane < nw ? sh[lane] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_down_sync(0xffffffffu, v, o));
+            if (lane == 0 && v != 0.0) atomicMax(tap.out, (unsigned long long)__double_as_longlong(v));
+        }
+    }
+};
+
+template <class E, class = void>
+struct has_finish { static constexpr bool value = false; };
+template <class E>
+struct has_finish<E, decltype((void)&E::finish)> { static constexpr bool value = true; };
+
 template <class T>
 __global__ void k_cfl_rate(Geo<T> g, F8<T> x, const double* ich, const double* vv, const double* ih, double gamma,
                            double whistler, double* partial) {
@@ -205,16 +294,8 @@ __global__ void k_cfl_rate(Geo<T> g, F8<T> x, const double* ich, const double* v
         const double cy = ichy[jj], vy_ = vvy[jj], cz = ichz[k], vz_ = vvz[k], hy = ihy[jj], hz = ihz[k];
         for (int i = threadIdx.x; i <= g.mx - 3; i += blockDim.x) {
             long c = (long)i + (long)jj * g.sy + (long)k * g.sz;
-            double rinv = 1.0 / (r0 + (double)x.f[0][c]);
-            double vx = (double)x.f[1][c] * rinv, vy = (double)x.f[2][c] * rinv, vz = (double)x.f[3][c] * rinv;
-            double b1 = bx0 + (double)x.f[4][c], b2 = by0 + (double)x.f[5][c], b3 = bz0 + (double)x.f[6][c];
-            double bb = b1 * b1 + b2 * b2 + b3 * b3;
-            double vf = sqrt(fabs((bb + gamma * (p0 + (double)x.f[7][c])) * rinv));
-            double w = whistler != 0.0 ? whistler * sqrt(bb) * rinv : 0.0;
-            double rx = (fabs(vx) + vf + w * ihx[i]) * ichx[i] + vvx[i];
-            double ry = (fabs(vy) + vf + w * hy) * cy + vy_;
-            double rz = (fabs(vz) + vf + w * hz) * cz + vz_;
-            best = nanmax(best, nanmax(rx, nanmax(ry, rz)));
+            best = nanmax(best, cfl_node_rate(x, c, r0, bx0, by0, bz0, p0, gamma, whistler, ichx[i], vvx[i], ihx[i],
+                                              cy, vy_, hy, cz, vz_, hz));
         }
     }
     __shared__ double sh[32];

@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
                 for (int e = 0; e < VX; ++e) { qm[u][f][e] = q0[u][f][e]; q0[u][f][e] = qp[u][f][e]; }
     }
     cp_async_wait<0>();
+    if constexpr (has_finish<Epi>::value) epi.finish();   // the fused CFL maximum (WithCfl)
 }
 
 }  // namespace dasha

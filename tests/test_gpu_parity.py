@@ -226,3 +226,27 @@ def test_invalid_arguments():
     with pytest.raises(capi.DashaError) as ei:
         capi.Dasha(x, y, z, capi.make_params(cfg, 0, rcr=1.0))
     assert ei.value.code == capi.E_UNSUPPORTED
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("every", [1, 3])
+def test_fused_cfl_rate_equals_the_sweep(precision, every):
+    """After a step that ran the post-step filter, the filter's last launch has taken the CFL
+    rate of the new state and dasha_setdt only reads it back; re-setting the (same) equilibrium
+    discards it, so the next dasha_setdt sweeps the state as setdt does: both dt agree to the
+    last bit, on filtered and unfiltered steps."""
+    import dataclasses
+    cfg = dataclasses.replace(RAGGED, filter_every=every)
+    d = capi.gem_context(cfg, precision)
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    t = 0.0
+    for n in range(4):
+        dt = d.setdt(t)
+        d.stepon(t, dt, n)
+        t += dt
+        fused = d.setdt(t)
+        d.set_equilibrium(rho0, b0, p0)
+        swept = d.setdt(t)
+        assert fused == swept, (n, fused, swept)
+    d.close()
