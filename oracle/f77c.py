@@ -975,7 +975,7 @@ class Translator:
                     size = 1
                     for lo, hi in s.dims:
                         size *= self.eval_const(u, hi) - self.eval_const(u, lo) + 1
-                    o.append(f"  static {CT[t]} v_{n}[{size}];")
+                    o.append(f"  static REF_TLS {CT[t]} v_{n}[{size}];")
                 except F77Error:
                     # bounds from run-time values (an automatic array): allocated at entry
                     ext = " * ".join(f"(long)(({self.dim_expr(u, hi)}) - ({self.dim_expr(u, lo)}) + 1)"
@@ -1149,7 +1149,7 @@ class Translator:
                 for lo, hi in dims:
                     size *= hi - lo + 1
                 out.append(f"  {CT[t]} {n}" + (f"[{size}]" if dims else "") + ";")
-            out.append(f"}} cb_{blk};")
+            out.append(f"}};\nREF_TLS struct cb_t_{blk} cb_{blk};")
         bodies, sigs = [], []
         for n in self.order:
             b, sig = self.translate_unit(self.units[n])
@@ -1174,7 +1174,9 @@ class Translator:
                     size *= hi - lo + 1
                     shape.append(hi - lo + 1)
                 rows.append((n, blk, t, size, shape))
-        o = ["typedef struct { const char* name; void* addr; char type; long size; int rank; long shape[7]; } ref_sym;",
+        # (the table holds addresses: not for a build whose COMMON blocks are thread-local)
+        o = ["#ifndef REF_NO_SYMBOLS",
+             "typedef struct { const char* name; void* addr; char type; long size; int rank; long shape[7]; } ref_sym;",
              "static ref_sym ref_syms[] = {"]
         for n, blk, t, size, shape in rows:
             sh = ", ".join(str(x) for x in shape + [0] * (7 - len(shape)))
@@ -1187,7 +1189,8 @@ class Translator:
     return 1;
   }
   return 0;
-}""")
+}
+#endif""")
         return "\n".join(o)
 
 
@@ -1246,6 +1249,11 @@ PRELUDE = r"""/* Generated by oracle/f77c.py from the reference program's Fortra
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+/* REF_TLS empty: one program per process.  -DREF_TLS=__thread: every COMMON block and static
+ * local array per thread, so that threads run as the ranks of an MPI decomposition. */
+#ifndef REF_TLS
+#define REF_TLS
+#endif
 void ref_unreachable(const char* what);
 void ref_stop(const char* where);
 #define DEF_POW(T, S) \

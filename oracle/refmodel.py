@@ -43,6 +43,10 @@ MPI_PROC_NULL = -2
 # interior band no boundary row reaches (160x144x33)
 PIN_GRIDS = [(64, 48, 33), (160, 144, 33)]
 
+# the benchmark's CPU leg: the 256x128x256 grid on these process grids (threads = ranks)
+BENCH_GRID = (256, 128, 256)
+BENCH_DECOMPS = [(8, 4), (4, 4), (4, 2), (2, 2), (2, 1), (1, 1)]
+
 NOT_TRANSLATED = ["readin", "cn"]
 DISABLED = ["recrd", "recrd2", "recrd3", "recrdint", "recrdpe", "gridpntnew2", "gridpnt", "gridpntnew"]
 
@@ -84,6 +88,55 @@ def build(mx: int, my: int, mz: int, uniform_cht: bool = False, force: bool = Fa
     subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-strict-aliasing", "-w",
                     "-o", out, cpath, os.path.join(HERE, "mpi_stub.c"), "-lm"], check=True)
     return out
+
+
+def ranks_path(mx, my, mz, nprx, nprz):
+    return os.path.join(REF_DIR, f"libref_ranks_{mx}x{my}x{mz}_{nprx}x{nprz}.so")
+
+
+def build_ranks(mx: int, my: int, mz: int, nprx: int, nprz: int, force: bool = False) -> str:
+    """The reference at this grid size and process grid, its ranks run as threads
+    (ref_ranks.c, mpi_threads.c); the Hall coefficient uniform as in `build(uniform_cht=True)`."""
+    if mx % nprx > 1 or mz % nprz > 1:
+        raise ValueError("the reference needs mod(mx, nprx) <= 1 and mod(mz, nprz) <= 1 (t3dsdsc.f:42)")
+    out = ranks_path(mx, my, mz, nprx, nprz)
+    if os.path.exists(out) and not force:
+        return out
+    if not os.path.exists(REFERENCE_SRC):
+        raise FileNotFoundError(f"the reference source {REFERENCE_SRC} is not on this machine")
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("dasha_f77c", os.path.join(HERE, "f77c.py"))
+    f77c = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(f77c)
+    csrc = f77c.translate(REFERENCE_SRC,
+                          params={"mx1": mx, "my1i": my, "my1o": 0, "mz1i": mz, "mz1o": 0, "nprx": nprx, "nprz": nprz},
+                          assign={("right", "cht"): "ref_cht_value"}, stubs=NOT_TRANSLATED, empty=DISABLED)
+    csrc = csrc.replace("#include <string.h>\n", "#include <string.h>\ndouble ref_cht_value = 0.0;\n", 1)
+    os.makedirs(REF_DIR, exist_ok=True)
+    cpath = out[:-3] + ".c"
+    with open(cpath, "w") as f:
+        f.write(csrc)
+    subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-strict-aliasing", "-w", "-pthread",
+                    "-DREF_TLS=__thread", "-DREF_NO_SYMBOLS", f'-DREF_GENERATED="{cpath}"', "-o", out,
+                    os.path.join(HERE, "ref_ranks.c"), os.path.join(HERE, "mpi_threads.c"), "-lm"], check=True)
+    return out
+
+
+def run_ranks(mx, my, mz, nprx, nprz, x, y, z, X, rho0, b0, p0, eta, di, hall, cfl, warm, steps, want_state=True):
+    """warm + steps steps of the reference on nprx x nprz thread ranks from state X (8, mz, my,
+    mx); returns (seconds of the timed steps, dt sequence, final state or None)."""
+    lib = C.CDLL(ranks_path(mx, my, mz, nprx, nprz))
+    D = C.POINTER(C.c_double)
+    lib.ref_ranks_run.argtypes = [C.c_int] * 5 + [D] * 9 + [C.c_double, C.c_double, C.c_int, C.c_double,
+                                                           C.c_int, C.c_int, D, D, D]
+    arrs = [np.ascontiguousarray(a, np.float64) for a in (x, y, z, X, rho0, b0[0], b0[1], b0[2], p0)]
+    out = np.zeros_like(arrs[3]) if want_state else None
+    sec = np.zeros(1)
+    dts = np.zeros(warm + steps)
+    p = lambda a: a.ctypes.data_as(D)  # noqa: E731
+    lib.ref_ranks_run(nprx, nprz, mx, my, mz, *[p(a) for a in arrs], eta, di, hall, cfl, warm, steps,
+                      p(out) if want_state else None, p(sec), p(dts))
+    return float(sec[0]), dts, out
 
 
 class RefProgram:
