@@ -9,11 +9,17 @@ nst (T:185-199); then nst advances by nint, the restart file is written when mod
 and m2d and m3d always.  The loop ends after nstop steps or when nst reaches nend.  A restart
 (lrstrt) reads the restart file of nst and writes m2d and m3d before the loop (T:124-129).
 
+Beside the reference's files, `Outputs` keeps a JSON-lines run log, run.jsonl: one object per
+diagn call (every 10 steps, the state after the step) with nstep, time, dt and the FP64
+diagnostics of dasha_diagnostics -- mass, energy, reconnected flux, the mid-y-plane current
+extrema -- and one closing object with the reason the loop ended.
+
     python -m dasha_b200.run --config c0 --out run_c0 --nend 3 --dtime 0.5
 """
 from __future__ import annotations
 
 import argparse
+import json
 import os
 from dataclasses import dataclass, field
 
@@ -56,6 +62,10 @@ class Outputs:
         self.dtlog_path = os.path.join(out_dir, "fort.20")
         if os.path.exists(self.dtlog_path):       # unit 20 starts a new file with the run
             os.remove(self.dtlog_path)
+        self.runlog_path = os.path.join(out_dir, "run.jsonl")
+        if os.path.exists(self.runlog_path):
+            os.remove(self.runlog_path)
+        self.last_diag = None
 
     def readin(self, nst: int):
         return restart.restore(self.d, self.dir, nst)
@@ -71,9 +81,19 @@ class Outputs:
         restart.write_m3d_ctx(self.d, os.path.join(self.data, f"m3d{restart.cn(nst)}"), time)
 
     def diagn(self, time: float):
-        restart.write_current_dat(os.path.join(self.dir, "current.dat"), self.d.diagnostics(), time,
+        self.last_diag = self.d.diagnostics()
+        restart.write_current_dat(os.path.join(self.dir, "current.dat"), self.last_diag, time,
                                   append=not self.first_diagn)
         self.first_diagn = False
+
+    def runlog(self, **entry):
+        """One JSON line of run.jsonl; after a diagn call it carries that call's diagnostics."""
+        if self.last_diag is not None and "reason" not in entry:
+            names = ("mass", "energy", "flux", "jx_max", "jx_min", "jy_max", "jy_min", "jz_max", "jz_min")
+            entry.update({k: float(v) for k, v in zip(names, self.last_diag)})
+            self.last_diag = None
+        with open(self.runlog_path, "a") as f:
+            f.write(json.dumps(entry) + "\n")
 
     def step_begin(self, nstep: int, time: float, dt: float):
         lib = capi.load()
@@ -112,6 +132,8 @@ def main_loop(d, ctl: RunControl, out, time: float = 0.0, nstep: int = 0, log=No
         d.stepon(time, dt, nstep)
         if nstep % 10 == 0:
             out.diagn(time)
+            if hasattr(out, "runlog"):
+                out.runlog(nstep=nstep, time=time + dt, dt=dt)
         nstep += 1
         time += dt
         out.step_end(dt, time, nstep)
@@ -131,6 +153,8 @@ def main_loop(d, ctl: RunControl, out, time: float = 0.0, nstep: int = 0, log=No
             res.reason = "nend"
             break
     res.nstep, res.time, res.nst = nstep, time, nst
+    if hasattr(out, "runlog"):
+        out.runlog(reason=res.reason, nstep=nstep, time=time, nst=nst)
     return res
 
 

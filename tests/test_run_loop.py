@@ -41,8 +41,8 @@ class Recorder:
         self.log = []
 
     def __getattr__(self, name):
-        def rec(*a):
-            self.log.append((name,) + a)
+        def rec(*a, **kw):
+            self.log.append((name,) + a + ((kw,) if kw else ()))
             return (1, 40, 10.0, 5) if name == "readin" else None
         return rec
 
@@ -146,6 +146,15 @@ def test_outputs_files(tmp_path):
     assert (tmp_path / "fort.20").read_text() == "".join(fio.dtlog_line(0.25, 0.25 * n, n) for n in range(1, 16))
     m2d = (data / "m2d003.dat").read_text()
     assert m2d == fio.m2d_text(1.75, d.x, d.z, np.ones((8, d.mz, 1, d.mx)), np.ones((3, d.mz, 1, d.mx)))
+    # run.jsonl: the diagnostics after steps 0 and 10 (the diagn steps), then the end of the run
+    import json
+    log = [json.loads(line) for line in (tmp_path / "run.jsonl").read_text().splitlines()]
+    assert [e.get("nstep") for e in log] == [0, 10, 15]
+    assert log[0]["time"] == 0.25 and log[0]["dt"] == 0.25 and log[1]["time"] == 2.75
+    for e in log[:2]:
+        assert [e[k] for k in ("mass", "energy", "flux", "jx_max", "jx_min", "jy_max", "jy_min", "jz_max",
+                               "jz_min")] == list(diag)
+    assert log[2] == {"reason": "nend", "nstep": 15, "time": 3.75, "nst": 5}
     # a second run in the same directory starts fort.20 and current.dat over, appends stepnm
     d2 = FakeBound()
     run.main_loop(d2, run.RunControl(nend=2, dtime=1.0, dnstep=3), run.Outputs(d2, str(tmp_path)))
