@@ -246,6 +246,21 @@ int dasha_get_state(dasha_ctx* c, double* x_f, long ld1, long ld2) {
 // z-plane chunks: record 2 is x(mx+4, my, mz+4, 8) in the reference's order, so each field is
 // 2 planes of zero z halo, the mz planes of the chunks (each row with the periodic x halo
 // copies that message4 leaves at a 1x1 process grid) and 2 more zero planes.
+// The exact-resume record beside a restart file, <path>.state: the device state as stored, so
+// that a run restored from it continues bit for bit (the reference's file holds FP64 totals,
+// from which neither the FP64 perturbation split nor the FP32 pair (x, Kahan compensation) can
+// be recovered exactly).  48-byte header: "DASHAST1", int32 precision, mx, my, mz, nfields,
+// ncase, nstep, nst, double time; then nfields x mx*my*mz values of the context's type, node
+// (i, j, k) at i + mx (j + my k), the 8 perturbation fields (rho - rho0, rho v, B - B0, p - p0)
+// and in FP32 their 8 compensations.
+static std::string state_record_path(const char* path) { return std::string(path) + ".state"; }
+static void pack_state_header(unsigned char* h, const dasha_ctx* c, int nf, int ncase, int nstep, int nst, double time) {
+    const int32_t v[8] = {c->P.precision, c->mx, c->my, c->mz, nf, ncase, nstep, nst};
+    std::memcpy(h, "DASHAST1", 8);
+    std::memcpy(h + 8, v, sizeof(v));
+    std::memcpy(h + 40, &time, sizeof(double));
+}
+
 int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, double time, int nst,
                      long max_subrecord) {
     CAPI_GUARD(c);
@@ -280,6 +295,19 @@ int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, doubl
         if (rc != DASHA_OK) return rc;
         const bool ok = w.finish();
         if (!f.close() || !ok) return fail(c, DASHA_E_INVALID, std::string("writing ") + path + " failed");
+        // the exact-resume record
+        const std::string sp = state_record_path(path);
+        File g(sp.c_str(), "wb");
+        if (!g.f) return fail(c, DASHA_E_INVALID, "cannot open " + sp);
+        unsigned char h[48];
+        pack_state_header(h, c, c->eng->raw_fields(), ncase, nstep, nst, time);
+        bool gok = std::fwrite(h, 1, 48, g.f) == 48;
+        const int rc3 = from_status(c, c->eng->raw_out([&](const void* p, size_t n) {
+            gok = gok && std::fwrite(p, 1, n, g.f) == n;
+            return gok;
+        }));
+        if (rc3 != DASHA_OK) return rc3;
+        if (!g.close() || !gok) return fail(c, DASHA_E_INVALID, "writing " + sp + " failed");
         return DASHA_OK;
     });
 }
@@ -300,6 +328,23 @@ int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double
         // the markers of record 2 are checked before the device state is touched
         if (!r1.finish() || !scan_record(f.f, total))
             return fail(c, DASHA_E_INVALID, std::string(path) + " is not a restart file of this grid");
+        // an exact-resume record beside the file must belong to it: checked before the state
+        // is touched
+        int h_ncase, h_nstep, h_nst;
+        double h_time;
+        unpack_restart_header(hdr, &h_ncase, &h_nstep, &h_time, &h_nst);
+        const std::string sp = state_record_path(path);
+        File g(sp.c_str(), "rb");
+        const size_t raw_bytes = c->eng->raw_elem() * (size_t)c->eng->raw_fields() * (size_t)mx * my * mz;
+        if (g.f) {
+            unsigned char h[48], want[48];
+            pack_state_header(want, c, c->eng->raw_fields(), h_ncase, h_nstep, h_nst, h_time);
+            std::fseek(g.f, 0, SEEK_END);
+            const long len = std::ftell(g.f);
+            std::fseek(g.f, 0, SEEK_SET);
+            if (std::fread(h, 1, 48, g.f) != 48 || std::memcmp(h, want, 48) != 0 || len != (long)(48 + raw_bytes))
+                return fail(c, DASHA_E_INVALID, sp + " does not belong to " + path + " and this context");
+        }
         RecReader r(f.f, total);
         std::vector<double> rb(row), skip(row);
         auto zplanes = [&]() { for (long q = 0; q < 2L * my && r.ok; ++q) r.get(skip.data(), (long)sizeof(double) * row); };
@@ -315,6 +360,14 @@ int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double
         }));
         if (rc2 != DASHA_OK) return rc2;
         if (!r.finish()) return fail(c, DASHA_E_INVALID, std::string("reading ") + path + " failed");
+        if (g.f) {   // the state exactly as it was stored
+            bool gok = true;
+            const int rc3 = from_status(c, c->eng->raw_in([&](void* p, size_t n) {
+                gok = gok && std::fread(p, 1, n, g.f) == n;
+                return gok;
+            }));
+            if (rc3 != DASHA_OK) return rc3;
+        }
         unpack_restart_header(hdr, ncase, nstep, time, nst);
         return DASHA_OK;
     });

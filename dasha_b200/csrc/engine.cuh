@@ -88,6 +88,14 @@ struct EngineBase {
     virtual Status state_in(const ChunkIn& fill) = 0;
     virtual Status state_out(const ChunkOut& take) = 0;
     virtual Status current_out(const ChunkOut& take) = 0;
+    // The device state as stored (the perturbation fields, and in FP32 their Kahan
+    // compensations after them), raw bytes in node order, in pieces of at most 64 MB: out hands
+    // each piece to `take`, in fills each piece from `give` and replaces the state only whole
+    // (the fields arrive in a spare buffer first).
+    virtual int raw_fields() const = 0;
+    virtual size_t raw_elem() const = 0;
+    virtual Status raw_out(const std::function<bool(const void*, size_t)>& take) = 0;
+    virtual Status raw_in(const std::function<bool(void*, size_t)>& give) = 0;
     virtual Status setdt(double* dt, int* blowup) = 0;
     virtual Status stepon(double time, double dt, int nstep) = 0;
     virtual Status current(double* cur, long ld1, long ld2) = 0;
@@ -509,6 +517,47 @@ public:
         return Status::ok();
     }
     Status state_out(const ChunkOut& take) override { return stream_out(X, 8, true, KAHAN ? C : nullptr, take); }
+
+    int raw_fields() const override { return KAHAN ? 16 : 8; }
+    size_t raw_elem() const override { return sizeof(T); }
+    Status raw_out(const std::function<bool(const void*, size_t)>& take) override {
+        Status s = xbuf();
+        if (s.code) return s;
+        const size_t cap = sizeof(double) * (size_t)mx * my * xnk, total = sizeof(T) * (size_t)N;
+        for (int f = 0; f < raw_fields(); ++f) {
+            const char* src = reinterpret_cast<const char*>(f < 8 ? X[f] : C[f - 8]);
+            for (size_t o = 0; o < total; o += cap) {
+                const size_t n = std::min(cap, total - o);
+                DASHA_CK(cudaMemcpyAsync(xh[0], src + o, n, cudaMemcpyDeviceToHost, st));
+                DASHA_CK(cudaStreamSynchronize(st));
+                if (!take(xh[0], n)) return Status::err(DASHA_E_INVALID, "the host side of the transfer failed");
+            }
+        }
+        return Status::ok();
+    }
+    Status raw_in(const std::function<bool(void*, size_t)>& give) override {
+        Status s = xbuf();
+        if (s.code) return s;
+        const size_t cap = sizeof(double) * (size_t)mx * my * xnk, total = sizeof(T) * (size_t)N;
+        // into S (and A for the FP32 compensations), spare between steps, then swapped in
+        for (int f = 0; f < raw_fields(); ++f) {
+            char* dst = reinterpret_cast<char*>(f < 8 ? S[f] : A[f - 8]);
+            for (size_t o = 0; o < total; o += cap) {
+                const size_t n = std::min(cap, total - o);
+                if (!give(xh[0], n)) return Status::err(DASHA_E_INVALID, "the host side of the transfer failed");
+                DASHA_CK(cudaMemcpyAsync(dst + o, xh[0], n, cudaMemcpyHostToDevice, st));
+                DASHA_CK(cudaStreamSynchronize(st));
+            }
+        }
+        for (int m = 0; m < 8; ++m) {
+            std::swap(X[m], S[m]);
+            if (KAHAN) std::swap(C[m], A[m]);
+        }
+        DASHA_CK(cudaMemsetAsync(flag, 0, sizeof(int), st));
+        DASHA_CK(cudaStreamSynchronize(st));
+        rate_ok = false;
+        return Status::ok();
+    }
     Status set_state(const double* x, long ld1, long ld2) override { return state_in(gather(x, ld1, ld2)); }
     Status get_state(double* x, long ld1, long ld2) override { return state_out(scatter(x, ld1, ld2)); }
 

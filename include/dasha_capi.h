@@ -103,7 +103,15 @@ int dasha_get_state(dasha_ctx* ctx, double* x_f, long ld1, long ld2);
  * dasha_restore checks the file's records against the grid before it replaces the state
  * (a mismatch returns DASHA_E_INVALID with the state unchanged); it needs the equilibrium set
  * and acts as dasha_set_state of the file's interior nodes.  An I/O error during the read
- * leaves the context without a state (DASHA_E_STATE until the next set_state or restore). */
+ * leaves the context without a state (DASHA_E_STATE until the next set_state or restore).
+ * Exact resume (no counterpart in the reference): the file holds FP64 totals, from which the
+ * context's stored state (the perturbation from the equilibrium; in FP32 also its Kahan
+ * compensation) can be recovered only to one rounding, so dasha_checkpoint also writes
+ * <path>.state, that stored state as it is (a 48-byte header "DASHAST1", int32 precision, mx,
+ * my, mz, field count, ncase, nstep, nst, double time; then the fields, node i + mx (j + my k)),
+ * and dasha_restore, when <path>.state exists, checks that it belongs to the file and the
+ * context (else DASHA_E_INVALID with the state unchanged) and takes the state from it: a run
+ * restored that way continues bit for bit.  Without <path>.state the file alone is read. */
 int dasha_checkpoint(dasha_ctx* ctx, const char* path, int ncase, int nstep, double time, int nst,
                      long max_subrecord);
 int dasha_restore(dasha_ctx* ctx, const char* path, int* ncase, int* nstep, double* time, int* nst);

@@ -2,6 +2,8 @@
 on the device equal the host gather from dasha_get_state and dasha_current bit for bit (the
 same FP64 operations on the same values), the m2d file made from them equals the oracle's
 text, and a run restored from its restart file continues as the uninterrupted run does."""
+import os
+
 import numpy as np
 import pytest
 
@@ -39,29 +41,53 @@ def test_m2d_from_device_plane(tmp_path):
     d.close()
 
 
-@pytest.mark.parametrize("precision,tol", [(0, 1e-13), (1, 1e-6)], ids=["fp64", "fp32"])
-def test_restart_continues_the_run(tmp_path, precision, tol):
-    """Checkpoint after 2 steps, restore into a fresh context, 2 more steps on both.  The file
-    holds FP64 totals; a context stores x - eq, so the restored state may differ from the live
-    one by the rounding of that subtraction (FP64) or by the compensation term that the file
-    does not carry (FP32)."""
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_restart_continues_the_run_bit_for_bit(tmp_path, precision):
+    """k steps, checkpoint, restore into a fresh context, k more steps == 2k steps, bit for bit
+    (survey §5): the restart file holds FP64 totals, from which neither the FP64 perturbation
+    split nor the FP32 Kahan pair can be recovered exactly, so the checkpoint also writes the
+    exact-resume record <file>.state, which the restore takes when it belongs to the file."""
     a = capi.gem_context(SMALL, precision)
     t, _ = a.run(2)
     path = restart.checkpoint(a, str(tmp_path), ncase=1, nstep=2, time=t, nst=3)
-    assert path.endswith("mhd003000")
+    assert path.endswith("mhd003000") and os.path.exists(path + ".state")
     b = capi.gem_context(SMALL, precision)
+    b.run(1)                                                   # another state before the restore
     ncase, nstep, tb, nst = restart.restore(b, str(tmp_path), 3)
     assert (ncase, nstep, tb, nst) == (1, 2, t, 3)
-    xa, xb = a.get_state(), b.get_state()
-    scale = np.abs(xa).reshape(8, -1).max(axis=1)
-    rt = np.abs(xa - xb).reshape(8, -1).max(axis=1) / scale
-    assert rt.max() < (1e-15 if precision == 0 else 1e-7), rt   # one FP64 / FP32 rounding
+    assert np.array_equal(a.get_state(), b.get_state())
     ta, _ = a.run(2, t, 2)
     tb2, _ = b.run(2, tb, 2)
-    assert abs(ta - tb2) <= 1e-12 * ta
-    xa, xb = a.get_state(), b.get_state()
-    err = np.abs(xa - xb).reshape(8, -1).max(axis=1) / scale
-    assert err.max() < tol, err
+    assert ta == tb2
+    assert np.array_equal(a.get_state(), b.get_state())
+    # without the record the file alone restores the state to one rounding (FP64) or to the
+    # compensation the file does not carry (FP32)
+    os.remove(path + ".state")
+    c = capi.gem_context(SMALL, precision)
+    restart.restore(c, str(tmp_path), 3)
+    a2 = capi.gem_context(SMALL, precision)
+    a2.run(2)
+    xa, xc = a2.get_state(), c.get_state()
+    scale = np.abs(xa).reshape(8, -1).max(axis=1)
+    rt = np.abs(xa - xc).reshape(8, -1).max(axis=1) / scale
+    assert rt.max() < (1e-15 if precision == 0 else 1e-7), rt
+    for x in (a, b, c, a2):
+        x.close()
+
+
+def test_restore_rejects_a_state_record_of_another_checkpoint(tmp_path):
+    a = capi.gem_context(SMALL, 1)
+    t, _ = a.run(1)
+    p1 = restart.checkpoint(a, str(tmp_path), 1, 1, t, 1)
+    t2, _ = a.run(1, t, 1)
+    p2 = restart.checkpoint(a, str(tmp_path), 1, 2, t2, 2)
+    os.replace(p2 + ".state", p1 + ".state")                    # step 2's record beside step 1's file
+    b = capi.gem_context(SMALL, 1)
+    before = b.get_state()
+    with pytest.raises(capi.DashaError) as e:
+        restart.restore(b, str(tmp_path), 1)
+    assert e.value.code == capi.E_INVALID
+    assert np.array_equal(b.get_state(), before)
     a.close()
     b.close()
 
