@@ -92,18 +92,29 @@ CHUNK_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER
 _lib = None
 
 
+# the same library built with -DDASHA_BOUNDS: every global access of the z-marching kernels
+# checked against its field's extent (a violation is recorded and skipped, and the call returns
+# DASHA_E_CUDA naming the site and index); for tests, not for production runs
+BOUNDS_LIB_PATH = os.path.join(_HERE, "_lib", "libdasha_bounds.so")
+
+
+def bind(path: str):
+    """A library at `path` with the argument types of every symbol (not cached)."""
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with __graft_entry__.build()")
+    lib = C.CDLL(path)
+    for name, (args, res) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    return lib
+
+
 def load(path: str = LIB_PATH):
     """Load libdasha.so (raises if it has not been built)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(path):
-            raise RuntimeError(f"{path} is missing: build it with __graft_entry__.build()")
-        lib = C.CDLL(path)
-        for name, (args, res) in SIGNATURES.items():
-            fn = getattr(lib, name)
-            fn.argtypes = args
-            fn.restype = res
-        _lib = lib
+        _lib = bind(path)
     return _lib
 
 
@@ -124,8 +135,8 @@ def make_params(cfg: harris.RunConfig, precision: int = 0, **over) -> ParamsC:
 class Dasha:
     """One GPU context: the state of one run (COMMON blocks of the reference)."""
 
-    def __init__(self, x: np.ndarray, y: np.ndarray, z: np.ndarray, params: ParamsC):
-        self.lib = load()
+    def __init__(self, x: np.ndarray, y: np.ndarray, z: np.ndarray, params: ParamsC, lib=None):
+        self.lib = lib if lib is not None else load()
         self.x = np.ascontiguousarray(x, dtype=np.float64)
         self.y = np.ascontiguousarray(y, dtype=np.float64)
         self.z = np.ascontiguousarray(z, dtype=np.float64)
@@ -289,10 +300,11 @@ def current_noalloc(x, y, z, db_ptr: int, cur_ptr: int, stream: int = 0) -> int:
                                      C.c_void_p(stream) if stream else None)
 
 
-def gem_context(cfg: harris.RunConfig, precision: int = 0, seed_v: int = harris.SEED_V, **over) -> Dasha:
+def gem_context(cfg: harris.RunConfig, precision: int = 0, seed_v: int = harris.SEED_V, lib=None,
+                **over) -> Dasha:
     """Context with the Harris equilibrium and the seeded GEM state of `cfg` uploaded."""
     x, y, z = harris.make_grid(cfg.mx, cfg.my, cfg.mz, cfg.stretch)
-    d = Dasha(x, y, z, make_params(cfg, precision, **over))
+    d = Dasha(x, y, z, make_params(cfg, precision, **over), lib=lib)
     rho0, b0, p0, j0 = harris.harris_profiles(z)
     d.set_equilibrium(rho0, b0, p0)
     if d.params.j0_mode == 1:

@@ -84,10 +84,34 @@ static int from_status(dasha_ctx* c, const Status& s) {
 
 // Runs the body of an entry point: a host exception (allocation, thread start) becomes a
 // status, as no exception may cross the C-ABI.
+#ifdef DASHA_BOUNDS
+// the checking build: after every entry point, the first out-of-range access its kernels met
+static int bounds_status(dasha_ctx* c, int rc) {
+    static const char* names[BS_COUNT] = {"k_zpv ring load", "k_zpv node", "k_zpv wall row", "k_zpv2 ring load",
+                                          "k_zpv2 node", "k_zcurl ring load", "k_zcurl store", "k_zhydro ring load",
+                                          "k_zhydro node load", "k_zhydro store", "k_zeh ring load",
+                                          "k_zeh node load", "k_zeh store"};
+    if (!c || !c->st) return rc;
+    unsigned long long hit = 0;
+    if (cudaStreamSynchronize(c->st) != cudaSuccess ||
+        cudaMemcpyFromSymbol(&hit, g_bounds_hit, sizeof(hit)) != cudaSuccess)
+        return rc;
+    if (!hit) return rc;
+    const unsigned long long zero = 0;
+    cudaMemcpyToSymbol(g_bounds_hit, &zero, sizeof(zero));
+    const int site = (int)(hit >> 48) - 1;
+    const long idx = (long)(hit & 0xFFFFFFFFFFFFull);
+    return fail(c, DASHA_E_CUDA, std::string("bounds check: ") + (site >= 0 && site < BS_COUNT ? names[site] : "?") +
+                                     " at node index " + std::to_string(idx));
+}
+#else
+static int bounds_status(dasha_ctx*, int rc) { return rc; }
+#endif
+
 template <class F>
 static int host_call(dasha_ctx* c, F body) {
     try {
-        return body();
+        return bounds_status(c, body());
     } catch (const std::bad_alloc&) {
         return fail(c, DASHA_E_NOMEM, "host allocation failed");
     } catch (const std::exception& e) {

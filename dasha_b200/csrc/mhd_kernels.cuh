@@ -47,6 +47,27 @@ struct F3 { T* f[3]; };
 
 __device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
+// -DDASHA_BOUNDS (a checking build for tests): the z-marching kernels test every global node
+// span they load or store against the field extent n; the first violation of a launch is kept
+// in g_bounds_hit as (site + 1) << 48 | index, the access is skipped (no trap, no fault), and the
+// C-ABI call that launched it returns DASHA_E_CUDA naming the site and index.  In the normal
+// build DASHA_SPAN is `true` and costs nothing.
+enum BoundsSite {
+    BS_ZPV_LOAD, BS_ZPV_STORE, BS_ZPV_WALL_LOAD, BS_ZPV2_LOAD, BS_ZPV2_STORE, BS_ZCURL_LOAD, BS_ZCURL_STORE,
+    BS_ZHYDRO_LOAD, BS_ZHYDRO_NODE_LOAD, BS_ZHYDRO_STORE, BS_ZEH_LOAD, BS_ZEH_NODE_LOAD, BS_ZEH_STORE, BS_COUNT
+};
+#ifdef DASHA_BOUNDS
+static __device__ unsigned long long g_bounds_hit;
+__device__ __forceinline__ bool dasha_span(long first, long count, long n, int site) {
+    if (first >= 0 && first + count <= n) return true;
+    atomicCAS(&g_bounds_hit, 0ull, ((unsigned long long)(site + 1) << 48) | ((unsigned long long)first & 0xFFFFFFFFFFFFull));
+    return false;
+}
+#define DASHA_SPAN(first, count, n, site) dasha_span((long)(first), (long)(count), (long)(n), (int)(site))
+#else
+#define DASHA_SPAN(first, count, n, site) true
+#endif
+
 template <class T>
 __device__ __forceinline__ T d1fc(T fm2, T fm, T f0, T fp, T fp2, T a, T b, T c, T d) {
     return a * (fp - f0) + b * (f0 - fm) + c * (fp2 - f0) + d * (f0 - fm2);

@@ -79,6 +79,7 @@ __global__ void __launch_bounds__(32 * TY) k_zcurl(Geo<T> g, SrcFields<T, 3> src
             for (int q = 0; q < NSL; ++q) {
                 if (gsrc[q] >= 0) {
                     const long zo = gsrc[q] + (long)p * g.sz;
+                    if (!DASHA_SPAN(zo, svec[q] ? EPC : 1, g.sz * (long)g.mz, BS_ZCURL_LOAD)) continue;
 #pragma unroll
                     for (int f = 0; f < 3; ++f) {
                         if (svec[q]) cp_async16(stg + f * SP + sdst[q], src.f[f] + zo);
@@ -168,7 +169,8 @@ __global__ void __launch_bounds__(32 * TY) k_zcurl(Geo<T> g, SrcFields<T, 3> src
             }
             const long col = (long)gi + (long)gj * g.sy;
 #pragma unroll
-            for (int m = 0; m < 3; ++m) IO::st(out.f[m] + col + (long)c * g.sz, o[m]);
+            for (int m = 0; m < 3; ++m)
+                if (DASHA_SPAN(col + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZCURL_STORE)) IO::st(out.f[m] + col + (long)c * g.sz, o[m]);
             if (c == 2 || c == mz - 3) {
                 const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
 #pragma unroll

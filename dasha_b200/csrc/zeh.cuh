@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(32 * TY) k_zeh(Geo<T> g, EHIO<T> io, int chunk
             T* stg = ring + (size_t)(p % NS) * SP;
 #pragma unroll
             for (int q = 0; q < NSL; ++q) {
-                if (gsrc[q] >= 0) {
+                if (gsrc[q] >= 0 && DASHA_SPAN(gsrc[q] + (long)p * g.sz, svec[q] ? EPC : 1, g.sz * (long)g.mz, BS_ZEH_LOAD)) {
                     if (svec[q]) cp_async16(stg + sdst[q], io.dp + gsrc[q] + (long)p * g.sz);
                     else cp_async_elem(stg + sdst[q], io.dp + gsrc[q] + (long)p * g.sz);
                 }
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(32 * TY) k_zeh(Geo<T> g, EHIO<T> io, int chunk
                 h2[e] = (q3[e] * B1 - q1[e] * B3 - py) * dir;
                 h3[e] = (q1[e] * B2 - q2[e] * B1 - pz + dzr * dr[e]) * dir;
             }
-            IO::st(io.e[0] + n, e1); IO::st(io.e[1] + n, e2); IO::st(io.e[2] + n, e3);
+            if (DASHA_SPAN(n, VX, g.sz * (long)g.mz, BS_ZEH_STORE)) { IO::st(io.e[0] + n, e1); IO::st(io.e[1] + n, e2); IO::st(io.e[2] + n, e3); }
             IO::st(io.h[0] + n, h1); IO::st(io.h[1] + n, h2); IO::st(io.h[2] + n, h3);
             if (c == 2 || c == mz - 3) {
                 const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;

@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
             for (int q = 0; q < NSL; ++q) {
                 if (gsrc[q] >= 0) {
                     const long zo = gsrc[q] + (long)p * g.sz;
+                    if (!DASHA_SPAN(zo, svec[q] ? EPC : 1, g.sz * (long)g.mz, BS_ZHYDRO_LOAD)) continue;
 #pragma unroll
                     for (int f = 0; f < NF; ++f) {
                         if (svec[q]) cp_async16(stg + f * SP + sdst[q], srcf[f] + zo);
@@ -136,7 +137,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
         issue(c + 2 + D);
         // pointwise operands of plane c, loaded before the barrier
         T j1[VX], j2[VX], j3[VX], b1[VX], b2[VX], b3[VX];
-        if (xon && yon) {
+        if (xon && yon && DASHA_SPAN(col + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZHYDRO_NODE_LOAD)) {
             const long q = col + (long)c * g.sz;
             IO::ld(io.j1 + q, j1); IO::ld(io.j2 + q, j2); IO::ld(io.j3 + q, j3);
             IO::ld(io.b1 + q, b1); IO::ld(io.b2 + q, b2); IO::ld(io.b3 + q, b3);
@@ -270,7 +271,8 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
                           (g.gamma - T(1)) * g.eta * (j1[e] * j1[e] + j2[e] * j2[e] + j3[e] * j3[e]);
             }
 #pragma unroll
-            for (int m = 0; m < 5; ++m) IO::st(io.out[m] + col + (long)c * g.sz, o[m]);
+            for (int m = 0; m < 5; ++m)
+                if (DASHA_SPAN(col + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZHYDRO_STORE)) IO::st(io.out[m] + col + (long)c * g.sz, o[m]);
             if (c == 2 || c == mz - 3) {
                 const int kh = c == 2 ? 1 : mz - 2, kz = c == 2 ? 0 : mz - 1;
 #pragma unroll

@@ -263,6 +263,7 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
             for (int q = 0; q < NSL; ++q) {
                 if (gsrc[q] >= 0) {
                     const long zo = gsrc[q] + (long)p * g.sz;
+                    if (!DASHA_SPAN(zo, svec[q] ? EPC : 1, g.sz * (long)g.mz, BS_ZPV_LOAD)) continue;
 #pragma unroll
                     for (int f = 0; f < NF; ++f) {
                         if (svec[q]) cp_async16(stg + f * SP + sdst[q], src.f[f] + zo);
@@ -303,7 +304,8 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
         typename Epi::Pre pre[RY];
 #pragma unroll
         for (int u = 0; u < RY; ++u)
-            if (xon && gj[u] < g.my) epi.pre((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, pre[u]);
+            if (xon && gj[u] < g.my && DASHA_SPAN((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE))
+                epi.pre((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, pre[u]);
         cp_async_wait<D>();
         __syncthreads();
         const T* pc = ring + (long)(c % NS) * NF * SP;
@@ -370,8 +372,9 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
                         val[f][e] = coef * (txp * wpx[e] - txm * wmx[e] + typ * wpy[u] - tym * wmy[u] + tzp * wpz - tzm * wmz);
                     }
                 }
-                epi.store(col + (long)c * g.sz, val, pre[u]);
-                if (wall) {
+                if (DASHA_SPAN(col + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE)) epi.store(col + (long)c * g.sz, val, pre[u]);
+                if (wall && DASHA_SPAN(col + (long)kh * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_WALL_LOAD) &&
+                    DASHA_SPAN(col + (long)kz * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_WALL_LOAD)) {
                     // wall rows of the pass result (row kh = half of row c, row kz = 0) as
                     // increments of x - comp
                     T hv[NO][VX], zv[NO][VX];
@@ -418,10 +421,14 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
                     }
                 }
                 if constexpr (MODE == 2) {
-                    epi.store_rows(col + (long)c * g.sz, wall, col + (long)kh * g.sz, col + (long)kz * g.sz, val, pre[u]);
+                    if (DASHA_SPAN(col + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE) &&
+                        (!wall || (DASHA_SPAN(col + (long)kh * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE) &&
+                                   DASHA_SPAN(col + (long)kz * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE))))
+                        epi.store_rows(col + (long)c * g.sz, wall, col + (long)kh * g.sz, col + (long)kz * g.sz, val, pre[u]);
                 } else {
-                    epi.store(col + (long)c * g.sz, val, pre[u]);
-                    if (wall) {
+                    if (DASHA_SPAN(col + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE)) epi.store(col + (long)c * g.sz, val, pre[u]);
+                    if (wall && DASHA_SPAN(col + (long)kh * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE) &&
+                        DASHA_SPAN(col + (long)kz * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE)) {
                         T hv[NF][VX], zv[NF][VX];
 #pragma unroll
                         for (int f = 0; f < NF; ++f)

@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
             for (int q = 0; q < NSL; ++q) {
                 if (gsrc[q] >= 0) {
                     const long zo = gsrc[q] + (long)p * g.sz;
+                    if (!DASHA_SPAN(zo, svec[q] ? EPC : 1, g.sz * (long)g.mz, BS_ZPV2_LOAD)) continue;
 #pragma unroll
                     for (int f = 0; f < NF; ++f) {
                         if (svec[q]) cp_async16(stg + f * SPI + sdst[q], src.f[f] + zo);
@@ -148,7 +149,8 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
         const int q = p - 1;                          // second-pass plane of this step
         const bool out = trow && yon && xon && q >= oA && q <= oB;
         typename Epi::Pre pre;
-        if (out) epi.pre((long)gi + (long)gy * g.sy + (long)q * g.sz, pre);
+        if (out && DASHA_SPAN((long)gi + (long)gy * g.sy + (long)q * g.sz, VX, g.sz * (long)g.mz, BS_ZPV2_STORE))
+            epi.pre((long)gi + (long)gy * g.sy + (long)q * g.sz, pre);
         cp_async_wait<D>();
         __syncthreads();
         const T* pm = ring + (size_t)((p + NSI - 1) % NSI) * NF * SPI;
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
                 }
             }
             const long col = (long)gi + (long)gy * g.sy;
-            epi.store(col + (long)q * g.sz, val, pre);
+            if (DASHA_SPAN(col + (long)q * g.sz, VX, g.sz * (long)g.mz, BS_ZPV2_STORE)) epi.store(col + (long)q * g.sz, val, pre);
             if (q == 2) {
                 T hv[NF][VX], zv[NF][VX];
 #pragma unroll
@@ -279,7 +281,7 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
         if (trow && yon && xon) {
             typename Epi::Pre pre;
             const long col = (long)gi + (long)gy * g.sy;
-            epi.pre(col + (long)q * g.sz, pre);
+            if (DASHA_SPAN(col + (long)q * g.sz, VX, g.sz * (long)g.mz, BS_ZPV2_STORE)) epi.pre(col + (long)q * g.sz, pre);
             const T* l1q = lv1 + (size_t)(q % 3) * NF * SP1;
             const int m1 = r1 * RS + OFF + xl;
             const T zwp = g.wpz[q], zwm = g.wmz[q], zws = zwp + zwm, qz2 = g.zc[q] * g.zc[q];
@@ -304,7 +306,7 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
                     val[f][e] = fma(c, sn, a * v0);
                 }
             }
-            epi.store(col + (long)q * g.sz, val, pre);
+            if (DASHA_SPAN(col + (long)q * g.sz, VX, g.sz * (long)g.mz, BS_ZPV2_STORE)) epi.store(col + (long)q * g.sz, val, pre);
             T hv[NF][VX], zv[NF][VX];
 #pragma unroll
             for (int f = 0; f < NF; ++f)

@@ -1,0 +1,29 @@
+"""The checking build (libdasha_bounds.so, -DDASHA_BOUNDS): every global node span that the
+z-marching kernels load or store is tested against its field's extent; a violation is recorded
+and skipped (no trap, no fault) and the C-ABI call returns DASHA_E_CUDA naming the site.  The
+ragged 96x12x36 grid (x not a multiple of the 64-node FP32 tile, y not a multiple of the 8 or 4
+rows of a CTA, two z chunks) runs the current, a right-hand side and 4 steps in FP64 and FP32
+with no violation, and gives the normal build's results bit for bit."""
+import numpy as np
+import pytest
+
+from dasha_b200 import capi, harris
+
+pytestmark = pytest.mark.gpu
+
+RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 4, dt_whistler=1)
+
+
+@pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
+def test_ragged_grid_stays_in_bounds(precision):
+    lib = capi.bind(capi.BOUNDS_LIB_PATH)
+    out = []
+    for which in (lib, None):
+        d = capi.gem_context(RAGGED, precision, lib=which)
+        cur = d.current()
+        rhs = d.rhs(0.5)
+        t, _ = d.run(RAGGED.steps)
+        out.append((cur, rhs, d.get_state(), t, d.setdt(t)))
+        d.close()
+    for a, b in zip(out[0], out[1]):
+        assert np.array_equal(a, b)
