@@ -12,6 +12,8 @@
 #include "adjoint.cuh"
 #include "checkpoint_schedule.h"
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
+#include <cstdlib>
 #include <type_traits>
 #include <string>
 #include <vector>
@@ -112,14 +114,26 @@ EngineBase* make_engine_f32(int mx, int my, int mz, const dasha_params_c& p, cud
                             Status& s);
 
 // Launch with optional event bracketing; bytes = algorithmic bytes of the launch.
+// Every launch is also an NVTX range named by its tag (a no-op unless a tool such as nsys or
+// ncu --nvtx is attached), so a timeline or a capture filter sees the step's structure.
 #define DASHA_LAUNCH(tag, bytes, ...)                                                          \
     do {                                                                                       \
         int tg_ = -1;                                                                          \
         cudaEvent_t a_ = nullptr;                                                              \
+        nvtxRangePushA(tag);                                                                   \
         if (prof.on) { tg_ = prof.tag_of(tag, (double)(bytes)); a_ = prof.ev(); cudaEventRecord(a_, st); } \
         __VA_ARGS__;                                                                           \
         if (prof.on) { cudaEvent_t b_ = prof.ev(); cudaEventRecord(b_, st); prof.recs.push_back({tg_, a_, b_}); } \
+        nvtxRangePop();                                                                        \
     } while (0)
+
+// an NVTX range over a scope: the reference routine a group of launches stands for
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // host transfer chunks and equilibrium profile lookup (defined after Engine)
 template <class T>
@@ -820,6 +834,7 @@ public:
 
     // E_total and the raw RHS of state xs into K (wall rows applied)
     void launch_rhs_raw(T* const* xs) {
+        NvtxRange range("right");
         launch_current(xs);
         T** cother = curF == cur[0] ? cur[1] : cur[0];
         (void)cother;
@@ -898,6 +913,7 @@ public:
 
     Status stepon(double time, double dt, int nstep) override {
         (void)time;
+        NvtxRange range("stepon");
         // stages 1..4: base = X, stage state in S, accumulator in A; both xdif smoothing
         // passes run in one k_zpv2 launch per field pair that ends in the RK stage update.  When
         // the post-step filter runs, its last launch (fields B, p) also takes the CFL rate of the
@@ -961,6 +977,7 @@ public:
     }
 
     Status setdt(double* dt, int* blowup) override {
+        NvtxRange range("setdt");
         if (rate_ok) {   // the rate of this state was taken by the last stepon's final launch
             DASHA_CK(cudaMemcpyAsync(hpin + 12, rate_bits, sizeof(double), cudaMemcpyDeviceToHost, st));
             DASHA_CK(cudaMemcpyAsync(hpin + 13, flag, sizeof(int), cudaMemcpyDeviceToHost, st));
