@@ -48,6 +48,7 @@ SIGNATURES = {
     "dasha_create": ([C.POINTER(GridC), C.POINTER(ParamsC), C.POINTER(C.c_void_p)], C.c_int),
     "dasha_set_equilibrium": ([_P, _D, _D, _D], C.c_int),
     "dasha_set_equilibrium_current": ([_P, _D], C.c_int),
+    "dasha_set_equilibrium_3d": ([_P, _D, C.c_long, C.c_long], C.c_int),
     "dasha_set_state": ([_P, _D, C.c_long, C.c_long], C.c_int),
     "dasha_get_state": ([_P, _D, C.c_long, C.c_long], C.c_int),
     "dasha_setdt": ([_P, C.c_double, _D], C.c_int),
@@ -135,14 +136,17 @@ def make_params(cfg: harris.RunConfig, precision: int = 0, **over) -> ParamsC:
 class Dasha:
     """One GPU context: the state of one run (COMMON blocks of the reference)."""
 
-    def __init__(self, x: np.ndarray, y: np.ndarray, z: np.ndarray, params: ParamsC, lib=None):
+    def __init__(self, x: np.ndarray, y: np.ndarray, z: np.ndarray, params: ParamsC, lib=None,
+                 periodic=(1, 1, 0)):
+        """periodic (1, 1, 0): x and y wrap, z walls (the Harris configurations); (0, 0, 0): the
+        bounded configuration of the reference's dipole runs (FP64)."""
         self.lib = lib if lib is not None else load()
         self.x = np.ascontiguousarray(x, dtype=np.float64)
         self.y = np.ascontiguousarray(y, dtype=np.float64)
         self.z = np.ascontiguousarray(z, dtype=np.float64)
         self.mx, self.my, self.mz = self.x.size, self.y.size, self.z.size
         self.params = params
-        g = GridC(self.mx, self.my, self.mz, _dp(self.x), _dp(self.y), _dp(self.z), (C.c_int * 3)(1, 1, 0))
+        g = GridC(self.mx, self.my, self.mz, _dp(self.x), _dp(self.y), _dp(self.z), (C.c_int * 3)(*periodic))
         h = C.c_void_p()
         rc = self.lib.dasha_create(C.byref(g), C.byref(params), C.byref(h))
         if rc != OK:
@@ -177,6 +181,11 @@ class Dasha:
         b0 = np.ascontiguousarray(b0, np.float64).reshape(-1)
         p0 = np.ascontiguousarray(p0, np.float64)
         self._check(self.lib.dasha_set_equilibrium(self.h, _dp(rho0), _dp(b0), _dp(p0)))
+
+    def set_equilibrium_3d(self, E):
+        """E: compact (5, mz, my, mx) rho0, bx0, by0, bz0, p0 (bounded contexts)."""
+        H = harris.to_halo(np.ascontiguousarray(E, np.float64))
+        self._check(self.lib.dasha_set_equilibrium_3d(self.h, _dp(H), H.shape[3], H.shape[2]))
 
     def set_equilibrium_current(self, j0):
         j0 = np.ascontiguousarray(j0, np.float64).reshape(-1)

@@ -61,6 +61,7 @@ struct dasha_ctx {
     Axis ax, ay, az;
     EngineBase* eng = nullptr;
     bool eq_set = false, state_set = false;
+    bool bounded = false;     // periodic = {0,0,0}: the reference's bounded configuration
     double dt0 = 0.;
     bool have_dt0 = false;
 };
@@ -132,21 +133,24 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
     *out = nullptr;
     if (!grid || !params || !grid->x || !grid->y || !grid->z) return DASHA_E_INVALID;
     if (grid->mx < 5 || grid->my < 5 || grid->mz < 7) return DASHA_E_INVALID;
-    if (grid->mx % 32 != 0) return DASHA_E_UNSUPPORTED;   // the z-marching tiles are 32 nodes wide in x
-    if (!(grid->periodic[0] == 1 && grid->periodic[1] == 1 && grid->periodic[2] == 0)) return DASHA_E_UNSUPPORTED;
+    const bool bounded = grid->periodic[0] == 0 && grid->periodic[1] == 0 && grid->periodic[2] == 0;
+    if (!bounded && grid->mx % 32 != 0) return DASHA_E_UNSUPPORTED;   // the z-marching tiles are 32 nodes wide in x
+    if (!bounded && !(grid->periodic[0] == 1 && grid->periodic[1] == 1 && grid->periodic[2] == 0)) return DASHA_E_UNSUPPORTED;
     const dasha_params_c& p = *params;
     if (p.precision != 0 && p.precision != 1) return DASHA_E_INVALID;
-    if (p.total_e != 1 || p.rcr > 0.0) return DASHA_E_UNSUPPORTED;
+    if (p.total_e != 1 || (!bounded && p.rcr > 0.0)) return DASHA_E_UNSUPPORTED;
+    if (bounded && p.precision != 0) return DASHA_E_UNSUPPORTED;     // the bounded configuration is FP64
     if (p.j0_mode != 0 && p.j0_mode != 1) return DASHA_E_INVALID;
     if (!(p.gamma > 1.0) || !(p.cfl > 0.0) || p.filter_every < 0) return DASHA_E_INVALID;
     dasha_ctx* c = new (std::nothrow) dasha_ctx();
     if (!c) return DASHA_E_NOMEM;
     try {
         c->mx = grid->mx; c->my = grid->my; c->mz = grid->mz;
+        c->bounded = bounded;
         c->N = (long)c->mx * c->my * c->mz;
         c->P = p;
-        c->ax.n = c->mx; c->ax.periodic = true; c->ax.c.assign(grid->x, grid->x + c->mx);
-        c->ay.n = c->my; c->ay.periodic = true; c->ay.c.assign(grid->y, grid->y + c->my);
+        c->ax.n = c->mx; c->ax.periodic = !bounded; c->ax.c.assign(grid->x, grid->x + c->mx);
+        c->ay.n = c->my; c->ay.periodic = !bounded; c->ay.c.assign(grid->y, grid->y + c->my);
         c->az.n = c->mz; c->az.periodic = false; c->az.c.assign(grid->z, grid->z + c->mz);
         // a periodic axis continues with its first spacing across the wrap (t3dsdsc.f:278-283)
         c->ax.L = c->ax.c[c->mx - 1] - c->ax.c[0] + (c->ax.c[1] - c->ax.c[0]);
@@ -197,7 +201,8 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
         for (int i = 0; i < c->mx; ++i) H.cbx[i] = (1.0 / 32.0) * (1.0 - std::tanh((c->ax.c[i] + 3.0) / 8.0));
 
         Status s;
-        if (p.precision == 0) c->eng = make_engine_f64(c->mx, c->my, c->mz, p, c->st, H, s);
+        if (bounded) c->eng = make_engine_walls(c->mx, c->my, c->mz, p, c->st, grid->x, grid->y, grid->z, s);
+        else if (p.precision == 0) c->eng = make_engine_f64(c->mx, c->my, c->mz, p, c->st, H, s);
         else c->eng = make_engine_f32(c->mx, c->my, c->mz, p, c->st, H, s);
         if (s.code != DASHA_OK) {
             int code = s.code;
@@ -233,8 +238,18 @@ int dasha_set_equilibrium(dasha_ctx* c, const double* rho0, const double* b0, co
     try {
         int rc = from_status(c, c->eng->set_equilibrium(rho0, b0, p0, nullptr));
         if (rc == DASHA_OK) c->eq_set = true;
+        if (rc == DASHA_OK && c->bounded) c->state_set = true;    // the state initia leaves
         return rc;
     } catch (...) { return fail(c, DASHA_E_NOMEM, "host allocation failed"); }
+}
+
+int dasha_set_equilibrium_3d(dasha_ctx* c, const double* eq_f, long ld1, long ld2) {
+    CAPI_GUARD(c);
+    if (!eq_f || ld1 < c->mx + 4 || ld2 < c->my) return fail(c, DASHA_E_INVALID, "bad equilibrium arguments");
+    const int rc = engine_call(c, [&] { return c->eng->set_equilibrium_3d(eq_f, ld1, ld2); });
+    if (rc == DASHA_OK) c->eq_set = true;
+    if (rc == DASHA_OK && c->bounded) c->state_set = true;        // the state initia leaves
+    return rc;
 }
 
 int dasha_set_equilibrium_current(dasha_ctx* c, const double* j0) {

@@ -85,6 +85,10 @@ struct EngineBase {
     }
     virtual Status set_equilibrium(const double* rho0, const double* b0, const double* p0, const double* j0) = 0;
     virtual Status set_j0(const double* j0) = 0;
+    // a 3-D equilibrium (rho0, B0, p0 as 5 fields in the state layout): bounded contexts only
+    virtual Status set_equilibrium_3d(const double*, long, long) {
+        return Status::err(DASHA_E_UNSUPPORTED, "a 3-D equilibrium needs a bounded (periodic 0,0,0) context");
+    }
     virtual Status set_state(const double* x, long ld1, long ld2) = 0;
     virtual Status get_state(double* x, long ld1, long ld2) = 0;
     virtual Status state_in(const ChunkIn& fill) = 0;
@@ -112,6 +116,9 @@ EngineBase* make_engine_f64(int mx, int my, int mz, const dasha_params_c& p, cud
                             Status& s);
 EngineBase* make_engine_f32(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const HostTables& H,
                             Status& s);
+// the reference's bounded configuration (walls.cu): periodic = {0, 0, 0}, FP64
+EngineBase* make_engine_walls(int mx, int my, int mz, const dasha_params_c& p, cudaStream_t st, const double* x,
+                              const double* y, const double* z, Status& s);
 
 // Launch with optional event bracketing; bytes = algorithmic bytes of the launch.
 // Every launch is also an NVTX range named by its tag (a no-op unless a tool such as nsys or

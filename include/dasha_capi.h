@@ -37,9 +37,10 @@ typedef struct dasha_ctx dasha_ctx;
 enum {
     DASHA_OK = 0,
     DASHA_E_INVALID = 1,      /* bad argument (null pointer, size, leading dimension) */
-    DASHA_E_UNSUPPORTED = 2,  /* an option the library does not implement: mx not a multiple of 32,
-                                 periodicity other than {1,1,0}, total_e != 1, rcr > 0, or the
-                                 adjoint on an FP32 context */
+    DASHA_E_UNSUPPORTED = 2,  /* an option the library does not implement: periodicity other than
+                                 {1,1,0} or {0,0,0}, mx not a multiple of 32 or rcr > 0 on a periodic
+                                 context, FP32 on a bounded one, total_e != 1, the adjoint on an FP32
+                                 context, or a call a bounded context does not offer */
     DASHA_E_CUDA = 3,         /* a CUDA runtime error; the context should be destroyed */
     DASHA_E_NOMEM = 4,        /* the grid does not fit in device memory */
     DASHA_E_DT_COLLAPSE = 5,  /* dt < 0.1*dt0 or not finite: the guard of t3dsdsc.f:142-154 */
@@ -49,7 +50,18 @@ enum {
 };
 
 /* Grid: node coordinates (FP64, host, borrowed).  Replaces gridpntnew2 (t3dsdsc.f:4380-4690)
- * and the local slices of input (t3dsdsc.f:296-313).  periodic must be {1,1,0}. */
+ * and the local slices of input (t3dsdsc.f:296-313).  periodic:
+ *  {1,1,0}  the build's Harris configurations: x and y periodic (a true wrap), z walls; FP64 or
+ *           the FP32 perturbation form; the fast z-marching kernels;
+ *  {0,0,0}  the reference's own bounded configuration (periodx = periody = periodz = .false.,
+ *           mhd03.for), the dipole magnetosphere of initia: walls on all six sides with the rows
+ *           of bndry / bndrytt / bndryc / bndryh / bndryE, the time-dependent inflow driver on
+ *           the x-min rows (T:1710-1773), the inner-sphere mask r <= rcr, the radial Hall
+ *           coefficient 0.5 di (tanh((r-1.1)/8) - tanh((r-2)/10)) (T:1398; di is chall), setdt
+ *           over the cells with r >= 1 and a 3-D equilibrium (dasha_set_equilibrium_3d).  FP64
+ *           only; the post-step filter every step as in the reference; the streamed transfers,
+ *           exact-resume record, mid-plane, diagnostics and adjoint are not offered
+ *           (DASHA_E_UNSUPPORTED). */
 typedef struct {
     int mx, my, mz;
     const double *x, *y, *z;
@@ -60,7 +72,7 @@ typedef struct {
  *  gamma, cfl                      mhd03.for:60,71
  *  eta (etan = eta0), mu (fmu0), drho (frho0), dp (fpr0)   foreta/formu t3dsdsc.f:6489-6532
  *  di: Hall coefficient cht, uniform (replaces the radial profile of t3dsdsc.f:1398)
- *  rcr: inner-sphere mask radius (mhd03.for:26); only rcr <= 0 (no mask) is supported
+ *  rcr: inner-sphere mask radius (mhd03.for:26); on periodic contexts only rcr <= 0 (no mask)
  *  hall, viscos, diffu, total_e: mhd03.for:18-23 (total_e must be 1)
  *  j0_mode: 0 = LITERAL (J = curl(B-B0), the reference's equations), 1 = FULL (J0 added)
  *  filter_every: cadence of the post-step filter avrgtt (reference: every step = 1)
@@ -86,6 +98,17 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
  * Replaces the 3-D COMMON arrays rhoi, bxi, byi, bzi, pri (t3dsdsc.f:805-813) and computes
  * the residual xresd of the pure equilibrium (t3dsdsc.f:816-834). */
 int dasha_set_equilibrium(dasha_ctx* ctx, const double* rho0, const double* b0, const double* p0);
+
+/* A 3-D equilibrium: rho0, bx0, by0, bz0, p0 as 5 fields in the state layout (leading
+ * dimensions ld1 >= mx+4, ld2 >= my as in dasha_set_state), replacing the COMMON arrays rhoi,
+ * bxi, byi, bzi, pri that initia sets (t3dsdsc.f:805-813).  Bounded contexts only (periodic =
+ * {0,0,0}, below); it also computes xresd as initia does (T:828-834): the momentum rates of
+ * right(0, 1e-9, 1) with the state set to the equilibrium and eta = 0.  The state is then the
+ * one initia leaves, ready to step: the equilibrium at rest, with the rho, vx and p of the two
+ * x-min node rows as that right call's inflow driver wrote them; dasha_set_state replaces it.
+ * dasha_set_equilibrium on a bounded context broadcasts its z-profiles over x and y and does
+ * the same. */
+int dasha_set_equilibrium_3d(dasha_ctx* ctx, const double* eq_f, long ld1, long ld2);
 
 /* J0 = curl B0 as FP64 z-profiles [j0x|j0y|j0z] (3*mz), used when j0_mode = FULL.  Without
  * this call FULL mode takes J0 from the z-derivative of b0 with the 4th-order stencil. */

@@ -43,6 +43,11 @@ MPI_PROC_NULL = -2
 # interior band no boundary row reaches (160x144x33)
 PIN_GRIDS = [(64, 48, 33), (160, 144, 33)]
 
+# the bounded dipole configuration as the reference runs it (its own cht, mask, driver): a box
+# x in [-2.1, 5.65], y and z in [-2.5, 2.5] around the planet
+DIPOLE_GRID = (41, 25, 33)
+DIPOLE_BOX = ((-2.1, 5.65), (-2.5, 2.5), (-2.5, 2.5))
+
 # the benchmark's CPU leg: the 256x128x256 grid on these process grids (threads = ranks)
 BENCH_GRID = (256, 128, 256)
 BENCH_DECOMPS = [(8, 4), (4, 4), (4, 2), (2, 2), (2, 1), (1, 1)]
