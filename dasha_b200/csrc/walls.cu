@@ -41,11 +41,6 @@ struct GpuExec {
     }
 };
 
-// x**k as the reference's translation evaluates integer powers: repeated multiplication
-inline double p2(double a) { return a * a; }
-inline double p3(double a) { return a * a * a; }
-inline double p4(double a) { const double b = a * a; return b * b; }
-
 class WallEngine : public EngineBase {
 public:
     GpuExec ex{};
@@ -70,100 +65,29 @@ public:
                 const double* zc) {
         st = st_;
         ex.st = st_;
-        d.mx = mx; d.my = my; d.mz = mz; d.mxpr = mx + 4; d.mzpr = mz + 4;
-        d.sy = d.mxpr; d.sz = (long)d.mxpr * my; d.n = d.sz * d.mzpr;
-        d.x_first = 5; d.x_last = mx; d.z_first = 5; d.z_last = mz;          // t3dsdsc.f:60-81 at 1x1
-        d.xfirst = 3; d.xlast = mx + 2; d.zfirst = 3; d.zlast = mz + 2;
+        d = walls::make_dims(mx, my, mz);
         n = d.n;
         par.gamma = p.gamma; par.eta = p.eta; par.mu = p.viscos ? p.mu : 0.; par.drho = p.diffu ? p.drho : 0.;
         par.dp = p.diffu ? p.dp : 0.; par.cfl = p.cfl; par.rcr = p.rcr; par.chall = p.di;
         par.hall = p.hall; par.viscos = p.viscos; par.diffu = p.diffu;
-        // fields: x, xm, xfold, xdif (8 each), cur, efld, xdh, xresd (3 each), w fs gs hs u v,
-        // rhoi bxi byi bzi pri rr0 rr1
-        const size_t nf = 4 * 8 + 4 * 3 + 6 + 7;
-        DASHA_CK(cudaMalloc(&pool, sizeof(double) * n * nf + 256));
-        DASHA_CK(cudaMemsetAsync(pool, 0, sizeof(double) * n * nf + 256, st));
+        DASHA_CK(cudaMalloc(&pool, sizeof(double) * n * walls::NFIELDS + 256));
+        DASHA_CK(cudaMemsetAsync(pool, 0, sizeof(double) * n * walls::NFIELDS + 256, st));
+        DASHA_CK(cudaStreamSynchronize(st));          // the stream does not order with the copies below
         double* q = static_cast<double*>(pool);
-        auto take = [&](int k) { double* r = q; q += (size_t)k * n; return r; };
-        a.x = take(8); a.xm = take(8); a.xfold = take(8); a.xdif = take(8);
-        a.cur = take(3); a.efld = take(3); a.xdh = take(3); a.xresd = take(3);
-        a.w = take(1); a.fs = take(1); a.gs = take(1); a.hs = take(1); a.u = take(1); a.v = take(1);
-        a.rhoi = take(1); a.bxi = take(1); a.byi = take(1); a.bzi = take(1); a.pri = take(1);
-        a.rr0 = take(1); a.rr1 = take(1);
+        walls::carve(a, [&](int k) { double* r = q; q += (size_t)k * n; return r; });
         a.dtbits = reinterpret_cast<unsigned long long*>(q);
-
-        // 1-D tables on the padded index (entry 0 unused): coordinates, spacings, the 4th-order
-        // first / second derivative weights of input (t3dsdsc.f:336-504) on the interior, the
-        // one-sided weights axp, bxp, cxp (T:505-517)
-        const int L[3] = {d.mxpr + 1, my + 1, d.mzpr + 1};
-        std::vector<double> xx(L[0], 0.), yy(L[1], 0.), zz(L[2], 0.), dx(L[0], 0.), dy(L[1], 0.), dz(L[2], 0.);
-        auto fwd = [](const double* c, int nn, int i) { return i + 1 < nn ? c[i + 1] - c[i] : c[i] - c[i - 1]; };
-        for (int i = 0; i < mx; ++i) { xx[i + 3] = xc[i]; dx[i + 3] = fwd(xc, mx, i); }
-        for (int j = 0; j < my; ++j) { yy[j + 1] = yc[j]; dy[j + 1] = fwd(yc, my, j); }
-        for (int k = 0; k < mz; ++k) { zz[k + 3] = zc[k]; dz[k + 3] = fwd(zc, mz, k); }
-        std::vector<double> c1[3][4], c2[3][4], cp[3];
-        const std::vector<double>* crd[3] = {&xx, &yy, &zz};
-        const int lo[3] = {d.x_first, 3, d.z_first}, hi[3] = {d.x_last, my - 2, d.z_last};
-        for (int ax = 0; ax < 3; ++ax) {
-            for (int q2 = 0; q2 < 4; ++q2) { c1[ax][q2].assign(L[ax], 0.); c2[ax][q2].assign(L[ax], 0.); }
-            const std::vector<double>& c = *crd[ax];
-            for (int j = lo[ax]; j <= hi[ax]; ++j) {
-                const double dxp1 = c[j + 1] - c[j], dxm1 = c[j] - c[j - 1], dxp2 = c[j + 2] - c[j], dxm2 = c[j] - c[j - 2];
-                {   // second derivative (T:336-364)
-                    const double f1 = p2(dxp1) + dxp1 * dxm2, f2 = p3(dxp1) - dxp1 * p2(dxm2), f3 = p4(dxp1) + dxp1 * p3(dxm2);
-                    const double g1 = -p2(dxm1) + dxm1 * dxm2, g2 = p3(dxm1) - dxm1 * p2(dxm2), g3 = -p4(dxm1) + dxm1 * p3(dxm2);
-                    const double h1 = p2(dxp2) + dxp2 * dxm2, h2 = p3(dxp2) - dxp2 * p2(dxm2), h3 = p4(dxp2) + dxp2 * p3(dxm2);
-                    const double ca = (f1 * h3 - f3 * h1) * (g2 * h3 - g3 * h2) - (g1 * h3 - g3 * h1) * (f2 * h3 - f3 * h2);
-                    const double a2 = 2. * h3 * (g2 * h3 - g3 * h2) / ca, b2 = 2. * h3 * (h2 * f3 - h3 * f2) / ca;
-                    const double cc2 = 2. * h3 * (f2 * g3 - f3 * g2) / ca;
-                    c2[ax][0][j] = a2; c2[ax][1][j] = b2; c2[ax][2][j] = cc2;
-                    c2[ax][3][j] = -(dxp1 * a2 + dxm1 * b2 + dxp2 * cc2) / dxm2;
-                }
-                {   // first derivative (T:439-504)
-                    const double f1 = dxp1 + p4(dxp1) / p3(dxm2), f2 = p2(dxp1) - p4(dxp1) / p2(dxm2), f3 = p3(dxp1) + p4(dxp1) / dxm2;
-                    const double g1 = dxm1 - p4(dxm1) / p3(dxm2), g2 = -p2(dxm1) + p4(dxm1) / p2(dxm2), g3 = p3(dxm1) - p4(dxm1) / dxm2;
-                    const double h1 = dxp2 + p4(dxp2) / p3(dxm2), h2 = p2(dxp2) - p4(dxp2) / p2(dxm2), h3 = p3(dxp2) + p4(dxp2) / dxm2;
-                    const double ca = (f1 * h3 - f3 * h1) * (g2 * h3 - g3 * h2) - (g1 * h3 - g3 * h1) * (f2 * h3 - f3 * h2);
-                    const double a1 = h3 * (g2 * h3 - g3 * h2) / ca, b1 = h3 * (h2 * f3 - h3 * f2) / ca, cc1 = h3 * (f2 * g3 - f3 * g2) / ca;
-                    c1[ax][0][j] = a1; c1[ax][1][j] = b1; c1[ax][2][j] = cc1;
-                    c1[ax][3][j] = (p2(dxp1) * a1 - p2(dxm1) * b1 + p2(dxp2) * cc1) / p2(dxm2);
-                }
-            }
-        }
-        for (int q2 = 0; q2 < 3; ++q2) cp[q2].assign(L[0], 0.);
-        for (int j = d.xfirst; j <= d.xlast - 3; ++j) {   // one-sided weights toward +x (T:505-517)
-            const double dxp1 = xx[j + 1] - xx[j], dxp2 = xx[j + 2] - xx[j], dxp3 = xx[j + 3] - xx[j];
-            const double f1 = dxp1 - p3(dxp1) / p2(dxp3), f2 = p2(dxp1) - p3(dxp1) / dxp3;
-            const double g1 = dxp2 - p3(dxp2) / p2(dxp3), g2 = p2(dxp2) - p3(dxp2) / dxp3;
-            const double ca = f1 * g2 - f2 * g1;
-            cp[0][j] = g2 / ca;
-            cp[1][j] = -f2 / ca;
-            cp[2][j] = (1 - cp[0][j] * dxp1 - cp[1][j] * dxp2) / dxp3;
-        }
+        // the 1-D tables, concatenated in one device buffer
+        const std::vector<std::vector<double>> tabs = walls::make_tables(d, xc, yc, zc);
         std::vector<double> ht;
         std::vector<size_t> off;
-        auto add = [&](const std::vector<double>& v) { off.push_back(ht.size()); ht.insert(ht.end(), v.begin(), v.end()); };
-        add(xx); add(yy); add(zz); add(dx); add(dy); add(dz);
-        for (int ax = 0; ax < 3; ++ax) for (int q2 = 0; q2 < 4; ++q2) add(c1[ax][q2]);
-        for (int ax = 0; ax < 3; ++ax) for (int q2 = 0; q2 < 4; ++q2) add(c2[ax][q2]);
-        for (int q2 = 0; q2 < 3; ++q2) add(cp[q2]);
+        for (const auto& v : tabs) { off.push_back(ht.size()); ht.insert(ht.end(), v.begin(), v.end()); }
         DASHA_CK(cudaMalloc(&tab, sizeof(double) * ht.size()));
         DASHA_CK(cudaMemcpy(tab, ht.data(), sizeof(double) * ht.size(), cudaMemcpyHostToDevice));
-        int o = 0;
-        auto nx = [&]() { return tab + off[o++]; };
-        t.xx = nx(); t.yy = nx(); t.zz = nx(); t.dx = nx(); t.dy = nx(); t.dz = nx();
-        const double** d1[12] = {&t.ax1, &t.bx1, &t.cx1, &t.dx1, &t.ay1, &t.by1, &t.cy1, &t.dy1, &t.az1, &t.bz1, &t.cz1, &t.dz1};
-        const double** d2[12] = {&t.ax2, &t.bx2, &t.cx2, &t.dx2, &t.ay2, &t.by2, &t.cy2, &t.dy2, &t.az2, &t.bz2, &t.cz2, &t.dz2};
-        for (auto* q2 : d1) *q2 = nx();
-        for (auto* q2 : d2) *q2 = nx();
-        t.axp = nx(); t.bxp = nx(); t.cxp = nx();
-        // r of every physical node (initia, T:771-776): rr0 and rr1 (its centre at x = 0.0)
+        const double* tp[walls::NTAB];
+        for (int k = 0; k < walls::NTAB; ++k) tp[k] = tab + off[k];
+        walls::bind_tables(t, tp);
         {
-            std::vector<double> r(n, 0.);
-            for (int jz = 3; jz <= mz + 2; ++jz)
-                for (int jy = 1; jy <= my; ++jy)
-                    for (int jx = 3; jx <= mx + 2; ++jx)
-                        r[d.at(jx, jy, jz)] = std::sqrt(xx[jx] * xx[jx] + yy[jy] * yy[jy] + zz[jz] * zz[jz]);
+            const std::vector<double> r = walls::make_radius(d, tabs);
             DASHA_CK(cudaMemcpy(a.rr0, r.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
             DASHA_CK(cudaMemcpy(a.rr1, r.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
         }

@@ -18,6 +18,7 @@
 // float values they are.
 #pragma once
 #include <cmath>
+#include <vector>
 
 #if !defined(__CUDACC__)
 #define __host__
@@ -446,6 +447,125 @@ struct Core {
         });
     }
 };
+
+
+// ---- host set-up, shared by the device engine (walls.cu) and host builds of this core ----
+
+// index ranges of a 1x1 process grid (t3dsdsc.f:60-81)
+inline Dims make_dims(int mx, int my, int mz) {
+    Dims d{};
+    d.mx = mx; d.my = my; d.mz = mz; d.mxpr = mx + 4; d.mzpr = mz + 4;
+    d.sy = d.mxpr; d.sz = (long)d.mxpr * my; d.n = d.sz * d.mzpr;
+    d.x_first = 5; d.x_last = mx; d.z_first = 5; d.z_last = mz;
+    d.xfirst = 3; d.xlast = mx + 2; d.zfirst = 3; d.zlast = mz + 2;
+    return d;
+}
+
+// x**k as the reference's translation evaluates integer powers: repeated multiplication
+inline double ipow2(double a) { return a * a; }
+inline double ipow3(double a) { return a * a * a; }
+inline double ipow4(double a) { const double b = a * a; return b * b; }
+
+// The 1-D tables of input on the padded index (entry 0 unused), in the order of the members of
+// Tables: xx yy zz dx dy dz; the first-derivative weights a b c d of x, y, z (T:439-504); the
+// second-derivative weights (T:336-364); the one-sided weights axp bxp cxp toward +x
+// (T:505-517).  Spacings are forward differences, the last one repeated.
+constexpr int NTAB = 6 + 12 + 12 + 3;
+inline std::vector<std::vector<double>> make_tables(const Dims& d, const double* xc, const double* yc,
+                                                    const double* zc) {
+    const int mx = d.mx, my = d.my, mz = d.mz;
+    const int L[3] = {d.mxpr + 1, my + 1, d.mzpr + 1};
+    std::vector<double> xx(L[0], 0.), yy(L[1], 0.), zz(L[2], 0.), dx(L[0], 0.), dy(L[1], 0.), dz(L[2], 0.);
+    auto fwd = [](const double* c, int nn, int i) { return i + 1 < nn ? c[i + 1] - c[i] : c[i] - c[i - 1]; };
+    for (int i = 0; i < mx; ++i) { xx[i + 3] = xc[i]; dx[i + 3] = fwd(xc, mx, i); }
+    for (int j = 0; j < my; ++j) { yy[j + 1] = yc[j]; dy[j + 1] = fwd(yc, my, j); }
+    for (int k = 0; k < mz; ++k) { zz[k + 3] = zc[k]; dz[k + 3] = fwd(zc, mz, k); }
+    std::vector<double> c1[3][4], c2[3][4], cp[3];
+    const std::vector<double>* crd[3] = {&xx, &yy, &zz};
+    const int lo[3] = {d.x_first, 3, d.z_first}, hi[3] = {d.x_last, my - 2, d.z_last};
+    for (int ax = 0; ax < 3; ++ax) {
+        for (int q = 0; q < 4; ++q) { c1[ax][q].assign(L[ax], 0.); c2[ax][q].assign(L[ax], 0.); }
+        const std::vector<double>& c = *crd[ax];
+        for (int j = lo[ax]; j <= hi[ax]; ++j) {
+            const double dxp1 = c[j + 1] - c[j], dxm1 = c[j] - c[j - 1], dxp2 = c[j + 2] - c[j], dxm2 = c[j] - c[j - 2];
+            {   // second derivative (T:336-364)
+                const double f1 = ipow2(dxp1) + dxp1 * dxm2, f2 = ipow3(dxp1) - dxp1 * ipow2(dxm2),
+                             f3 = ipow4(dxp1) + dxp1 * ipow3(dxm2);
+                const double g1 = -ipow2(dxm1) + dxm1 * dxm2, g2 = ipow3(dxm1) - dxm1 * ipow2(dxm2),
+                             g3 = -ipow4(dxm1) + dxm1 * ipow3(dxm2);
+                const double h1 = ipow2(dxp2) + dxp2 * dxm2, h2 = ipow3(dxp2) - dxp2 * ipow2(dxm2),
+                             h3 = ipow4(dxp2) + dxp2 * ipow3(dxm2);
+                const double ca = (f1 * h3 - f3 * h1) * (g2 * h3 - g3 * h2) - (g1 * h3 - g3 * h1) * (f2 * h3 - f3 * h2);
+                const double a2 = 2. * h3 * (g2 * h3 - g3 * h2) / ca, b2 = 2. * h3 * (h2 * f3 - h3 * f2) / ca;
+                const double cc2 = 2. * h3 * (f2 * g3 - f3 * g2) / ca;
+                c2[ax][0][j] = a2; c2[ax][1][j] = b2; c2[ax][2][j] = cc2;
+                c2[ax][3][j] = -(dxp1 * a2 + dxm1 * b2 + dxp2 * cc2) / dxm2;
+            }
+            {   // first derivative (T:439-504)
+                const double f1 = dxp1 + ipow4(dxp1) / ipow3(dxm2), f2 = ipow2(dxp1) - ipow4(dxp1) / ipow2(dxm2),
+                             f3 = ipow3(dxp1) + ipow4(dxp1) / dxm2;
+                const double g1 = dxm1 - ipow4(dxm1) / ipow3(dxm2), g2 = -ipow2(dxm1) + ipow4(dxm1) / ipow2(dxm2),
+                             g3 = ipow3(dxm1) - ipow4(dxm1) / dxm2;
+                const double h1 = dxp2 + ipow4(dxp2) / ipow3(dxm2), h2 = ipow2(dxp2) - ipow4(dxp2) / ipow2(dxm2),
+                             h3 = ipow3(dxp2) + ipow4(dxp2) / dxm2;
+                const double ca = (f1 * h3 - f3 * h1) * (g2 * h3 - g3 * h2) - (g1 * h3 - g3 * h1) * (f2 * h3 - f3 * h2);
+                const double a1 = h3 * (g2 * h3 - g3 * h2) / ca, b1 = h3 * (h2 * f3 - h3 * f2) / ca,
+                             cc1 = h3 * (f2 * g3 - f3 * g2) / ca;
+                c1[ax][0][j] = a1; c1[ax][1][j] = b1; c1[ax][2][j] = cc1;
+                c1[ax][3][j] = (ipow2(dxp1) * a1 - ipow2(dxm1) * b1 + ipow2(dxp2) * cc1) / ipow2(dxm2);
+            }
+        }
+    }
+    for (int q = 0; q < 3; ++q) cp[q].assign(L[0], 0.);
+    for (int j = d.xfirst; j <= d.xlast - 3; ++j) {
+        const double dxp1 = xx[j + 1] - xx[j], dxp2 = xx[j + 2] - xx[j], dxp3 = xx[j + 3] - xx[j];
+        const double f1 = dxp1 - ipow3(dxp1) / ipow2(dxp3), f2 = ipow2(dxp1) - ipow3(dxp1) / dxp3;
+        const double g1 = dxp2 - ipow3(dxp2) / ipow2(dxp3), g2 = ipow2(dxp2) - ipow3(dxp2) / dxp3;
+        const double ca = f1 * g2 - f2 * g1;
+        cp[0][j] = g2 / ca;
+        cp[1][j] = -f2 / ca;
+        cp[2][j] = (1 - cp[0][j] * dxp1 - cp[1][j] * dxp2) / dxp3;
+    }
+    std::vector<std::vector<double>> out{xx, yy, zz, dx, dy, dz};
+    for (int ax = 0; ax < 3; ++ax) for (int q = 0; q < 4; ++q) out.push_back(c1[ax][q]);
+    for (int ax = 0; ax < 3; ++ax) for (int q = 0; q < 4; ++q) out.push_back(c2[ax][q]);
+    for (int q = 0; q < 3; ++q) out.push_back(cp[q]);
+    return out;
+}
+
+// Tables from NTAB pointers in the order of make_tables
+inline void bind_tables(Tables& t, const double* const* p) {
+    int o = 0;
+    t.xx = p[o++]; t.yy = p[o++]; t.zz = p[o++]; t.dx = p[o++]; t.dy = p[o++]; t.dz = p[o++];
+    const double** d1[12] = {&t.ax1, &t.bx1, &t.cx1, &t.dx1, &t.ay1, &t.by1, &t.cy1, &t.dy1, &t.az1, &t.bz1, &t.cz1, &t.dz1};
+    const double** d2[12] = {&t.ax2, &t.bx2, &t.cx2, &t.dx2, &t.ay2, &t.by2, &t.cy2, &t.dy2, &t.az2, &t.bz2, &t.cz2, &t.dz2};
+    for (auto* q : d1) *q = p[o++];
+    for (auto* q : d2) *q = p[o++];
+    t.axp = p[o++]; t.bxp = p[o++]; t.cxp = p[o++];
+}
+
+// r of every physical node, zero elsewhere (initia, T:771-776; rr0 and rr1 alike, the centre of
+// rr1 at x = 0.0); tab: the tables of make_tables
+inline std::vector<double> make_radius(const Dims& d, const std::vector<std::vector<double>>& tab) {
+    const std::vector<double>&xx = tab[0], &yy = tab[1], &zz = tab[2];
+    std::vector<double> r(d.n, 0.);
+    for (int jz = 3; jz <= d.mz + 2; ++jz)
+        for (int jy = 1; jy <= d.my; ++jy)
+            for (int jx = 3; jx <= d.mx + 2; ++jx)
+                r[d.at(jx, jy, jz)] = std::sqrt(xx[jx] * xx[jx] + yy[jy] * yy[jy] + zz[jz] * zz[jz]);
+    return r;
+}
+
+// Fields of one context, carved from consecutive blocks: take(k) returns k fields
+template <class Take>
+inline void carve(Arr& a, Take take) {
+    a.x = take(8); a.xm = take(8); a.xfold = take(8); a.xdif = take(8);
+    a.cur = take(3); a.efld = take(3); a.xdh = take(3); a.xresd = take(3);
+    a.w = take(1); a.fs = take(1); a.gs = take(1); a.hs = take(1); a.u = take(1); a.v = take(1);
+    a.rhoi = take(1); a.bxi = take(1); a.byi = take(1); a.bzi = take(1); a.pri = take(1);
+    a.rr0 = take(1); a.rr1 = take(1);
+}
+constexpr int NFIELDS = 4 * 8 + 4 * 3 + 6 + 7;   // fields carve takes
 
 }  // namespace walls
 }  // namespace dasha
