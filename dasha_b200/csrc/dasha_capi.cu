@@ -108,11 +108,26 @@ static int bounds_status(dasha_ctx* c, int rc) {
 #else
 static int bounds_status(dasha_ctx*, int rc) { return rc; }
 #endif
+#ifdef DASHA_ZHYDRO_TMA
+// the TMA build: a bounded mbarrier wait of k_zhydro that ran out (the kernel returned early)
+static int wait_status(dasha_ctx* c, int rc) {
+    if (!c || !c->st) return rc;
+    unsigned int hit = 0;
+    if (cudaStreamSynchronize(c->st) != cudaSuccess || cudaMemcpyFromSymbol(&hit, g_wait_timeout, sizeof(hit)) != cudaSuccess)
+        return rc;
+    if (!hit) return rc;
+    const unsigned int zero = 0;
+    cudaMemcpyToSymbol(g_wait_timeout, &zero, sizeof(zero));
+    return fail(c, DASHA_E_CUDA, "k_zhydro: a TMA ring wait ran out");
+}
+#else
+static int wait_status(dasha_ctx*, int rc) { return rc; }
+#endif
 
 template <class F>
 static int host_call(dasha_ctx* c, F body) {
     try {
-        return bounds_status(c, body());
+        return wait_status(c, bounds_status(c, body()));
     } catch (const std::bad_alloc&) {
         return fail(c, DASHA_E_NOMEM, "host allocation failed");
     } catch (const std::exception& e) {

@@ -134,6 +134,24 @@ EngineBase* make_engine_walls(int mx, int my, int mz, const dasha_params_c& p, c
         nvtxRangePop();                                                                        \
     } while (0)
 
+#ifdef DASHA_ZHYDRO_TMA
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+inline EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiledFn) nullptr;
+        return reinterpret_cast<EncodeTiledFn>(f);
+    }();
+    return fn;
+}
+#endif
+
 // an NVTX range over a scope: the reference routine a group of launches stands for
 struct NvtxRange {
     explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
@@ -699,6 +717,11 @@ public:
         if ((e = cudaFuncSetAttribute(k_zhydro<T, ZH_VX, ZH_TY, 1, ZH_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZHc::smem())))
             return e;
+#ifdef DASHA_ZHYDRO_TMA
+        if ((e = cudaFuncSetAttribute(k_zhydro_tma<T, ZH_VX, ZH_TY, 1, ZH_MINB>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZHc::smem_tma())))
+            return e;
+#endif
         if ((e = cudaFuncSetAttribute(k_zcurl<T, ZVX, 8, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZC3c::smem())))
             return e;
@@ -832,6 +855,26 @@ public:
     }
 
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
+    const char* launch_err = nullptr;   // a launch that could not be set up (reported by stepon)
+#ifdef DASHA_ZHYDRO_TMA
+    // the five ring fields of k_zhydro as tensor maps, boxes of one ring plane (RS x NR x 1)
+    bool hydro_maps(const HydroIO<T>& io, ZhMaps& m) {
+        EncodeTiledFn enc = encode_tiled();
+        if (!enc) return false;
+        const T* f[5] = {io.m1, io.m2, io.m3, io.dp, io.drho};
+        const cuuint64_t dims[3] = {(cuuint64_t)mx, (cuuint64_t)my, (cuuint64_t)mz};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(T), (cuuint64_t)g.sz * sizeof(T)};
+        const cuuint32_t box[3] = {(cuuint32_t)ZHc::RS, (cuuint32_t)ZHc::NR, 1u};
+        const cuuint32_t estr[3] = {1u, 1u, 1u};
+        const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        for (int q = 0; q < 5; ++q)
+            if (enc(&m.m[q], dt, 3u, const_cast<T*>(f[q]), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return false;
+        return true;
+    }
+#endif
     void launch_current(T* const* xs) {
         T* bb[3] = {xs[4], xs[5], xs[6]};
         zcurl<1>("k_curl", src3(bb), f3(cur[0]));
@@ -885,8 +928,15 @@ public:
             dim3 gh((mx + ZHc::TX - 1) / ZHc::TX, (my + ZH_TY - 1) / ZH_TY, 1);
             int chh = zchunk(gh.x * gh.y, 16);
             gh.z = (mz + chh - 1) / chh;
+#ifdef DASHA_ZHYDRO_TMA
+            ZhMaps maps;
+            if (!hydro_maps(hio, maps)) launch_err = "cuTensorMapEncodeTiled failed for the hydro ring";
+            DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
+                         (k_zhydro_tma<T, ZH_VX, ZH_TY, 1, ZH_MINB><<<gh, 32 * ZH_TY, ZHc::smem_tma(), st>>>(g, hio, chh, maps)));
+#else
             DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),
                          (k_zhydro<T, ZH_VX, ZH_TY, 1, ZH_MINB><<<gh, 32 * ZH_TY, ZHc::smem(), st>>>(g, hio, chh)));
+#endif
         } else {
         SrcFields<T, 5> sh;
         sh.f[0] = xs[0]; sh.f[1] = xs[1]; sh.f[2] = xs[2]; sh.f[3] = xs[3]; sh.f[4] = xs[7];
@@ -954,6 +1004,11 @@ public:
             if (s.code) return s;
         }
         DASHA_CK(cudaGetLastError());
+        if (launch_err) {
+            const char* e = launch_err;
+            launch_err = nullptr;
+            return Status::err(DASHA_E_CUDA, e);
+        }
         rate_ok = filt;
         return Status::ok();
     }

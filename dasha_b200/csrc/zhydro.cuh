@@ -8,13 +8,63 @@
 // copy landed turns rho - rho0 into 1/rho in place.  The five quantities of the own nodes for
 // planes c-2 .. c+2 stay in a register queue (the z stencil), so per plane a thread reads plane
 // c+2 of its nodes, the x neighbours beyond its pair and rows c+-1, c+-2.  Fluxes are formed at
-// each stencil node from (m, p - p0, 1/rho) there, as in the reference.  At step c the ring is
+// each stencil node from (m, p - p0, 1/rho) there, as in the reference (m_i m_d / rho as
+// m_i v_d with v_d = m_d / rho formed once per node).  At step c the ring is
 // read at planes c and c+2, and by threads one step behind at c-1 and c+1; the first step also
 // reads planes c-2 .. c+1 for the queue, so it holds planes c-2 .. c+2+D (hence D + 5 stages),
 // and ends with a second barrier.
+//
+// TMA (built with -DDASHA_ZHYDRO_TMA, for comparison): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1,
+// rows y0-2 .. y0+TY+1) lies inside the grid loads each ring plane as 5 `cp.async.bulk.tensor`
+// boxes of exactly the ring plane's layout, issued by thread 0 against one mbarrier per stage;
+// every thread waits on the stage's mbarrier (time-bounded: after about a second the kernel
+// records g_wait_timeout, waits, again bounded, for the boxes it issued and returns) and turns
+// its share of the plane's rho - rho0 into 1/rho before the plane's barrier.  CTAs whose halo
+// wraps around x or y keep the cp.async element copies (a box cannot wrap).  The compute is the
+// same code in both builds.
 #pragma once
 
+#include <cuda.h>
+
 namespace dasha {
+
+// the five ring fields (m1 m2 m3 dp drho) as 3-D tensor maps with the box of one ring plane
+struct ZhMaps { CUtensorMap m[5]; };
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+#ifdef DASHA_ZHYDRO_TMA
+static __device__ unsigned int g_wait_timeout;    // a bounded mbarrier wait ran out
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// waits for phase `parity` of an mbarrier for at most about 2^31 clocks; false if it ran out
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > (1ll << 31)) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+#endif
 
 template <class T, int VX, int TY, int D>
 struct ZH {
@@ -28,6 +78,8 @@ struct ZH {
     static constexpr int NS = D + 5;
     static constexpr int CH = TX / EPC;
     static constexpr size_t smem() { return sizeof(T) * (size_t)NS * NF * SP; }
+    // the TMA build: the ring 128-byte aligned, then one mbarrier per stage
+    static constexpr size_t smem_tma() { return 128 + smem() + 8 * NS; }
 };
 
 // out: xdif 0 (rho), 1..3 (m), 4 (p); src: rho-rho0, m1, m2, m3, p-p0; pointwise J, B
@@ -38,8 +90,8 @@ struct HydroIO {
     T* out[5];
 };
 
-template <class T, int VX, int TY, int D, int MINB = 1>
-__global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> io, int chunk) {
+template <class T, int VX, int TY, int D, bool TMA>
+__device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& io, int chunk, const ZhMaps* maps) {
     using Z = ZH<T, VX, TY, D>;
     constexpr int TX = Z::TX, EPC = Z::EPC, OFF = Z::OFF, RS = Z::RS, NR = Z::NR, SP = Z::SP, NF = Z::NF,
                   NS = Z::NS, CH = Z::CH;
@@ -48,7 +100,9 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
     constexpr int NHAL = 4 * TY;                      // x-halo columns x0-2, x0-1, x0+wx, x0+wx+1 on the tile rows
     using IO = VIO<T, VX>;
     extern __shared__ __align__(16) unsigned char zh_smem_raw[];
-    T* ring = reinterpret_cast<T*>(zh_smem_raw);      // [NS][NF][SP]: m1 m2 m3 dp ri
+    unsigned char* sbase = zh_smem_raw;
+    if constexpr (TMA) sbase += (128 - (smem_addr(zh_smem_raw) & 127)) & 127;
+    T* ring = reinterpret_cast<T*>(sbase);            // [NS][NF][SP]: m1 m2 m3 dp ri
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int wx = min(TX, g.mx - x0);
@@ -57,6 +111,17 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
     const int k1 = min(k0 + chunk, mz);
     const int cA = max(k0, 2), cB = min(k1 - 1, mz - 3);
     if (cA > cB) return;
+    // a CTA whose ring box lies inside the grid loads it by TMA (the TMA build)
+    const bool tma = TMA && x0 >= OFF && x0 + TX + OFF <= g.mx && y0 >= 2 && y0 + TY + 2 <= g.my;
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(ring + (size_t)NS * NF * SP);
+#ifdef DASHA_ZHYDRO_TMA
+    if constexpr (TMA) {
+        if (tid == 0)
+            for (int q = 0; q < NS; ++q) mbar_init(bars + q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        __syncthreads();
+    }
+#endif
     const T* srcf[NF] = {io.m1, io.m2, io.m3, io.dp, io.drho};
     constexpr int NSL = (NVEC + NHAL + NT - 1) / NT;
     long gsrc[NSL];
@@ -83,6 +148,22 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
     }
     const int phi = cB + 2;
     auto issue = [&](int p) {
+#ifdef DASHA_ZHYDRO_TMA
+        if (tma) {
+            if (tid == 0 && p <= phi) {
+                T* stg = ring + (size_t)(p % NS) * NF * SP;
+                unsigned long long* bar = bars + p % NS;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after the stage's generic accesses
+                mbar_expect_tx(bar, (unsigned)(NF * SP * sizeof(T)));
+#pragma unroll
+                for (int f = 0; f < NF; ++f) tma_load_3d(stg + f * SP, &maps->m[f], x0 - OFF, y0 - 2, p, bar);
+            }
+            return;
+        }
+#else
+        (void)bars;
+        (void)maps;
+#endif
         if (p <= phi) {
             T* stg = ring + (size_t)(p % NS) * NF * SP;
 #pragma unroll
@@ -109,9 +190,9 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
             if (gsrc[q] >= 0) {
                 if (svec[q]) {
 #pragma unroll
-                    for (int e = 0; e < EPC; ++e) ri[sdst[q] + e] = T(1) / (r0 + ri[sdst[q] + e]);
+                    for (int e = 0; e < EPC; ++e) ri[sdst[q] + e] = recip(r0 + ri[sdst[q] + e]);
                 } else {
-                    ri[sdst[q]] = T(1) / (r0 + ri[sdst[q]]);
+                    ri[sdst[q]] = recip(r0 + ri[sdst[q]]);
                 }
             }
         }
@@ -143,12 +224,37 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
             IO::ld(io.b1 + q, b1); IO::ld(io.b2 + q, b2); IO::ld(io.b3 + q, b3);
         }
         const T az = g.a1z[c], bz = g.b1z[c], cz = g.c1z[c], dz = g.d1z[c];
-        cp_async_wait<D>();
-        if (!primed)
-            for (int p = c - 2; p <= c + 2; ++p) make_ri(p);
-        else
-            make_ri(c + 2);
-        __syncthreads();
+#ifdef DASHA_ZHYDRO_TMA
+        if (tma) {
+            // planes c-2 .. c+2 on the first step, then c+2: wait, then 1/rho over the plane
+            bool late = false;
+            for (int p = primed ? c + 2 : c - 2; p <= c + 2; ++p) {
+                if (!mbar_wait_bounded(bars + p % NS, (unsigned)(((p - (cA - 2)) / NS) & 1))) { late = true; break; }
+                const T r0 = T(g.rho0[p]);
+                T* ri = ring + (size_t)(p % NS) * NF * SP + 4 * SP;
+                for (int i = tid; i < SP; i += NT) ri[i] = recip(r0 + ri[i]);
+            }
+            // these generic writes precede the boxes that refill the stage later
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            if (__syncthreads_or(late)) {
+                // every box issued so far (planes up to c+2+D) lands before the CTA leaves
+                if (tid == 0) atomicExch(&g_wait_timeout, 1u);
+                for (int p = c - 2; p <= min(c + 2 + D, phi); ++p) {
+                    if (p < cA - 2) continue;
+                    mbar_wait_bounded(bars + p % NS, (unsigned)(((p - (cA - 2)) / NS) & 1));
+                }
+                return;
+            }
+        } else
+#endif
+        {
+            cp_async_wait<D>();
+            if (!primed)
+                for (int p = c - 2; p <= c + 2; ++p) make_ri(p);
+            else
+                make_ri(c + 2);
+            __syncthreads();
+        }
         const T* pc = ring + (size_t)(c % NS) * NF * SP;
         if (!primed) {
 #pragma unroll
@@ -178,27 +284,29 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
                     lo[f][0] = pc[f * SP + me - 2]; lo[f][1] = pc[f * SP + me - 1];
                     hi[f][0] = pc[f * SP + me + VX]; hi[f][1] = pc[f * SP + me + VX + 1];
                 }
+                // the six quantities at the VX + 4 x nodes -2 .. VX+1, each formed once for the
+                // VX stencils that share it
+                T q6[6][VX + 4];
+#pragma unroll
+                for (int k = -2; k < VX + 2; ++k) {
+                    T v[NF];
+#pragma unroll
+                    for (int f = 0; f < NF; ++f)
+                        v[f] = k < 0 ? lo[f][k + 2] : (k >= VX ? hi[f][k - VX] : zq[2][f][k < 0 ? 0 : (k >= VX ? VX - 1 : k)]);
+                    const T a = v[0] * v[4];                 // v1
+                    q6[0][k + 2] = v[0];
+                    q6[1][k + 2] = v[0] * a + v[3];
+                    q6[2][k + 2] = v[1] * a;
+                    q6[3][k + 2] = v[2] * a;
+                    q6[4][k + 2] = v[3];
+                    q6[5][k + 2] = a;
+                }
 #pragma unroll
                 for (int e = 0; e < VX; ++e) {
-                    T q6[6][5];   // quantity, offset -2..2
-#pragma unroll
-                    for (int s = -2; s <= 2; ++s) {
-                        const int k = e + s;
-                        T v[NF];
-#pragma unroll
-                        for (int f = 0; f < NF; ++f)
-                            v[f] = k < 0 ? lo[f][k + 2] : (k >= VX ? hi[f][k - VX] : zq[2][f][k < 0 ? 0 : (k >= VX ? VX - 1 : k)]);
-                        const T a = v[0] * v[4];
-                        q6[0][s + 2] = v[0];
-                        q6[1][s + 2] = v[0] * v[0] * v[4] + v[3];
-                        q6[2][s + 2] = v[0] * v[1] * v[4];
-                        q6[3][s + 2] = v[0] * v[2] * v[4];
-                        q6[4][s + 2] = v[3];
-                        q6[5][s + 2] = a;
-                    }
                     T dd[6];
 #pragma unroll
-                    for (int u = 0; u < 6; ++u) dd[u] = d1fc(q6[u][0], q6[u][1], q6[u][2], q6[u][3], q6[u][4], ax[e], bx[e], cx[e], dx[e]);
+                    for (int u = 0; u < 6; ++u)
+                        dd[u] = d1fc(q6[u][e], q6[u][e + 1], q6[u][e + 2], q6[u][e + 3], q6[u][e + 4], ax[e], bx[e], cx[e], dx[e]);
                     o[0][e] = -dd[0]; o[1][e] = -dd[1]; o[2][e] = -dd[2]; o[3][e] = -dd[3];
                     px[e] = dd[4]; dvv[e] = -dd[5];
                 }
@@ -220,11 +328,11 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
 #pragma unroll
                         for (int f = 0; f < NF; ++f)
                             v[f] = s < 2 ? ym[s][f][e] : (s == 2 ? zq[2][f][e] : yp[s - 3 < 0 ? 0 : s - 3][f][e]);
-                        const T b = v[1] * v[4];
+                        const T b = v[1] * v[4];                 // v2
                         q6[0][s] = v[1];
-                        q6[1][s] = v[0] * v[1] * v[4];
-                        q6[2][s] = v[1] * v[1] * v[4] + v[3];
-                        q6[3][s] = v[1] * v[2] * v[4];
+                        q6[1][s] = v[0] * b;
+                        q6[2][s] = v[1] * b + v[3];
+                        q6[3][s] = v[2] * b;
                         q6[4][s] = v[3];
                         q6[5][s] = b;
                     }
@@ -242,12 +350,13 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
 #pragma unroll
                 for (int s = 0; s < 5; ++s) {
                     const T m1 = zq[s][0][e], m2 = zq[s][1][e], m3 = zq[s][2][e], dp = zq[s][3][e], ri = zq[s][4][e];
+                    const T v3 = m3 * ri;
                     q6[0][s] = m3;
-                    q6[1][s] = m1 * m3 * ri;
-                    q6[2][s] = m2 * m3 * ri;
-                    q6[3][s] = m3 * m3 * ri + dp;
+                    q6[1][s] = m1 * v3;
+                    q6[2][s] = m2 * v3;
+                    q6[3][s] = m3 * v3 + dp;
                     q6[4][s] = dp;
-                    q6[5][s] = m3 * ri;
+                    q6[5][s] = v3;
                 }
                 T dd[6];
 #pragma unroll
@@ -294,5 +403,18 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
     }
     cp_async_wait<0>();
 }
+
+template <class T, int VX, int TY, int D, int MINB = 1>
+__global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> io, int chunk) {
+    zhydro_body<T, VX, TY, D, false>(g, io, chunk, nullptr);
+}
+
+#ifdef DASHA_ZHYDRO_TMA
+template <class T, int VX, int TY, int D, int MINB = 1>
+__global__ void __launch_bounds__(32 * TY, MINB) k_zhydro_tma(Geo<T> g, HydroIO<T> io, int chunk,
+                                                              const __grid_constant__ ZhMaps maps) {
+    zhydro_body<T, VX, TY, D, true>(g, io, chunk, &maps);
+}
+#endif
 
 }  // namespace dasha

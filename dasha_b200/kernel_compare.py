@@ -1,0 +1,91 @@
+"""Per-kernel times of the same RK4 steps under two builds of the library.
+
+    python -m dasha_b200.kernel_compare [--grid MX MY MZ] [--precision fp32|fp64] [--steps K]
+                                        [--warmup W] [--check-grid MX MY MZ]
+
+The builds: the default library and the one whose hydro right-hand side (k_zhydro) loads its
+shared-memory ring by TMA (`-DDASHA_ZHYDRO_TMA`, built by __graft_entry__.build() as
+libdasha_zhtma.so).  Each runs the bench's seeded Harris/GEM run (sinh z grid, d_i = 1, whistler
+CFL; 1024x512x1024 by default) for W untimed and K timed steps: the step time by CUDA events
+around the K steps, then the same K steps again with every launch bracketed by events for the
+time of each kernel tag.  The builds share the arithmetic, so their states must agree bit for
+bit: checked on a smaller grid (--check-grid) after 2 steps.  One JSON line on stdout.
+"""
+import argparse
+import dataclasses
+import json
+import os
+import sys
+
+import numpy as np
+
+from . import capi, harris
+
+BUILDS = {"default": capi.LIB_PATH, "hydro-tma": os.path.join(os.path.dirname(capi.LIB_PATH), "libdasha_zhtma.so")}
+
+
+def _cfg(grid, precision):
+    return dataclasses.replace(harris.CONFIGS["c4"], mx=grid[0], my=grid[1], mz=grid[2]), 1 if precision == "fp32" else 0
+
+
+def _run(lib, cfg, prec, warmup, steps):
+    d = capi.gem_context(cfg, prec, lib=lib)
+    t = 0.0
+
+    def step(n):
+        nonlocal t
+        dt = d.setdt(t)
+        d.stepon(t, dt, n)
+        t += dt
+
+    for n in range(warmup):
+        step(n)
+    d.timer_start()
+    for n in range(steps):
+        step(warmup + n)
+    ms = d.timer_stop() / steps
+    d.profile(True)
+    for n in range(steps):
+        step(warmup + steps + n)
+    prof = d.profile_read()
+    d.profile(False)
+    d.close()
+    return {"ms_per_step": ms,
+            "kernels": {k: round(v[0] / steps, 3) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}}
+
+
+def _state(lib, cfg, prec, steps):
+    d = capi.gem_context(cfg, prec, lib=lib)
+    t = 0.0
+    for n in range(steps):
+        dt = d.setdt(t)
+        d.stepon(t, dt, n)
+        t += dt
+    X = d.get_state()
+    d.close()
+    return X
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", type=int, nargs=3, default=[1024, 512, 1024])
+    ap.add_argument("--check-grid", type=int, nargs=3, default=[256, 128, 128])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    libs = {name: capi.bind(path) for name, path in BUILDS.items()}
+    cfg, prec = _cfg(a.grid, a.precision)
+    out = {"grid": a.grid, "precision": a.precision, "steps": a.steps, "warmup": a.warmup, "builds": {}}
+    for name, lib in libs.items():
+        out["builds"][name] = _run(lib, cfg, prec, a.warmup, a.steps)
+    ccfg, _ = _cfg(a.check_grid, a.precision)
+    states = [_state(lib, ccfg, prec, 2) for lib in libs.values()]
+    out["check"] = {"grid": a.check_grid, "steps": 2, "max_abs_diff": float(np.abs(states[0] - states[1]).max()),
+                    "bitwise_equal": bool(np.array_equal(states[0], states[1]))}
+    print(json.dumps(out))
+    return 0 if out["check"]["bitwise_equal"] else 1
+
+
+if __name__ == "__main__":
+    sys.exit(main())
