@@ -23,6 +23,8 @@
 // Needs mx % 32 == 0 (a tile narrower than 32*VX at the x end is handled).
 #pragma once
 
+#include <type_traits>
+
 namespace dasha {
 
 // VX consecutive values of a field, one access (8-byte aligned float pairs in FP32)
@@ -403,21 +405,48 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
                 T wsum[VX];
 #pragma unroll
                 for (int e = 0; e < VX; ++e) wsum[e] = wsx[e] + (wpy[u] + wmy[u]) + wsz;
+                if constexpr (std::is_same<T, float>::value && VX == 2) {
+                    // FP32 pairs: each operation on the thread's two nodes is one packed FFMA2 /
+                    // FMUL2 (sm_100), with the roundings of the scalar form below
+                    const float2 Wpx = make_float2(wpx[0], wpx[1]), Wmx = make_float2(wmx[0], wmx[1]);
+                    const float2 Wpy = make_float2(wpy[u], wpy[u]), Wmy = make_float2(wmy[u], wmy[u]);
+                    const float2 Wpz = make_float2(wpz, wpz), Wmz = make_float2(wmz, wmz);
+                    const float2 Ws = make_float2(wsum[0], wsum[1]);
+                    const float2 one = MODE == 2 ? make_float2(2.f, 2.f) : make_float2(1.f, 1.f);
 #pragma unroll
-                for (int f = 0; f < NF; ++f) {
-                    const unsigned kind = (KINDS >> (2 * f)) & 3u;
+                    for (int f = 0; f < NF; ++f) {
+                        const unsigned kind = (KINDS >> (2 * f)) & 3u;
+                        const float2 v0 = make_float2(q0[u][f][0], q0[u][f][1]);
+                        float2 sn = __fmul2_rn(Wpx, make_float2(nxp(f, 0), nxp(f, 1)));
+                        sn = __ffma2_rn(Wmx, make_float2(nxm(f, 0), nxm(f, 1)), sn);
+                        sn = __ffma2_rn(Wpy, make_float2(nyp(f, 0), nyp(f, 1)), sn);
+                        sn = __ffma2_rn(Wmy, make_float2(nym(f, 0), nym(f, 1)), sn);
+                        sn = __ffma2_rn(Wpz, make_float2(qp[u][f][0], qp[u][f][1]), sn);
+                        sn = __ffma2_rn(Wmz, make_float2(qm[u][f][0], qm[u][f][1]), sn);
+                        const float2 cf = kind == 0u ? make_float2(cr[0], cr[1])
+                                                     : (kind == 1u ? make_float2(0.125f, 0.125f) : make_float2(cbx[0], cbx[1]));
+                        const float2 a = __ffma2_rn(make_float2(-cf.x, -cf.y), Ws, one);
+                        const float2 r = __ffma2_rn(cf, sn, __fmul2_rn(a, v0));
+                        val[f][0] = r.x;
+                        val[f][1] = r.y;
+                    }
+                } else {
 #pragma unroll
-                    for (int e = 0; e < VX; ++e) {
-                        const T v0 = q0[u][f][e];
-                        T sn = wpx[e] * nxp(f, e);
-                        sn = fma(wmx[e], nxm(f, e), sn);
-                        sn = fma(wpy[u], nyp(f, e), sn);
-                        sn = fma(wmy[u], nym(f, e), sn);
-                        sn = fma(wpz, qp[u][f][e], sn);
-                        sn = fma(wmz, qm[u][f][e], sn);
-                        const T coef = kind == 0u ? cr[e] : (kind == 1u ? T(0.125) : cbx[e]);
-                        const T a = fma(-coef, wsum[e], MODE == 2 ? T(2) : T(1));
-                        val[f][e] = fma(coef, sn, a * v0);
+                    for (int f = 0; f < NF; ++f) {
+                        const unsigned kind = (KINDS >> (2 * f)) & 3u;
+#pragma unroll
+                        for (int e = 0; e < VX; ++e) {
+                            const T v0 = q0[u][f][e];
+                            T sn = wpx[e] * nxp(f, e);
+                            sn = fma(wmx[e], nxm(f, e), sn);
+                            sn = fma(wpy[u], nyp(f, e), sn);
+                            sn = fma(wmy[u], nym(f, e), sn);
+                            sn = fma(wpz, qp[u][f][e], sn);
+                            sn = fma(wmz, qm[u][f][e], sn);
+                            const T coef = kind == 0u ? cr[e] : (kind == 1u ? T(0.125) : cbx[e]);
+                            const T a = fma(-coef, wsum[e], MODE == 2 ? T(2) : T(1));
+                            val[f][e] = fma(coef, sn, a * v0);
+                        }
                     }
                 }
                 if constexpr (MODE == 2) {
