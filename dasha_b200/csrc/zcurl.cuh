@@ -15,6 +15,8 @@
 // once (hence D + 5 stages) and ends with a second barrier.
 #pragma once
 
+#include <type_traits>
+
 namespace dasha {
 
 template <class T, int VX, int TY, int D>
@@ -147,6 +149,29 @@ __global__ void __launch_bounds__(32 * TY) k_zcurl(Geo<T> g, SrcFields<T, 3> src
                 return k < 0 ? lo[k + 2] : (k >= VX ? hi[k - VX] : cen[k < 0 ? 0 : (k >= VX ? VX - 1 : k)]);
             };
             T o[3][VX];
+            if constexpr (std::is_same<T, float>::value && VX == 2) {
+                // the pair's six derivatives as packed pairs (node 0, node 1), the roundings of
+                // the scalar form below
+                const float2 AX = make_float2(ax[0], ax[1]), BX = make_float2(bx[0], bx[1]);
+                const float2 CX = make_float2(cx[0], cx[1]), DX = make_float2(dx[0], dx[1]);
+                auto v2 = [](const float (&a)[2]) { return make_float2(a[0], a[1]); };
+                auto zp = [&](int s, int f) { return make_float2(zq[s][f][0], zq[s][f][1]); };
+                const float2 d1x = d1fc2(v2(l1), make_float2(l1[1], c1[0]), v2(c1), make_float2(c1[1], r1[0]), v2(r1),
+                                         AX, BX, CX, DX);
+                const float2 d2x = d1fc2(v2(l2), make_float2(l2[1], c2[0]), v2(c2), make_float2(c2[1], r2[0]), v2(r2),
+                                         AX, BX, CX, DX);
+                const float2 d0y = d1fc2(v2(y0m2), v2(y0m1), zp(2, 0), v2(y0p1), v2(y0p2), bc2(ay), bc2(by), bc2(cy), bc2(dy));
+                const float2 d2y = d1fc2(v2(y2m2), v2(y2m1), v2(c2), v2(y2p1), v2(y2p2), bc2(ay), bc2(by), bc2(cy), bc2(dy));
+                const float2 d0z = d1fc2(zp(0, 0), zp(1, 0), zp(2, 0), zp(3, 0), zp(4, 0), bc2(az), bc2(bz), bc2(cz), bc2(dz));
+                const float2 d1z = d1fc2(zp(0, 1), zp(1, 1), zp(2, 1), zp(3, 1), zp(4, 1), bc2(az), bc2(bz), bc2(cz), bc2(dz));
+                float2 r0, r1v, r2v;
+                if (SIGN > 0) {
+                    r0 = __fadd2_rn(d2y, neg2(d1z)); r1v = __fadd2_rn(d0z, neg2(d2x)); r2v = __fadd2_rn(d1x, neg2(d0y));
+                } else {
+                    r0 = __fadd2_rn(neg2(d2y), d1z); r1v = __fadd2_rn(neg2(d0z), d2x); r2v = __fadd2_rn(neg2(d1x), d0y);
+                }
+                o[0][0] = r0.x; o[0][1] = r0.y; o[1][0] = r1v.x; o[1][1] = r1v.y; o[2][0] = r2v.x; o[2][1] = r2v.y;
+            } else {
 #pragma unroll
             for (int e = 0; e < VX; ++e) {
                 const T d1x = d1fc(xv(c1, l1, r1, e, -2), xv(c1, l1, r1, e, -1), c1[e], xv(c1, l1, r1, e, 1),
@@ -166,6 +191,7 @@ __global__ void __launch_bounds__(32 * TY) k_zcurl(Geo<T> g, SrcFields<T, 3> src
                     o[1][e] = -d0z + d2x;
                     o[2][e] = -d1x + d0y;
                 }
+            }
             }
             const long col = (long)gi + (long)gj * g.sy;
 #pragma unroll

@@ -25,6 +25,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <type_traits>
 
 namespace dasha {
 
@@ -276,6 +277,68 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
             T o[5][VX], dvv[VX], px[VX], py[VX], pz[VX];
             // the six x/y/z quantities of one stencil node from (m1 m2 m3 dp ri) there:
             // direction d: m_d, F_1d, F_2d, F_3d (+ dp on the diagonal), dp, v_d
+            if constexpr (std::is_same<T, float>::value && VX == 1) {
+            // FP32, one node per thread: the six quantities of a direction as three packed pairs,
+            // each five-point derivative of a pair one FMUL2 + three FFMA2 after four FADD2
+            auto d1p = [](const float2 (&q)[5], float2 a2, float2 b2, float2 c2, float2 d2) {
+                return d1fc2(q[0], q[1], q[2], q[3], q[4], a2, b2, c2, d2);
+            };
+            // ---- x: pairs (m1, m1 v1 + dp), (m2 v1, m3 v1), (dp, v1) ----
+            {
+                float2 P0[5], P1[5], P2[5];
+#pragma unroll
+                for (int s2 = 0; s2 < 5; ++s2) {
+                    const int off = s2 - 2;
+                    float v[NF];
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) v[f] = off == 0 ? zq[2][f][0] : pc[f * SP + me + off];
+                    const float a = v[0] * v[4];
+                    P0[s2] = make_float2(v[0], fmaf(v[0], a, v[3]));
+                    P1[s2] = __fmul2_rn(make_float2(v[1], v[2]), make_float2(a, a));
+                    P2[s2] = make_float2(v[3], a);
+                }
+                const float2 A2 = make_float2(ax[0], ax[0]), B2 = make_float2(bx[0], bx[0]);
+                const float2 C2 = make_float2(cx[0], cx[0]), D2 = make_float2(dx[0], dx[0]);
+                const float2 r0 = d1p(P0, A2, B2, C2, D2), r1 = d1p(P1, A2, B2, C2, D2), r2 = d1p(P2, A2, B2, C2, D2);
+                o[0][0] = -r0.x; o[1][0] = -r0.y; o[2][0] = -r1.x; o[3][0] = -r1.y;
+                px[0] = r2.x; dvv[0] = -r2.y;
+            }
+            // ---- y: pairs (m2, m2 v2 + dp), (m1 v2, m3 v2), (dp, v2) ----
+            {
+                float2 P0[5], P1[5], P2[5];
+#pragma unroll
+                for (int s2 = 0; s2 < 5; ++s2) {
+                    const int off = s2 - 2;
+                    float v[NF];
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) v[f] = off == 0 ? zq[2][f][0] : pc[f * SP + me + off * RS];
+                    const float b = v[1] * v[4];
+                    P0[s2] = make_float2(v[1], fmaf(v[1], b, v[3]));
+                    P1[s2] = __fmul2_rn(make_float2(v[0], v[2]), make_float2(b, b));
+                    P2[s2] = make_float2(v[3], b);
+                }
+                const float2 A2 = make_float2(ay, ay), B2 = make_float2(by, by), C2 = make_float2(cy, cy), D2 = make_float2(dy, dy);
+                const float2 r0 = d1p(P0, A2, B2, C2, D2), r1 = d1p(P1, A2, B2, C2, D2), r2 = d1p(P2, A2, B2, C2, D2);
+                o[0][0] -= r0.x; o[2][0] -= r0.y; o[1][0] -= r1.x; o[3][0] -= r1.y;
+                py[0] = r2.x; dvv[0] -= r2.y;
+            }
+            // ---- z: pairs (m3, m3 v3 + dp), (m1 v3, m2 v3), (dp, v3), from the register queue ----
+            {
+                float2 P0[5], P1[5], P2[5];
+#pragma unroll
+                for (int s2 = 0; s2 < 5; ++s2) {
+                    const float m1 = zq[s2][0][0], m2 = zq[s2][1][0], m3 = zq[s2][2][0], dp = zq[s2][3][0], ri = zq[s2][4][0];
+                    const float v3 = m3 * ri;
+                    P0[s2] = make_float2(m3, fmaf(m3, v3, dp));
+                    P1[s2] = __fmul2_rn(make_float2(m1, m2), make_float2(v3, v3));
+                    P2[s2] = make_float2(dp, v3);
+                }
+                const float2 A2 = make_float2(az, az), B2 = make_float2(bz, bz), C2 = make_float2(cz, cz), D2 = make_float2(dz, dz);
+                const float2 r0 = d1p(P0, A2, B2, C2, D2), r1 = d1p(P1, A2, B2, C2, D2), r2 = d1p(P2, A2, B2, C2, D2);
+                o[0][0] -= r0.x; o[3][0] -= r0.y; o[1][0] -= r1.x; o[2][0] -= r1.y;
+                pz[0] = r2.x + T(g.dzp0[c]); dvv[0] -= r2.y;
+            }
+            } else {
             // ---- x ----
             {
                 T lo[NF][2], hi[NF][2];
@@ -363,6 +426,7 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
                 for (int u = 0; u < 6; ++u) dd[u] = d1fc(q6[u][0], q6[u][1], q6[u][2], q6[u][3], q6[u][4], az, bz, cz, dz);
                 o[0][e] -= dd[0]; o[1][e] -= dd[1]; o[2][e] -= dd[2]; o[3][e] -= dd[3];
                 pz[e] = dd[4] + T(g.dzp0[c]); dvv[e] -= dd[5];
+            }
             }
             // ---- pointwise: J x B - xresd, pressure equation ----
             const T rsx = T(g.rsx[c]), rsy = T(g.rsy[c]), rsz = T(g.rsz[c]), p0 = T(g.p0[c]);

@@ -26,6 +26,8 @@
 // kind for both passes.  Needs mx % 32 == 0.
 #pragma once
 
+#include <type_traits>
+
 namespace dasha {
 
 template <class T, int NF, int VX, int TY, int D>
@@ -180,21 +182,43 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
                 xle[f] = pc[f * SPI + me - 1];
                 xri[f] = pc[f * SPI + me + VX];
             }
+            if constexpr (std::is_same<T, float>::value && VX == 2) {
+                // FP32 pairs as packed FFMA2 / FMUL2, with the roundings of the scalar form below
+                const float2 Wpx = make_float2(wpx[0], wpx[1]), Wmx = make_float2(wmx[0], wmx[1]);
+                const float2 Wpy = make_float2(wpy, wpy), Wmy = make_float2(wmy, wmy);
+                const float2 Wpz = make_float2(wpz, wpz), Wmz = make_float2(wmz, wmz);
+                const float2 Ws = make_float2(wsx[0] + (wpy + wmy) + wsz, wsx[1] + (wpy + wmy) + wsz);
 #pragma unroll
-            for (int f = 0; f < NF; ++f)
-#pragma unroll
-                for (int e = 0; e < VX; ++e) {
-                    const T v0 = q0[f][e];
-                    T sn = wpx[e] * (e < VX - 1 ? q0[f][e < VX - 1 ? e + 1 : e] : xri[f]);
-                    sn = fma(wmx[e], e > 0 ? q0[f][e > 0 ? e - 1 : 0] : xle[f], sn);
-                    sn = fma(wpy, yhi[f][e], sn);
-                    sn = fma(wmy, ylo[f][e], sn);
-                    sn = fma(wpz, qp[f][e], sn);
-                    sn = fma(wmz, qm[f][e], sn);
-                    const T c = coef_of(f, cbx[e], xx2[e] + yy2, zz2);
-                    const T a = fma(-c, wsx[e] + (wpy + wmy) + wsz, T(1));
-                    l1[f][e] = fma(c, sn, a * v0);
+                for (int f = 0; f < NF; ++f) {
+                    float2 sn = __fmul2_rn(Wpx, make_float2(q0[f][1], xri[f]));
+                    sn = __ffma2_rn(Wmx, make_float2(xle[f], q0[f][0]), sn);
+                    sn = __ffma2_rn(Wpy, make_float2(yhi[f][0], yhi[f][1]), sn);
+                    sn = __ffma2_rn(Wmy, make_float2(ylo[f][0], ylo[f][1]), sn);
+                    sn = __ffma2_rn(Wpz, make_float2(qp[f][0], qp[f][1]), sn);
+                    sn = __ffma2_rn(Wmz, make_float2(qm[f][0], qm[f][1]), sn);
+                    const float2 cf = make_float2(coef_of(f, cbx[0], xx2[0] + yy2, zz2), coef_of(f, cbx[1], xx2[1] + yy2, zz2));
+                    const float2 a = __ffma2_rn(make_float2(-cf.x, -cf.y), Ws, make_float2(1.f, 1.f));
+                    const float2 r = __ffma2_rn(cf, sn, __fmul2_rn(a, make_float2(q0[f][0], q0[f][1])));
+                    l1[f][0] = r.x;
+                    l1[f][1] = r.y;
                 }
+            } else {
+#pragma unroll
+                for (int f = 0; f < NF; ++f)
+#pragma unroll
+                    for (int e = 0; e < VX; ++e) {
+                        const T v0 = q0[f][e];
+                        T sn = wpx[e] * (e < VX - 1 ? q0[f][e < VX - 1 ? e + 1 : e] : xri[f]);
+                        sn = fma(wmx[e], e > 0 ? q0[f][e > 0 ? e - 1 : 0] : xle[f], sn);
+                        sn = fma(wpy, yhi[f][e], sn);
+                        sn = fma(wmy, ylo[f][e], sn);
+                        sn = fma(wpz, qp[f][e], sn);
+                        sn = fma(wmz, qm[f][e], sn);
+                        const T c = coef_of(f, cbx[e], xx2[e] + yy2, zz2);
+                        const T a = fma(-c, wsx[e] + (wpy + wmy) + wsz, T(1));
+                        l1[f][e] = fma(c, sn, a * v0);
+                    }
+            }
 #pragma unroll
             for (int f = 0; f < NF; ++f) IO::st(l1p + f * SP1 + r1 * RS + OFF + xl, l1[f]);
         }
@@ -243,18 +267,33 @@ __global__ void __launch_bounds__(32 * (TY + 2)) k_zpv2(Geo<T> g, SrcFields<T, N
                 IO::ld(l1q + f * SP1 + m1 - RS, ylo);
                 IO::ld(l1q + f * SP1 + m1 + RS, yhi);
                 const T xle = l1q[f * SP1 + m1 - 1], xri = l1q[f * SP1 + m1 + VX];
+                if constexpr (std::is_same<T, float>::value && VX == 2) {
+                    float2 sn = __fmul2_rn(make_float2(wpx[0], wpx[1]), make_float2(lb[f][1], xri));
+                    sn = __ffma2_rn(make_float2(wmx[0], wmx[1]), make_float2(xle, lb[f][0]), sn);
+                    sn = __ffma2_rn(make_float2(wpy, wpy), make_float2(yhi[0], yhi[1]), sn);
+                    sn = __ffma2_rn(make_float2(wmy, wmy), make_float2(ylo[0], ylo[1]), sn);
+                    sn = __ffma2_rn(make_float2(zwp, zwp), make_float2(lc[f][0], lc[f][1]), sn);
+                    sn = __ffma2_rn(make_float2(zwm, zwm), make_float2(la[f][0], la[f][1]), sn);
+                    const float2 cf = make_float2(coef_of(f, cbx[0], xx2[0] + yy2, qz2), coef_of(f, cbx[1], xx2[1] + yy2, qz2));
+                    const float2 ws = make_float2(wsx[0] + (wpy + wmy) + zws, wsx[1] + (wpy + wmy) + zws);
+                    const float2 a = __ffma2_rn(make_float2(-cf.x, -cf.y), ws, make_float2(1.f, 1.f));
+                    const float2 r = __ffma2_rn(cf, sn, __fmul2_rn(a, make_float2(lb[f][0], lb[f][1])));
+                    val[f][0] = r.x;
+                    val[f][1] = r.y;
+                } else {
 #pragma unroll
-                for (int e = 0; e < VX; ++e) {
-                    const T v0 = lb[f][e];
-                    T sn = wpx[e] * (e < VX - 1 ? lb[f][e < VX - 1 ? e + 1 : e] : xri);
-                    sn = fma(wmx[e], e > 0 ? lb[f][e > 0 ? e - 1 : 0] : xle, sn);
-                    sn = fma(wpy, yhi[e], sn);
-                    sn = fma(wmy, ylo[e], sn);
-                    sn = fma(zwp, lc[f][e], sn);
-                    sn = fma(zwm, la[f][e], sn);
-                    const T c = coef_of(f, cbx[e], xx2[e] + yy2, qz2);
-                    const T a = fma(-c, wsx[e] + (wpy + wmy) + zws, T(1));
-                    val[f][e] = fma(c, sn, a * v0);
+                    for (int e = 0; e < VX; ++e) {
+                        const T v0 = lb[f][e];
+                        T sn = wpx[e] * (e < VX - 1 ? lb[f][e < VX - 1 ? e + 1 : e] : xri);
+                        sn = fma(wmx[e], e > 0 ? lb[f][e > 0 ? e - 1 : 0] : xle, sn);
+                        sn = fma(wpy, yhi[e], sn);
+                        sn = fma(wmy, ylo[e], sn);
+                        sn = fma(zwp, lc[f][e], sn);
+                        sn = fma(zwm, la[f][e], sn);
+                        const T c = coef_of(f, cbx[e], xx2[e] + yy2, qz2);
+                        const T a = fma(-c, wsx[e] + (wpy + wmy) + zws, T(1));
+                        val[f][e] = fma(c, sn, a * v0);
+                    }
                 }
             }
             const long col = (long)gi + (long)gy * g.sy;
