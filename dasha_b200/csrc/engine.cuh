@@ -11,6 +11,7 @@
 #include "zeh.cuh"
 #include "adjoint.cuh"
 #include "checkpoint_schedule.h"
+#include "host_pool.h"
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <cstdlib>
@@ -428,20 +429,9 @@ public:
             xev[b] = nullptr;
         }
     }
-    // f(r0, r1) over rows [0, n), split across host threads
+    // f(r0, r1) over rows [0, n), split across the host thread pool
     template <class F>
-    static void par_rows(long n, F f) {
-        const unsigned hw = std::thread::hardware_concurrency();
-        const long nt = std::min<long>(16, std::max<long>(1, (long)hw));
-        if (n < 256 || nt == 1) { f(0L, n); return; }
-        std::vector<std::thread> th;
-        const long per = (n + nt - 1) / nt;
-        for (long t = 0; t < nt; ++t) {
-            const long a0 = t * per, a1 = std::min(n, a0 + per);
-            if (a0 < a1) th.emplace_back(f, a0, a1);
-        }
-        for (auto& x : th) x.join();
-    }
+    static void par_rows(long n, F f) { HostPool::get().run(n, f); }
     // Chunked host transfers.  z-plane chunks of one field move through the two pinned host
     // buffers and the two device buffers, so that the host work on one chunk overlaps the DMA
     // and the conversion kernel of the other.  The host work is the caller's: fill(m, k0, k1,
