@@ -2,8 +2,11 @@
 z-marching kernels load or store is tested against its field's extent; a violation is recorded
 and skipped (no trap, no fault) and the C-ABI call returns DASHA_E_CUDA naming the site.  The
 ragged 96x12x36 grid (x not a multiple of the 64-node FP32 tile, y not a multiple of the 8 or 4
-rows of a CTA, two z chunks) runs the current, a right-hand side and 4 steps in FP64 and FP32
-with no violation, and gives the normal build's results bit for bit."""
+rows of a CTA, two z chunks), the smallest grid the library accepts (32x5x7: one x tile, fewer
+y rows than a CTA, three interior planes), an odd one (160x7x9) and a tall one (32x8x300, many
+z chunks) run the current, a right-hand side and 4 steps in FP64 and FP32 with no violation,
+and give the normal build's results bit for bit.  Runs before the parity tests of the same
+grids (file order), so that a violation is reported by this build first."""
 import numpy as np
 import pytest
 
@@ -12,17 +15,21 @@ from dasha_b200 import capi, harris
 pytestmark = pytest.mark.gpu
 
 RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 4, dt_whistler=1)
+MINI = harris.RunConfig("mini-32x5x7", 32, 5, 7, False, 0.005, 0.5, 4)
+ODD = harris.RunConfig("odd-160x7x9-sinh", 160, 7, 9, True, 0.003, 1.0, 4, dt_whistler=1)
+TALL = harris.RunConfig("tall-32x8x300-sinh", 32, 8, 300, True, 0.003, 1.0, 4)
 
 
+@pytest.mark.parametrize("cfg", [RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
 @pytest.mark.parametrize("precision", [0, 1], ids=["fp64", "fp32"])
-def test_ragged_grid_stays_in_bounds(precision):
+def test_grid_stays_in_bounds(precision, cfg):
     lib = capi.bind(capi.BOUNDS_LIB_PATH)
     out = []
     for which in (lib, None):
-        d = capi.gem_context(RAGGED, precision, lib=which)
+        d = capi.gem_context(cfg, precision, lib=which)
         cur = d.current()
         rhs = d.rhs(0.5)
-        t, _ = d.run(RAGGED.steps)
+        t, _ = d.run(cfg.steps)
         out.append((cur, rhs, d.get_state(), t, d.setdt(t)))
         d.close()
     for a, b in zip(out[0], out[1]):

@@ -19,6 +19,11 @@ SMALL_S = harris.RunConfig("small-32x16x40-sinh", 32, 16, 40, True, 0.003, 1.0, 
 # ragged tiles: mx not a multiple of the 64-node FP32 tile, my not a multiple of the 8 or 4
 # rows of a CTA, two z chunks of 18 planes
 RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 4, dt_whistler=1)
+# the smallest accepted grid (one x tile, 5 rows, 3 interior planes), an odd one, a tall one
+# (many z chunks); checked in bounds by tests/test_gpu_bounds.py first
+MINI = harris.RunConfig("mini-32x5x7", 32, 5, 7, False, 0.005, 0.5, 4)
+ODD = harris.RunConfig("odd-160x7x9-sinh", 160, 7, 9, True, 0.003, 1.0, 4, dt_whistler=1)
+TALL = harris.RunConfig("tall-32x8x300-sinh", 32, 8, 300, True, 0.003, 1.0, 4)
 
 
 def rel_err(a, b):
@@ -41,14 +46,14 @@ def test_state_roundtrip(cfg):
     assert rel_err(d.get_state(), o.get_state()).max() < 1e-15
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
 def test_current_parity(cfg):
     o, d = pair(cfg)
     e = rel_err(d.current(), o.current())
     assert e.max() < 1e-11, e
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, harris.CONFIGS["c0"], RAGGED], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, harris.CONFIGS["c0"], RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
 @pytest.mark.parametrize("t", [0.0, 0.5])
 def test_rhs_parity(cfg, t):
     o, d = pair(cfg)
@@ -98,7 +103,7 @@ def test_setdt_parity_whistler_option():
     assert d.setdt() < 0.5 * plain
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
 def test_steps_parity(cfg):
     o, d = pair(cfg)
     t = 0.0
