@@ -171,16 +171,6 @@ __global__ void k_midplane(Geo<T> g, int j, F8<T> x, F8<T> comp, F3<T> cur, doub
 template <class T>
 inline const double* eq_profile(const Geo<T>& g, int m);
 
-// radial smoothing coefficient per node, computed in FP64 then stored as T
-template <class T>
-__global__ void k_init_cr(int mx, int my, int mz, const double* xc, const double* yc, const double* zc, T* cr) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= mx) return;
-    int j = blockIdx.y, k = blockIdx.z;
-    double r = sqrt(xc[i] * xc[i] + yc[j] * yc[j] + zc[k] * zc[k]);
-    cr[(long)i + (long)mx * (j + (long)my * k)] = T(1.0 / 32.0 + (1.0 / 8.0 - 1.0 / 32.0) * 0.5 * (1 + tanh((r - 3.) / 3.)));
-}
-
 template <class T>
 class Engine : public EngineBase {
 public:
@@ -193,7 +183,6 @@ public:
     void* pool = nullptr;
     T *X[8], *S[8], *A[8], *K[8], *C[8];
     T *cur[2][3], *E[2][3], *Hh[2][3];
-    T* cr = nullptr;
     T* tab = nullptr;            // 1-D tables in T
     double* dtab = nullptr;      // 1-D tables in FP64
     double* red = nullptr;       // reduction scratch
@@ -278,7 +267,6 @@ public:
             *w2[d][0] = t + off[d][8]; *w2[d][1] = t + off[d][9];
         }
         g.cbx = t + offcb;
-        g.cr = nullptr;
         g.xc = t + off[0][10]; g.yc = t + off[1][10]; g.zc = t + off[2][10];
         g.eta = T(p.eta); g.di = T(p.di); g.gamma = T(p.gamma); g.mu = T(p.mu); g.drho = T(p.drho); g.dp = T(p.dp);
         g.hall = p.hall; g.viscos = p.viscos && p.mu != 0.0; g.diffu = p.diffu && (p.drho != 0.0 || p.dp != 0.0);

@@ -27,8 +27,8 @@ struct Geo {
     // difc weights: difc = (f+ - f0)*wp - (f0 - f-)*wm  (t3dsdsc.f:5618-5619)
     const T *wpx, *wmx, *wpy, *wmy, *wpz, *wmz;
     const T *cbx;    // (1/32)(1 - tanh((x+3)/8)), smoothing coefficient of B (t3dsdsc.f:5636-5642)
-    const T *cr;     // 1/32 + 3/32 * (1 + tanh((r-3)/3))/2 per node (t3dsdsc.f:5659-5661), optional
-    const T *xc, *yc, *zc;   // node coordinates (radial coefficient evaluated on the fly)
+    const T *xc, *yc, *zc;   // node coordinates: the radial coefficient 1/32 + 3/32 (1 + tanh((r-3)/3))/2
+                             // (t3dsdsc.f:5659-5661) is evaluated per node, not stored
     // equilibrium z-profiles (FP64)
     const double *rho0, *bx0, *by0, *bz0, *p0;
     const double *dzp0;               // Dz p0 (interior rows)
