@@ -38,7 +38,7 @@ class ParamsC(C.Structure):
                 ("drho", C.c_double), ("dp", C.c_double), ("cfl", C.c_double), ("rcr", C.c_double),
                 ("hall", C.c_int), ("viscos", C.c_int), ("diffu", C.c_int), ("total_e", C.c_int),
                 ("j0_mode", C.c_int), ("filter_every", C.c_int), ("precision", C.c_int),
-                ("dt_whistler", C.c_int)]
+                ("dt_whistler", C.c_int), ("uyzlimiter", C.c_int)]
 
 
 # every symbol include/dasha_capi.h declares, with its argument types

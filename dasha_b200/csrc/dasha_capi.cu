@@ -155,6 +155,8 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
     if (p.precision != 0 && p.precision != 1) return DASHA_E_INVALID;
     if (p.total_e != 1 || (!bounded && p.rcr > 0.0)) return DASHA_E_UNSUPPORTED;
     if (bounded && p.precision != 0) return DASHA_E_UNSUPPORTED;     // the bounded configuration is FP64
+    if (p.uyzlimiter != 0 && p.uyzlimiter != 1) return DASHA_E_INVALID;
+    if (!bounded && p.uyzlimiter) return DASHA_E_UNSUPPORTED;         // the limiter is a bounded-context option
     if (p.j0_mode != 0 && p.j0_mode != 1) return DASHA_E_INVALID;
     if (!(p.gamma > 1.0) || !(p.cfl > 0.0) || p.filter_every < 0) return DASHA_E_INVALID;
     dasha_ctx* c = new (std::nothrow) dasha_ctx();

@@ -69,7 +69,7 @@ public:
         n = d.n;
         par.gamma = p.gamma; par.eta = p.eta; par.mu = p.viscos ? p.mu : 0.; par.drho = p.diffu ? p.drho : 0.;
         par.dp = p.diffu ? p.dp : 0.; par.cfl = p.cfl; par.rcr = p.rcr; par.chall = p.di;
-        par.hall = p.hall; par.viscos = p.viscos; par.diffu = p.diffu;
+        par.hall = p.hall; par.viscos = p.viscos; par.diffu = p.diffu; par.uyzlimiter = p.uyzlimiter;
         DASHA_CK(cudaMalloc(&pool, sizeof(double) * n * walls::NFIELDS + 256));
         DASHA_CK(cudaMemsetAsync(pool, 0, sizeof(double) * n * walls::NFIELDS + 256, st));
         DASHA_CK(cudaStreamSynchronize(st));          // the stream does not order with the copies below

@@ -49,6 +49,7 @@ struct Tables {
 struct Par {
     double gamma, eta, mu, drho, dp, cfl, rcr, chall;
     int hall, viscos, diffu;
+    int uyzlimiter;
 };
 
 // device arrays of one context (padded layout); 8-field arrays hold field m at m*n
@@ -238,6 +239,29 @@ struct Core {
                 f[cl - sz] = 0.5 * f[cl - 2 * sz];
             }
         });
+        // the uy/uz limiter of bndry and bndrytt (T:1928-1975, 2231-2278): on the two wall rows
+        // at each z end the z momentum, on the two rows at each y end the y momentum, may only
+        // point into the domain
+        if (p.uyzlimiter && (kind == ROWS_XDIF || kind == ROWS_TT)) {
+            double* mz3 = base + 3 * n;
+            ex.run({d.x_first, d.x_last + 2, 1, d.my, 3, 4}, [=] WHD(int jx, int jy, int jz) {
+                const long c = dd.at(jx, jy, jz);
+                if (mz3[c] >= 0.) mz3[c] = 0.;
+            });
+            ex.run({d.x_first, d.x_last + 2, 1, d.my, d.zlast - 1, d.zlast}, [=] WHD(int jx, int jy, int jz) {
+                const long c = dd.at(jx, jy, jz);
+                if (mz3[c] <= 0.) mz3[c] = 0.;
+            });
+            double* my2 = base + 2 * n;
+            ex.run({d.x_first, d.x_last + 2, 1, 2, d.z_first - 2, d.z_last + 2}, [=] WHD(int jx, int jy, int jz) {
+                const long c = dd.at(jx, jy, jz);
+                if (my2[c] >= 0.) my2[c] = 0.;
+            });
+            ex.run({d.x_first, d.x_last + 2, d.my - 1, d.my, d.z_first - 2, d.z_last + 2}, [=] WHD(int jx, int jy, int jz) {
+                const long c = dd.at(jx, jy, jz);
+                if (my2[c] <= 0.) my2[c] = 0.;
+            });
+        }
     }
 
     // ---- current (T:2452-2500): J = curl(B - B0), bndryc, avrgc(1,3,4) ----

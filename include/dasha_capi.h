@@ -71,7 +71,8 @@ typedef struct {
 /* Run-time constants and flags, mhd03.for:1-83 and COMMON /cst/ (mhd01.for:55).
  *  gamma, cfl                      mhd03.for:60,71
  *  eta (etan = eta0), mu (fmu0), drho (frho0), dp (fpr0)   foreta/formu t3dsdsc.f:6489-6532
- *  di: Hall coefficient cht, uniform (replaces the radial profile of t3dsdsc.f:1398)
+ *  di: Hall coefficient cht: uniform on periodic contexts; on bounded contexts the reference's
+ *    radial profile of it (t3dsdsc.f:1398)
  *  rcr: inner-sphere mask radius (mhd03.for:26); on periodic contexts only rcr <= 0 (no mask)
  *  hall, viscos, diffu, total_e: mhd03.for:18-23 (total_e must be 1)
  *  j0_mode: 0 = LITERAL (J = curl(B-B0), the reference's equations), 1 = FULL (J0 added)
@@ -79,13 +80,18 @@ typedef struct {
  *  precision: 0 = FP64 state and arithmetic; 1 = FP32 perturbation + Kahan-compensated RK4
  *  dt_whistler: 0 = the reference's CFL (fast speed only, t3dsdsc.f:4719-4733); 1 = also add
  *    the grid-scale whistler speed di*pi*|B|/(rho*h) to each direction's signal speed (the
- *    explicit Hall term is unstable at fine grids without it; no counterpart in the reference) */
+ *    explicit Hall term is unstable at fine grids without it; no counterpart in the reference)
+ *  uyzlimiter: the reference's uy/uz limiter (mhd03.for:22, .false. there): after bndry and
+ *    bndrytt, the z momentum of the two wall rows at each z end and the y momentum of the two
+ *    rows at each y end may only point into the domain (t3dsdsc.f:1928-1975, 2231-2278).
+ *    Bounded contexts only; 1 on a periodic context returns DASHA_E_UNSUPPORTED */
 typedef struct {
     double gamma, eta, di, mu, drho, dp, cfl, rcr;
     int hall, viscos, diffu, total_e, j0_mode;
     int filter_every;
     int precision;
     int dt_whistler;
+    int uyzlimiter;
 } dasha_params_c;
 
 #define DASHA_NDIAG 9

@@ -71,3 +71,18 @@ def test_unsupported_bounded_options_are_refused_before_the_device(periodic, pre
     h = ctypes.c_void_p()
     assert lib.dasha_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == capi.E_UNSUPPORTED
     assert not h.value
+
+
+@pytest.mark.parametrize("periodic,uyz,code", [((1, 1, 0), 1, capi.E_UNSUPPORTED), ((0, 0, 0), 2, capi.E_INVALID)])
+def test_uyzlimiter_argument_checks(periodic, uyz, code):
+    """The uy/uz limiter is a bounded-context option (0 or 1), refused before a device call."""
+    lib = capi.load()
+    x = np.linspace(-2.1, 5.65, 64) if periodic[0] else np.linspace(-2.1, 5.65, 41)
+    y, z = np.linspace(-2.5, 2.5, 25), np.linspace(-2.5, 2.5, 33)
+    keep = [np.ascontiguousarray(a) for a in (x, y, z)]
+    g = capi.GridC(x.size, 25, 33, *(a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) for a in keep),
+                   (ctypes.c_int * 3)(*periodic))
+    p = capi.make_params(harris.RunConfig("lim", x.size, 25, 33, False, 2e-4, 0.07, 1), 0, uyzlimiter=uyz)
+    h = ctypes.c_void_p()
+    assert lib.dasha_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == code
+    assert not h.value

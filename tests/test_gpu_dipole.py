@@ -19,11 +19,11 @@ T0 = 12.0            # the driver's ramp is under way (its amplitude changes wit
 NOISE = 0.01
 
 
-def _params(R, hall):
+def _params(R, hall, uyz=0):
     return capi.ParamsC(gamma=R.get("gamma"), eta=R.get("eta0"), di=R.get("chall"), mu=R.get("fmu0"),
                         drho=R.get("frho0"), dp=R.get("fpr0"), cfl=R.get("cfl"), rcr=R.get("rcr"),
                         hall=hall, viscos=1, diffu=1, total_e=1, j0_mode=0, filter_every=0, precision=0,
-                        dt_whistler=0)
+                        dt_whistler=0, uyzlimiter=uyz)
 
 
 def _perturb(R, seed=3):
@@ -48,12 +48,13 @@ def test_bounded_equilibrium_and_initial_state_match_initia():
     assert err.max() < 1e-14, err
 
 
-@pytest.mark.parametrize("hall", [0, 1], ids=["hall-off", "hall-on"])
-def test_bounded_steps_match_the_reference(hall, report):
+@pytest.mark.parametrize("hall,uyz", [(0, 0), (1, 0), (1, 1)], ids=["hall-off", "hall-on", "hall-on-uyzlimiter"])
+def test_bounded_steps_match_the_reference(hall, uyz, report):
     R, x, y, z = dipole_reference(hall=hall)
+    R.set(uyzlimiter=uyz)
     E = np.stack([R.interior(n) for n in ("rhoi", "bxi", "byi", "bzi", "pri")])
     _perturb(R)
-    d = dipole.bounded_context(x, y, z, _params(R, hall), equilibrium=E, state=R.interior("x", 8))
+    d = dipole.bounded_context(x, y, z, _params(R, hall, uyz), equilibrium=E, state=R.interior("x", 8))
     t, worst, worst_dt = T0, 0.0, 0.0
     X0 = R.interior("x", 8)
     for s in range(4):
@@ -68,7 +69,7 @@ def test_bounded_steps_match_the_reference(hall, report):
         err = field_err(d.get_state(), R.interior("x", 8))
         worst = max(worst, float(err.max()))
     change = field_err(R.interior("x", 8), X0)
-    report(f"bounded dipole vs reference, 4 RK4 steps, hall={hall}", max_field_err=worst, dt_rel_err=worst_dt,
+    report(f"bounded dipole vs reference, 4 RK4 steps, hall={hall} uyzlimiter={uyz}", max_field_err=worst, dt_rel_err=worst_dt,
            state_change=float(change.max()))
     d.close()
     assert change.max() > 1e-6                     # the steps moved the state

@@ -31,7 +31,7 @@ def host_core(tmp_path_factory):
                     os.path.join(ROOT, "tests", "walls_host.cpp")], check=True)
     L = C.CDLL(out)
     L.wh_create.restype = C.c_void_p
-    L.wh_create.argtypes = [C.c_int] * 3 + [D] * 4 + [C.c_int] * 3
+    L.wh_create.argtypes = [C.c_int] * 3 + [D] * 4 + [C.c_int] * 4
     L.wh_set_eq.argtypes = [C.c_void_p, D]
     L.wh_set_x.argtypes = [C.c_void_p, D]
     L.wh_get.argtypes = [C.c_void_p, C.c_int, D]
@@ -52,14 +52,17 @@ def padded(R, name, nf):
     return np.array(R.arr(name).reshape(-1, order="F")[: n * nf], copy=True)
 
 
-@pytest.mark.parametrize("hall,order,guard_end", [(1, 0, 0), (1, 1, 1), (1, 2, 0), (0, 2, 1)],
-                         ids=["hall-forward", "hall-backward-guard-end", "hall-shuffled", "no-hall-shuffled-guard-end"])
-def test_bounded_core_is_the_reference_bit_for_bit(host_core, hall, order, guard_end):
+@pytest.mark.parametrize("hall,order,guard_end,uyz", [(1, 0, 0, 0), (1, 1, 1, 0), (1, 2, 0, 0), (0, 2, 1, 0), (1, 2, 1, 1)],
+                         ids=["hall-forward", "hall-backward-guard-end", "hall-shuffled", "no-hall-shuffled-guard-end",
+                              "hall-uyzlimiter-shuffled-guard-end"])
+def test_bounded_core_is_the_reference_bit_for_bit(host_core, hall, order, guard_end, uyz):
+    """uyz: the reference's uy/uz limiter (T:1928-1975, 2231-2278) switched on in both."""
     L = host_core
     R, x, y, z = dipole_reference(hall=hall)
+    R.set(uyzlimiter=uyz)
     par = np.array([R.get("gamma"), R.get("eta0"), R.get("fmu0"), R.get("frho0"), R.get("fpr0"), R.get("cfl"),
                     R.get("rcr"), R.get("chall")])
-    h = L.wh_create(R.mx, R.my, R.mz, _p(x), _p(y), _p(z), _p(par), hall, order, guard_end)
+    h = L.wh_create(R.mx, R.my, R.mz, _p(x), _p(y), _p(z), _p(par), hall, uyz, order, guard_end)
     n = R.mxpr * R.my * R.mzpr
     eq = np.concatenate([padded(R, q, 1) for q in ("rhoi", "bxi", "byi", "bzi", "pri")])
     L.wh_set_eq(h, _p(eq))

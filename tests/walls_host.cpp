@@ -93,7 +93,7 @@ extern "C" {
 
 // Arrays on the caller's side are the padded layout, S = (mx+4)*my*(mz+4) doubles per field.
 void* wh_create(int mx, int my, int mz, const double* xc, const double* yc, const double* zc, const double* par,
-                int hall, int order, int guard_end) {
+                int hall, int uyzlimiter, int order, int guard_end) {
     g_order = order;
     g_end = guard_end != 0;
     Ctx* h = new Ctx();
@@ -103,7 +103,7 @@ void* wh_create(int mx, int my, int mz, const double* xc, const double* yc, cons
     long stride = 0;
     guarded(h->S, 1, G, &stride);            // the stride every field array shares
     h->d.n = stride;                         // field m of an array at m * stride
-    h->par = Par{par[0], par[1], par[2], par[3], par[4], par[5], par[6], par[7], hall, 1, 1};
+    h->par = Par{par[0], par[1], par[2], par[3], par[4], par[5], par[6], par[7], hall, 1, 1, uyzlimiter};
     carve(h->a, [&](int k) { long st; return guarded(h->S, k, G, &st); });
     h->a.dtbits = &h->bits;
     const std::vector<std::vector<double>> tabs = make_tables(make_dims(mx, my, mz), xc, yc, zc);
