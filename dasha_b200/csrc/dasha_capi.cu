@@ -108,7 +108,7 @@ static int bounds_status(dasha_ctx* c, int rc) {
 #else
 static int bounds_status(dasha_ctx*, int rc) { return rc; }
 #endif
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
 // the TMA build: a bounded mbarrier wait of k_zhydro that ran out (the kernel returned early)
 static int wait_status(dasha_ctx* c, int rc) {
     if (!c || !c->st) return rc;

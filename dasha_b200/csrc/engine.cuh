@@ -135,7 +135,7 @@ EngineBase* make_engine_walls(int mx, int my, int mz, const dasha_params_c& p, c
         nvtxRangePop();                                                                        \
     } while (0)
 
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -606,6 +606,28 @@ public:
     using ZVc = ZV<T, NF, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D>;
     template <int NF, unsigned KINDS, class Epi, int MODE>
     static constexpr auto zpv_fn() { return k_zpv<T, NF, KINDS, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D, Epi, MODE>; }
+#ifdef DASHA_TMA
+    template <int NF, unsigned KINDS, class Epi, int MODE>
+    static constexpr auto zpv_tma_fn() { return k_zpv_tma<T, NF, KINDS, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D, Epi, MODE>; }
+    // the source fields of a pass as tensor maps, boxes of one ring plane (RS x NR x 1)
+    template <int NF>
+    bool zpv_maps(const SrcFields<T, NF>& src, ZpMaps& m) {
+        using Z = ZVc<NF>;
+        EncodeTiledFn enc = encode_tiled();
+        if (!enc) return false;
+        const cuuint64_t dims[3] = {(cuuint64_t)mx, (cuuint64_t)my, (cuuint64_t)mz};
+        const cuuint64_t strides[2] = {(cuuint64_t)g.sy * sizeof(T), (cuuint64_t)g.sz * sizeof(T)};
+        const cuuint32_t box[3] = {(cuuint32_t)Z::RS, (cuuint32_t)Z::NR, 1u};
+        const cuuint32_t estr[3] = {1u, 1u, 1u};
+        const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        for (int q = 0; q < NF; ++q)
+            if (enc(&m.m[q], dt, 3u, const_cast<T*>(src.f[q]), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+                return false;
+        return true;
+    }
+#endif
     // one smoothing pass of NF fields: src -> epi
     template <int NF, unsigned KINDS, int MODE = 0, class Epi>
     void zp(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
@@ -613,10 +635,21 @@ public:
         dim3 gg((mx + Z::TX - 1) / Z::TX, (my + Z::TY - 1) / Z::TY, 1);
         int ch = zchunk(gg.x * gg.y, 16);
         gg.z = (mz + ch - 1) / ch;
+#ifdef DASHA_TMA
+        ZpMaps maps;
+        if (!zpv_maps<NF>(src, maps)) launch_err = "cuTensorMapEncodeTiled failed for a smoothing pass";
+        DASHA_LAUNCH(tag, bytes, (zpv_tma_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem_tma(), st>>>(g, src, epi, ch, maps)));
+#else
         DASHA_LAUNCH(tag, bytes, (zpv_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem(), st>>>(g, src, epi, ch)));
+#endif
     }
     template <int NF, unsigned KINDS, class Epi, int MODE = 0>
     static cudaError_t zp_attr1() {
+#ifdef DASHA_TMA
+        cudaError_t e = cudaFuncSetAttribute(zpv_tma_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)ZVc<NF>::smem_tma());
+        if (e) return e;
+#endif
         return cudaFuncSetAttribute(zpv_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ZVc<NF>::smem());
     }
@@ -695,7 +728,7 @@ public:
         if ((e = cudaFuncSetAttribute(k_zhydro<T, ZH_VX, ZH_TY, 1, ZH_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZHc::smem())))
             return e;
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
         if ((e = cudaFuncSetAttribute(k_zhydro_tma<T, ZH_VX, ZH_TY, 1, ZH_MINB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZHc::smem_tma())))
             return e;
@@ -834,7 +867,7 @@ public:
 
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
     const char* launch_err = nullptr;   // a launch that could not be set up (reported by stepon)
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
     // the five ring fields of k_zhydro as tensor maps, boxes of one ring plane (RS x NR x 1)
     bool hydro_maps(const HydroIO<T>& io, ZhMaps& m) {
         EncodeTiledFn enc = encode_tiled();
@@ -906,7 +939,7 @@ public:
             dim3 gh((mx + ZHc::TX - 1) / ZHc::TX, (my + ZH_TY - 1) / ZH_TY, 1);
             int chh = zchunk(gh.x * gh.y, 16);
             gh.z = (mz + chh - 1) / chh;
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
             ZhMaps maps;
             if (!hydro_maps(hio, maps)) launch_err = "cuTensorMapEncodeTiled failed for the hydro ring";
             DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),

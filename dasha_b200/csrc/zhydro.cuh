@@ -14,7 +14,7 @@
 // reads planes c-2 .. c+1 for the queue, so it holds planes c-2 .. c+2+D (hence D + 5 stages),
 // and ends with a second barrier.
 //
-// TMA (built with -DDASHA_ZHYDRO_TMA, for comparison): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1,
+// TMA (built with -DDASHA_TMA, for comparison): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1,
 // rows y0-2 .. y0+TY+1) lies inside the grid loads each ring plane as 5 `cp.async.bulk.tensor`
 // boxes of exactly the ring plane's layout, issued by thread 0 against one mbarrier per stage;
 // every thread waits on the stage's mbarrier (time-bounded: after about a second the kernel
@@ -24,48 +24,14 @@
 // same code in both builds.
 #pragma once
 
-#include <cuda.h>
 #include <type_traits>
+
+#include "tma.cuh"
 
 namespace dasha {
 
 // the five ring fields (m1 m2 m3 dp drho) as 3-D tensor maps with the box of one ring plane
 struct ZhMaps { CUtensorMap m[5]; };
-
-__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-#ifdef DASHA_ZHYDRO_TMA
-static __device__ unsigned int g_wait_timeout;    // a bounded mbarrier wait ran out
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// waits for phase `parity` of an mbarrier for at most about 2^31 clocks; false if it ran out
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > (1ll << 31)) return false;
-    return true;
-}
-__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z, unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
-        : "memory");
-}
-#endif
 
 template <class T, int VX, int TY, int D>
 struct ZH {
@@ -115,7 +81,7 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
     // a CTA whose ring box lies inside the grid loads it by TMA (the TMA build)
     const bool tma = TMA && x0 >= OFF && x0 + TX + OFF <= g.mx && y0 >= 2 && y0 + TY + 2 <= g.my;
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(ring + (size_t)NS * NF * SP);
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
     if constexpr (TMA) {
         if (tid == 0)
             for (int q = 0; q < NS; ++q) mbar_init(bars + q, 1);
@@ -149,7 +115,7 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
     }
     const int phi = cB + 2;
     auto issue = [&](int p) {
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
         if (tma) {
             if (tid == 0 && p <= phi) {
                 T* stg = ring + (size_t)(p % NS) * NF * SP;
@@ -225,7 +191,7 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
             IO::ld(io.b1 + q, b1); IO::ld(io.b2 + q, b2); IO::ld(io.b3 + q, b3);
         }
         const T az = g.a1z[c], bz = g.b1z[c], cz = g.c1z[c], dz = g.d1z[c];
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
         if (tma) {
             // planes c-2 .. c+2 on the first step, then c+2: wait, then 1/rho over the plane
             bool late = false;
@@ -473,7 +439,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
     zhydro_body<T, VX, TY, D, false>(g, io, chunk, nullptr);
 }
 
-#ifdef DASHA_ZHYDRO_TMA
+#ifdef DASHA_TMA
 template <class T, int VX, int TY, int D, int MINB = 1>
 __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro_tma(Geo<T> g, HydroIO<T> io, int chunk,
                                                               const __grid_constant__ ZhMaps maps) {

@@ -15,6 +15,12 @@
 // per stage, measured 7-40 % slower per pass on B200 in every arrangement tried: the passes are
 // issue-bound and cp.async's per-thread copies cost about 2 % of their instructions.)
 //
+// TMA (built with -DDASHA_TMA, for comparison): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1, rows
+// y0-1 .. y0+TY) lies inside the grid loads each ring plane as NF `cp.async.bulk.tensor` boxes of
+// exactly the ring plane's layout, issued by thread 0 against one mbarrier per stage; every thread
+// waits (time-bounded) on the stages it reads before the plane's barrier.  CTAs whose halo wraps
+// keep the cp.async copies.  The compute is the same code in both builds.
+//
 // KINDS: 2 bits per output field, 0 radial coefficient, 1 constant 1/8, 2 x-profile cbx.
 // MODE 0 writes the smoothed fields through the epilogue.  MODES 1 and 2 are the two passes of
 // avrgtt on a compensated FP32 state (x, comp) whose value is x - comp: MODE 1 reads x in
@@ -25,7 +31,12 @@
 
 #include <type_traits>
 
+#include "tma.cuh"
+
 namespace dasha {
+
+// the source fields of a pass as 3-D tensor maps with the box of one ring plane (TMA build)
+struct ZpMaps { CUtensorMap m[8]; };
 
 // VX consecutive values of a field, one access (8-byte aligned float pairs in FP32)
 template <class T, int VX>
@@ -206,14 +217,17 @@ struct ZV {
     static constexpr int OFF = EPC;                   // interior column offset in a ring row
     static constexpr int RS = TX + 2 * OFF;           // ring row stride
     static constexpr int NR = TY + 2;                 // rows y0-1 .. y0+TY
-    static constexpr int SP = RS * NR;                // one field-plane
+    static constexpr int SP = (RS * NR * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);   // one field-plane, 128-byte aligned
     static constexpr int NS = D + 3;                  // ring stages
     static constexpr int CH = TX / EPC;               // 16-byte copies per full row
     static constexpr size_t smem() { return sizeof(T) * (size_t)NS * NF * SP; }
+    // the TMA build: the ring 128-byte aligned, then one mbarrier per stage
+    static constexpr size_t smem_tma() { return 128 + smem() + 8 * NS; }
 };
 
-template <class T, int NF, unsigned KINDS, int VX, int TYH, int RY, int D, class Epi, int MODE = 0>
-__global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src, Epi epi, int chunk) {
+template <class T, int NF, unsigned KINDS, int VX, int TYH, int RY, int D, class Epi, int MODE, bool TMA>
+__device__ __forceinline__ void zpv_body(const Geo<T>& g, const SrcFields<T, NF>& src, const Epi& epi, int chunk,
+                                         const ZpMaps* maps) {
     using Z = ZV<T, NF, VX, TYH, RY, D>;
     constexpr int TX = Z::TX, TY = Z::TY, EPC = Z::EPC, OFF = Z::OFF, RS = Z::RS, SP = Z::SP, NS = Z::NS,
                   CH = Z::CH;
@@ -224,7 +238,9 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
     constexpr int NHAL = 2 * TY;                      // halo-column element copies
     using IO = VIO<T, VX>;
     extern __shared__ __align__(16) unsigned char zv_smem_raw[];
-    T* ring = reinterpret_cast<T*>(zv_smem_raw);      // [NS][NF][SP]
+    unsigned char* sbase = zv_smem_raw;
+    if constexpr (TMA) sbase += (128 - (smem_addr(zv_smem_raw) & 127)) & 127;
+    T* ring = reinterpret_cast<T*>(sbase);            // [NS][NF][SP]
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int wx = min(TX, g.mx - x0);
@@ -233,6 +249,20 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
     const int k1 = min(k0 + chunk, mz);
     const int cA = max(k0, 2), cB = min(k1 - 1, mz - 3);
     if (cA > cB) return;
+    // a CTA whose ring box lies inside the grid loads it by TMA (the TMA build)
+    const bool tma = TMA && x0 >= OFF && x0 + TX + OFF <= g.mx && y0 >= 1 && y0 + TY + 1 <= g.my;
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(ring + (size_t)NS * NF * SP);
+#ifdef DASHA_TMA
+    if constexpr (TMA) {
+        if (tid == 0)
+            for (int q = 0; q < NS; ++q) mbar_init(bars + q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        __syncthreads();
+    }
+#else
+    (void)bars;
+    (void)maps;
+#endif
     // this thread's copy slots (the same for every field and plane); -1 = none
     constexpr int NSL = (NVEC + NHAL + NT - 1) / NT;
     long gsrc[NSL];
@@ -259,6 +289,19 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
     }
     const int phi = cB + 1;
     auto issue = [&](int p) {
+#ifdef DASHA_TMA
+        if (tma) {
+            if (tid == 0 && p <= phi) {
+                T* stg = ring + (long)(p % NS) * NF * SP;
+                unsigned long long* bar = bars + p % NS;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // after the stage's generic reads
+                mbar_expect_tx(bar, (unsigned)(NF * RS * Z::NR * sizeof(T)));   // the boxes, not the padding
+#pragma unroll
+                for (int f = 0; f < NF; ++f) tma_load_3d(stg + f * SP, &maps->m[f], x0 - OFF, y0 - 1, p, bar);
+            }
+            return;
+        }
+#endif
         if (p <= phi) {
             T* stg = ring + (long)(p % NS) * NF * SP;
 #pragma unroll
@@ -308,8 +351,25 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
         for (int u = 0; u < RY; ++u)
             if (xon && gj[u] < g.my && DASHA_SPAN((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE))
                 epi.pre((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, pre[u]);
-        cp_async_wait<D>();
-        __syncthreads();
+#ifdef DASHA_TMA
+        if (tma) {
+            // planes c-1 .. c+1 on the first step, then c+1
+            bool late = false;
+            for (int p = primed ? c + 1 : c - 1; p <= c + 1; ++p)
+                if (!mbar_wait_bounded(bars + p % NS, (unsigned)(((p - (cA - 1)) / NS) & 1))) { late = true; break; }
+            if (__syncthreads_or(late)) {
+                // every box issued so far (planes up to c+1+D) lands before the CTA leaves
+                if (tid == 0) atomicExch(&g_wait_timeout, 1u);
+                for (int p = c - 1; p <= min(c + 1 + D, phi); ++p)
+                    if (p >= cA - 1) mbar_wait_bounded(bars + p % NS, (unsigned)(((p - (cA - 1)) / NS) & 1));
+                return;
+            }
+        } else
+#endif
+        {
+            cp_async_wait<D>();
+            __syncthreads();
+        }
         const T* pc = ring + (long)(c % NS) * NF * SP;
         const T* pp = ring + (long)((c + 1) % NS) * NF * SP;
         const int base = (w * RY + 1) * RS + OFF + xl;   // ring index of row u = 0, own first node
@@ -479,5 +539,18 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
     cp_async_wait<0>();
     if constexpr (has_finish<Epi>::value) epi.finish();   // the fused CFL maximum (WithCfl)
 }
+
+template <class T, int NF, unsigned KINDS, int VX, int TYH, int RY, int D, class Epi, int MODE = 0>
+__global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src, Epi epi, int chunk) {
+    zpv_body<T, NF, KINDS, VX, TYH, RY, D, Epi, MODE, false>(g, src, epi, chunk, nullptr);
+}
+
+#ifdef DASHA_TMA
+template <class T, int NF, unsigned KINDS, int VX, int TYH, int RY, int D, class Epi, int MODE = 0>
+__global__ void __launch_bounds__(32 * TYH) k_zpv_tma(Geo<T> g, SrcFields<T, NF> src, Epi epi, int chunk,
+                                                      const __grid_constant__ ZpMaps maps) {
+    zpv_body<T, NF, KINDS, VX, TYH, RY, D, Epi, MODE, true>(g, src, epi, chunk, &maps);
+}
+#endif
 
 }  // namespace dasha

@@ -3,10 +3,11 @@
     python -m dasha_b200.kernel_compare [--grid MX MY MZ] [--precision fp32|fp64] [--steps K]
                                         [--warmup W] [--check-grid MX MY MZ]
 
-The builds: the default library and the one whose hydro right-hand side (k_zhydro) loads its
-shared-memory ring by TMA (`-DDASHA_ZHYDRO_TMA`, built by __graft_entry__.build() as
-libdasha_zhtma.so).  Each runs the bench's seeded Harris/GEM run (sinh z grid, d_i = 1, whistler
-CFL; 1024x512x1024 by default) for W untimed and K timed steps: the step time by CUDA events
+The builds: the default library and the one whose smoothing passes (k_zpv) and hydro
+right-hand side (k_zhydro) load their shared-memory rings by TMA (`-DDASHA_TMA`, built by
+__graft_entry__.build() as libdasha_tma.so).  Each runs the bench's seeded Harris/GEM run (sinh
+z grid, d_i = 1, whistler CFL; 1024x512x1024 by default) for W untimed and K timed steps: the
+step time by CUDA events
 around the K steps, then the same K steps again with every launch bracketed by events for the
 time of each kernel tag.  The builds share the arithmetic, so their states must agree bit for
 bit: checked on a smaller grid (--check-grid) after 2 steps.  One JSON line on stdout.
@@ -21,7 +22,7 @@ import numpy as np
 
 from . import capi, harris
 
-BUILDS = {"default": capi.LIB_PATH, "hydro-tma": os.path.join(os.path.dirname(capi.LIB_PATH), "libdasha_zhtma.so")}
+BUILDS = {"default": capi.LIB_PATH, "tma": os.path.join(os.path.dirname(capi.LIB_PATH), "libdasha_tma.so")}
 
 
 def _cfg(grid, precision):
