@@ -108,8 +108,8 @@ static int bounds_status(dasha_ctx* c, int rc) {
 #else
 static int bounds_status(dasha_ctx*, int rc) { return rc; }
 #endif
-#ifdef DASHA_TMA
-// the TMA build: a bounded mbarrier wait of k_zhydro that ran out (the kernel returned early)
+#ifndef DASHA_NO_TMA
+// a bounded mbarrier wait of a TMA ring that ran out (the kernel returned early)
 static int wait_status(dasha_ctx* c, int rc) {
     if (!c || !c->st) return rc;
     unsigned int hit = 0;
@@ -118,7 +118,7 @@ static int wait_status(dasha_ctx* c, int rc) {
     if (!hit) return rc;
     const unsigned int zero = 0;
     cudaMemcpyToSymbol(g_wait_timeout, &zero, sizeof(zero));
-    return fail(c, DASHA_E_CUDA, "k_zhydro: a TMA ring wait ran out");
+    return fail(c, DASHA_E_CUDA, "a TMA ring wait ran out (k_zpv_tma / k_zhydro_tma)");
 }
 #else
 static int wait_status(dasha_ctx*, int rc) { return rc; }

@@ -135,7 +135,7 @@ EngineBase* make_engine_walls(int mx, int my, int mz, const dasha_params_c& p, c
         nvtxRangePop();                                                                        \
     } while (0)
 
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
@@ -606,7 +606,7 @@ public:
     using ZVc = ZV<T, NF, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D>;
     template <int NF, unsigned KINDS, class Epi, int MODE>
     static constexpr auto zpv_fn() { return k_zpv<T, NF, KINDS, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D, Epi, MODE>; }
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
     template <int NF, unsigned KINDS, class Epi, int MODE>
     static constexpr auto zpv_tma_fn() { return k_zpv_tma<T, NF, KINDS, ZVX, ZC<NF>::TYH, ZC<NF>::RY, ZC<NF>::D, Epi, MODE>; }
     // the source fields of a pass as tensor maps, boxes of one ring plane (RS x NR x 1)
@@ -628,6 +628,17 @@ public:
         return true;
     }
 #endif
+    // Ring loads by TMA where they measured faster on B200 (1024x512x1024 FP32, 512x256x512 FP64,
+    // bitwise the same states): every FP64 pass (4-9 % faster) and the FP64 hydro RHS (13 %); in
+    // FP32 the passes of 4 and 6 fields (the summed E/Hall pass 18 %, filter pass 1 14 %) and the
+    // hydro RHS (2 %), while the 3-field passes stay on cp.async (TMA 10 % slower there)
+#ifndef DASHA_NO_TMA
+    template <int NF>
+    static constexpr bool zp_tma() { return sizeof(T) == 8 || NF >= 4; }
+#else
+    template <int NF>
+    static constexpr bool zp_tma() { return false; }
+#endif
     // one smoothing pass of NF fields: src -> epi
     template <int NF, unsigned KINDS, int MODE = 0, class Epi>
     void zp(const char* tag, double bytes, const SrcFields<T, NF>& src, const Epi& epi) {
@@ -635,20 +646,23 @@ public:
         dim3 gg((mx + Z::TX - 1) / Z::TX, (my + Z::TY - 1) / Z::TY, 1);
         int ch = zchunk(gg.x * gg.y, 16);
         gg.z = (mz + ch - 1) / ch;
-#ifdef DASHA_TMA
-        ZpMaps maps;
-        if (!zpv_maps<NF>(src, maps)) launch_err = "cuTensorMapEncodeTiled failed for a smoothing pass";
-        DASHA_LAUNCH(tag, bytes, (zpv_tma_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem_tma(), st>>>(g, src, epi, ch, maps)));
-#else
-        DASHA_LAUNCH(tag, bytes, (zpv_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem(), st>>>(g, src, epi, ch)));
+#ifndef DASHA_NO_TMA
+        if constexpr (zp_tma<NF>()) {
+            ZpMaps maps;
+            if (!zpv_maps<NF>(src, maps)) launch_err = "cuTensorMapEncodeTiled failed for a smoothing pass";
+            DASHA_LAUNCH(tag, bytes, (zpv_tma_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem_tma(), st>>>(g, src, epi, ch, maps)));
+        } else
 #endif
+        {
+            DASHA_LAUNCH(tag, bytes, (zpv_fn<NF, KINDS, Epi, MODE>()<<<gg, 32 * ZC<NF>::TYH, Z::smem(), st>>>(g, src, epi, ch)));
+        }
     }
     template <int NF, unsigned KINDS, class Epi, int MODE = 0>
     static cudaError_t zp_attr1() {
-#ifdef DASHA_TMA
-        cudaError_t e = cudaFuncSetAttribute(zpv_tma_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)ZVc<NF>::smem_tma());
-        if (e) return e;
+#ifndef DASHA_NO_TMA
+        if constexpr (zp_tma<NF>())
+            return cudaFuncSetAttribute(zpv_tma_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)ZVc<NF>::smem_tma());
 #endif
         return cudaFuncSetAttribute(zpv_fn<NF, KINDS, Epi, MODE>(), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)ZVc<NF>::smem());
@@ -728,7 +742,7 @@ public:
         if ((e = cudaFuncSetAttribute(k_zhydro<T, ZH_VX, ZH_TY, 1, ZH_MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)ZHc::smem())))
             return e;
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
         if ((e = cudaFuncSetAttribute(k_zhydro_tma<T, ZH_VX, ZH_TY, 1, ZH_MINB>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ZHc::smem_tma())))
             return e;
@@ -867,7 +881,7 @@ public:
 
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
     const char* launch_err = nullptr;   // a launch that could not be set up (reported by stepon)
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
     // the five ring fields of k_zhydro as tensor maps, boxes of one ring plane (RS x NR x 1)
     bool hydro_maps(const HydroIO<T>& io, ZhMaps& m) {
         EncodeTiledFn enc = encode_tiled();
@@ -939,7 +953,7 @@ public:
             dim3 gh((mx + ZHc::TX - 1) / ZHc::TX, (my + ZH_TY - 1) / ZH_TY, 1);
             int chh = zchunk(gh.x * gh.y, 16);
             gh.z = (mz + chh - 1) / chh;
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
             ZhMaps maps;
             if (!hydro_maps(hio, maps)) launch_err = "cuTensorMapEncodeTiled failed for the hydro ring";
             DASHA_LAUNCH("k_rhs_hydro", 16.0 * N * sizeof(T),

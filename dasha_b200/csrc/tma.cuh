@@ -1,6 +1,7 @@
-// tma.cuh -- the pieces of the TMA comparison build (-DDASHA_TMA): ring planes of the z-marching
-// kernels loaded by `cp.async.bulk.tensor` against one mbarrier per ring stage, with waits that
-// give up after about a second (g_wait_timeout, reported by the C-ABI) instead of spinning.
+// tma.cuh -- ring planes of the z-marching kernels loaded by `cp.async.bulk.tensor` against one
+// mbarrier per ring stage, with waits that give up after about a second (g_wait_timeout,
+// reported by the C-ABI) instead of spinning.  Built unless -DDASHA_NO_TMA (the comparison build
+// whose rings all use cp.async).
 #pragma once
 
 #include <cuda.h>
@@ -9,7 +10,7 @@ namespace dasha {
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
 static __device__ unsigned int g_wait_timeout;    // a bounded mbarrier wait ran out
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");

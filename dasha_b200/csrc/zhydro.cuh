@@ -14,14 +14,14 @@
 // reads planes c-2 .. c+1 for the queue, so it holds planes c-2 .. c+2+D (hence D + 5 stages),
 // and ends with a second barrier.
 //
-// TMA (built with -DDASHA_TMA, for comparison): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1,
+// TMA (k_zhydro_tma; not built with -DDASHA_NO_TMA): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1,
 // rows y0-2 .. y0+TY+1) lies inside the grid loads each ring plane as 5 `cp.async.bulk.tensor`
 // boxes of exactly the ring plane's layout, issued by thread 0 against one mbarrier per stage;
 // every thread waits on the stage's mbarrier (time-bounded: after about a second the kernel
 // records g_wait_timeout, waits, again bounded, for the boxes it issued and returns) and turns
 // its share of the plane's rho - rho0 into 1/rho before the plane's barrier.  CTAs whose halo
 // wraps around x or y keep the cp.async element copies (a box cannot wrap).  The compute is the
-// same code in both builds.
+// same code in both kernels; the engine picks one.
 #pragma once
 
 #include <type_traits>
@@ -45,7 +45,7 @@ struct ZH {
     static constexpr int NS = D + 5;
     static constexpr int CH = TX / EPC;
     static constexpr size_t smem() { return sizeof(T) * (size_t)NS * NF * SP; }
-    // the TMA build: the ring 128-byte aligned, then one mbarrier per stage
+    // k_zhydro_tma: the ring 128-byte aligned, then one mbarrier per stage
     static constexpr size_t smem_tma() { return 128 + smem() + 8 * NS; }
 };
 
@@ -78,10 +78,10 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
     const int k1 = min(k0 + chunk, mz);
     const int cA = max(k0, 2), cB = min(k1 - 1, mz - 3);
     if (cA > cB) return;
-    // a CTA whose ring box lies inside the grid loads it by TMA (the TMA build)
+    // a CTA whose ring box lies inside the grid loads it by TMA (k_zhydro_tma)
     const bool tma = TMA && x0 >= OFF && x0 + TX + OFF <= g.mx && y0 >= 2 && y0 + TY + 2 <= g.my;
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(ring + (size_t)NS * NF * SP);
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
     if constexpr (TMA) {
         if (tid == 0)
             for (int q = 0; q < NS; ++q) mbar_init(bars + q, 1);
@@ -115,7 +115,7 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
     }
     const int phi = cB + 2;
     auto issue = [&](int p) {
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
         if (tma) {
             if (tid == 0 && p <= phi) {
                 T* stg = ring + (size_t)(p % NS) * NF * SP;
@@ -191,7 +191,7 @@ __device__ __forceinline__ void zhydro_body(const Geo<T>& g, const HydroIO<T>& i
             IO::ld(io.b1 + q, b1); IO::ld(io.b2 + q, b2); IO::ld(io.b3 + q, b3);
         }
         const T az = g.a1z[c], bz = g.b1z[c], cz = g.c1z[c], dz = g.d1z[c];
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
         if (tma) {
             // planes c-2 .. c+2 on the first step, then c+2: wait, then 1/rho over the plane
             bool late = false;
@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro(Geo<T> g, HydroIO<T> i
     zhydro_body<T, VX, TY, D, false>(g, io, chunk, nullptr);
 }
 
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
 template <class T, int VX, int TY, int D, int MINB = 1>
 __global__ void __launch_bounds__(32 * TY, MINB) k_zhydro_tma(Geo<T> g, HydroIO<T> io, int chunk,
                                                               const __grid_constant__ ZhMaps maps) {

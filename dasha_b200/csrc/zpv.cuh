@@ -15,11 +15,12 @@
 // per stage, measured 7-40 % slower per pass on B200 in every arrangement tried: the passes are
 // issue-bound and cp.async's per-thread copies cost about 2 % of their instructions.)
 //
-// TMA (built with -DDASHA_TMA, for comparison): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1, rows
+// TMA (k_zpv_tma; not built with -DDASHA_NO_TMA): a CTA whose ring box (x0-OFF .. x0+TX+OFF-1, rows
 // y0-1 .. y0+TY) lies inside the grid loads each ring plane as NF `cp.async.bulk.tensor` boxes of
 // exactly the ring plane's layout, issued by thread 0 against one mbarrier per stage; every thread
 // waits (time-bounded) on the stages it reads before the plane's barrier.  CTAs whose halo wraps
-// keep the cp.async copies.  The compute is the same code in both builds.
+// keep the cp.async copies.  The compute is the same code in both kernels; the engine picks one
+// per launch.
 //
 // KINDS: 2 bits per output field, 0 radial coefficient, 1 constant 1/8, 2 x-profile cbx.
 // MODE 0 writes the smoothed fields through the epilogue.  MODES 1 and 2 are the two passes of
@@ -35,7 +36,7 @@
 
 namespace dasha {
 
-// the source fields of a pass as 3-D tensor maps with the box of one ring plane (TMA build)
+// the source fields of a pass as 3-D tensor maps with the box of one ring plane (k_zpv_tma)
 struct ZpMaps { CUtensorMap m[8]; };
 
 // VX consecutive values of a field, one access (8-byte aligned float pairs in FP32)
@@ -221,7 +222,7 @@ struct ZV {
     static constexpr int NS = D + 3;                  // ring stages
     static constexpr int CH = TX / EPC;               // 16-byte copies per full row
     static constexpr size_t smem() { return sizeof(T) * (size_t)NS * NF * SP; }
-    // the TMA build: the ring 128-byte aligned, then one mbarrier per stage
+    // k_zpv_tma: the ring 128-byte aligned, then one mbarrier per stage
     static constexpr size_t smem_tma() { return 128 + smem() + 8 * NS; }
 };
 
@@ -249,10 +250,10 @@ __device__ __forceinline__ void zpv_body(const Geo<T>& g, const SrcFields<T, NF>
     const int k1 = min(k0 + chunk, mz);
     const int cA = max(k0, 2), cB = min(k1 - 1, mz - 3);
     if (cA > cB) return;
-    // a CTA whose ring box lies inside the grid loads it by TMA (the TMA build)
+    // a CTA whose ring box lies inside the grid loads it by TMA (k_zpv_tma)
     const bool tma = TMA && x0 >= OFF && x0 + TX + OFF <= g.mx && y0 >= 1 && y0 + TY + 1 <= g.my;
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(ring + (size_t)NS * NF * SP);
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
     if constexpr (TMA) {
         if (tid == 0)
             for (int q = 0; q < NS; ++q) mbar_init(bars + q, 1);
@@ -289,7 +290,7 @@ __device__ __forceinline__ void zpv_body(const Geo<T>& g, const SrcFields<T, NF>
     }
     const int phi = cB + 1;
     auto issue = [&](int p) {
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
         if (tma) {
             if (tid == 0 && p <= phi) {
                 T* stg = ring + (long)(p % NS) * NF * SP;
@@ -351,7 +352,7 @@ __device__ __forceinline__ void zpv_body(const Geo<T>& g, const SrcFields<T, NF>
         for (int u = 0; u < RY; ++u)
             if (xon && gj[u] < g.my && DASHA_SPAN((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, VX, g.sz * (long)g.mz, BS_ZPV_STORE))
                 epi.pre((long)gi + (long)gj[u] * g.sy + (long)c * g.sz, pre[u]);
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
         if (tma) {
             // planes c-1 .. c+1 on the first step, then c+1
             bool late = false;
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(32 * TYH) k_zpv(Geo<T> g, SrcFields<T, NF> src
     zpv_body<T, NF, KINDS, VX, TYH, RY, D, Epi, MODE, false>(g, src, epi, chunk, nullptr);
 }
 
-#ifdef DASHA_TMA
+#ifndef DASHA_NO_TMA
 template <class T, int NF, unsigned KINDS, int VX, int TYH, int RY, int D, class Epi, int MODE = 0>
 __global__ void __launch_bounds__(32 * TYH) k_zpv_tma(Geo<T> g, SrcFields<T, NF> src, Epi epi, int chunk,
                                                       const __grid_constant__ ZpMaps maps) {

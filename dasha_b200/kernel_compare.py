@@ -3,9 +3,10 @@
     python -m dasha_b200.kernel_compare [--grid MX MY MZ] [--precision fp32|fp64] [--steps K]
                                         [--warmup W] [--check-grid MX MY MZ]
 
-The builds: the default library and the one whose smoothing passes (k_zpv) and hydro
-right-hand side (k_zhydro) load their shared-memory rings by TMA (`-DDASHA_TMA`, built by
-__graft_entry__.build() as libdasha_tma.so).  Each runs the bench's seeded Harris/GEM run (sinh
+The builds: the default library (ring planes of the FP64 passes, the FP32 passes of 4 and 6
+fields and the hydro RHS loaded by TMA, the FP32 3-field passes by cp.async) and the one whose
+rings all use cp.async (`-DDASHA_NO_TMA`, built by __graft_entry__.build() as
+libdasha_cpasync.so).  Each runs the bench's seeded Harris/GEM run (sinh
 z grid, d_i = 1, whistler CFL; 1024x512x1024 by default) for W untimed and K timed steps: the
 step time by CUDA events
 around the K steps, then the same K steps again with every launch bracketed by events for the
@@ -22,7 +23,7 @@ import numpy as np
 
 from . import capi, harris
 
-BUILDS = {"default": capi.LIB_PATH, "tma": os.path.join(os.path.dirname(capi.LIB_PATH), "libdasha_tma.so")}
+BUILDS = {"default": capi.LIB_PATH, "cp.async": os.path.join(os.path.dirname(capi.LIB_PATH), "libdasha_cpasync.so")}
 
 
 def _cfg(grid, precision):
