@@ -632,7 +632,10 @@ public:
     // bitwise the same states): every FP64 pass (4-9 % faster) and the FP64 hydro RHS (13 %); in
     // FP32 the passes of 4 and 6 fields (the summed E/Hall pass 18 %, filter pass 1 14 %) and the
     // hydro RHS (2 %), while the 3-field passes stay on cp.async (TMA 10 % slower there)
-#ifndef DASHA_NO_TMA
+#if defined(DASHA_TMA_ALL)
+    template <int NF>
+    static constexpr bool zp_tma() { return true; }                  // measurement build: every pass
+#elif !defined(DASHA_NO_TMA)
     template <int NF>
     static constexpr bool zp_tma() { return sizeof(T) == 8 || NF >= 4; }
 #else
