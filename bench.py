@@ -225,12 +225,23 @@ KERNEL_OF = {
 }
 
 
-def by_kernel(prof):
+def kernel_of(tag, prec):
+    """The __global__ a tag launches: the smoothing passes and the hydro RHS load their rings by
+    TMA (k_zpv_tma, k_zhydro_tma) in FP64, and in FP32 for the passes of 4 and 6 fields."""
+    k = KERNEL_OF.get(tag, tag)
+    if k.startswith("k_zpv<") and (prec == "fp64" or not k.startswith("k_zpv<3 ")):
+        return "k_zpv_tma<" + k[len("k_zpv<"):]
+    if k == "k_zhydro":
+        return "k_zhydro_tma"
+    return k
+
+
+def by_kernel(prof, prec="fp32"):
     """Group the per-tag profile {tag: (ms, launches, bytes_per_launch)} by __global__:
     {kernel: {"ms", "launches", "bytes", "tags"}} with bytes the algorithmic total."""
     out = {}
     for tag, (ms, n, b) in prof.items():
-        k = KERNEL_OF.get(tag, tag)
+        k = kernel_of(tag, prec)
         e = out.setdefault(k, {"ms": 0.0, "launches": 0, "bytes": 0.0, "tags": []})
         e["ms"] += ms
         e["launches"] += n
@@ -342,7 +353,7 @@ def run_dasha(args, rank, world):
     d.profile(False)
     launches_per_step = sum(v[1] for v in prof.values())
     tot = sum(v[0] for v in prof.values())
-    kern = by_kernel(prof)
+    kern = by_kernel(prof, prec)
     dom_name, dom = max(kern.items(), key=lambda kv: kv[1]["ms"])
     dom_ms, dom_n = dom["ms"], dom["launches"]
     dom_bytes = dom["bytes"] / dom_n
