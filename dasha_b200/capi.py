@@ -83,6 +83,15 @@ SIGNATURES = {
     "dasha_dtlog_write": ([C.c_char_p, C.c_double, C.c_double, C.c_int], C.c_int),
     "dasha_m3d_write": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, _D, _D, _D,
                          C.c_long, C.c_long], C.c_int),
+    "dasha_slab_partition": ([C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "dasha_create_slab": ([C.POINTER(GridC), C.POINTER(ParamsC), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "dasha_slab_rows": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "dasha_slab_link": ([C.POINTER(C.c_void_p), C.c_int], C.c_int),
+    "dasha_group_setdt": ([C.POINTER(C.c_void_p), C.c_int, C.c_double, _D], C.c_int),
+    "dasha_group_stepon": ([C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_double, C.c_int], C.c_int),
+    "dasha_group_current": ([C.POINTER(C.c_void_p), C.c_int, C.POINTER(_D), C.c_long, C.c_long], C.c_int),
+    "dasha_nccl_unique_id": ([C.c_void_p, C.c_int], C.c_int),
+    "dasha_slab_nccl": ([_P, C.c_void_p, C.c_int], C.c_int),
     "dasha_last_error": ([_P], C.c_char_p),
     "dasha_destroy": ([_P], None),
 }

@@ -9,7 +9,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 #include <new>
 
@@ -64,6 +66,12 @@ struct dasha_ctx {
     bool bounded = false;     // periodic = {0,0,0}: the reference's bounded configuration
     double dt0 = 0.;
     bool have_dt0 = false;
+    // z-slab contexts (dasha_create_slab): slab `slab` of `nslabs`, own global rows zfirst ..,
+    // local planes = global rows zfirst-2 .. zfirst+mz-3, global grid mzg planes
+    int nslabs = 1, slab = 0, zfirst = 2, mzg = 0;
+    std::unique_ptr<Halo> halo;
+    std::shared_ptr<LocalGroup> group;   // the in-process group it was linked into
+    bool is_slab() const { return nslabs > 1; }
 };
 
 static int fail(dasha_ctx* c, int code, const std::string& msg) {
@@ -77,6 +85,20 @@ static int fail(dasha_ctx* c, int code, const std::string& msg) {
 #define CAPI_GUARD(ctx)                                                                       \
     if (!(ctx)) return DASHA_E_INVALID;                                                       \
     if ((ctx)->sticky) return (ctx)->sticky;
+
+// entry points over the whole grid (outputs, restart, adjoint) that a z-slab context refuses
+#define SLAB_UNSUPPORTED(c, what)                                                              \
+    if ((c)->is_slab()) return fail((c), DASHA_E_UNSUPPORTED, what " needs the whole grid: not on a z-slab context");
+
+// a z-slab's own setdt / stepon / current: a slab of a one-process-per-GPU run (dasha_slab_nccl);
+// the slabs of one process step together through the dasha_group_* calls
+static int slab_single_call(dasha_ctx* c) {
+    if (!c->is_slab()) return DASHA_OK;
+    if (!c->halo) return fail(c, DASHA_E_STATE, "z-slab not joined to its neighbours (dasha_slab_link or dasha_slab_nccl)");
+    if (!c->halo->per_process())
+        return fail(c, DASHA_E_STATE, "linked slabs step together: dasha_group_setdt / dasha_group_stepon / dasha_group_current");
+    return DASHA_OK;
+}
 
 static int from_status(dasha_ctx* c, const Status& s) {
     if (s.code == DASHA_OK) return DASHA_OK;
@@ -143,7 +165,32 @@ static int engine_call(dasha_ctx* c, F call) {
 
 extern "C" {
 
+static int create_ctx(const dasha_grid_c* grid, const dasha_params_c* params, int nslabs, int slab, dasha_ctx** out);
+
 int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_ctx** out) {
+    return create_ctx(grid, params, 1, 0, out);
+}
+
+int dasha_slab_partition(int mz, int nslabs, int slab, int* first, int* count) {
+    SlabPart sp;
+    if (!first || !count || !slab_partition(mz, nslabs, slab, sp)) return DASHA_E_INVALID;
+    *first = sp.first;
+    *count = sp.count;
+    return DASHA_OK;
+}
+
+int dasha_create_slab(const dasha_grid_c* grid, const dasha_params_c* params, int nslabs, int slab, dasha_ctx** out) {
+    if (!out) return DASHA_E_INVALID;
+    *out = nullptr;
+    if (!grid || !params) return DASHA_E_INVALID;
+    if (grid->periodic[0] == 0 && grid->periodic[1] == 0 && grid->periodic[2] == 0)
+        return DASHA_E_UNSUPPORTED;   // the bounded configuration runs on one context
+    SlabPart sp;
+    if (!slab_partition(grid->mz, nslabs, slab, sp)) return DASHA_E_INVALID;
+    return create_ctx(grid, params, nslabs, slab, out);
+}
+
+static int create_ctx(const dasha_grid_c* grid, const dasha_params_c* params, int nslabs, int slab, dasha_ctx** out) {
     if (!out) return DASHA_E_INVALID;
     *out = nullptr;
     if (!grid || !params || !grid->x || !grid->y || !grid->z) return DASHA_E_INVALID;
@@ -217,6 +264,20 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
         H.cbx.assign(c->mx, 0.0);
         for (int i = 0; i < c->mx; ++i) H.cbx[i] = (1.0 / 32.0) * (1.0 - std::tanh((c->ax.c[i] + 3.0) / 8.0));
 
+        if (nslabs > 1) {   // a z-slab: the local planes of every z table, the global grid's values
+            SlabPart sp;
+            slab_partition(c->mz, nslabs, slab, sp);
+            const int z0 = sp.first - 2, mzl = sp.count + 4;
+            auto cut = [&](std::vector<double>& v) { v = std::vector<double>(v.begin() + z0, v.begin() + z0 + mzl); };
+            for (int q = 0; q < 8; ++q) cut(H.coef[2][q]);
+            cut(H.wp[2]); cut(H.wm[2]); cut(H.spacing[2]); cut(H.weight[2]); cut(H.coord[2]);
+            cut(c->az.c);
+            c->nslabs = nslabs; c->slab = slab; c->zfirst = sp.first; c->mzg = c->mz;
+            c->mz = mzl; c->az.n = mzl; H.mz = mzl;
+            c->N = (long)c->mx * c->my * c->mz;
+        } else {
+            c->mzg = c->mz;
+        }
         Status s;
         if (bounded) c->eng = make_engine_walls(c->mx, c->my, c->mz, p, c->st, grid->x, grid->y, grid->z, s);
         else if (p.precision == 0) c->eng = make_engine_f64(c->mx, c->my, c->mz, p, c->st, H, s);
@@ -234,22 +295,33 @@ int dasha_create(const dasha_grid_c* grid, const dasha_params_c* params, dasha_c
         delete c;
         return DASHA_E_NOMEM;
     }
+    if (c->slab > 0) c->eng->set_cfl_k0(2);   // planes 0 and 1 are the slab below's
     *out = c;
     return DASHA_OK;
 }
 
 void dasha_destroy(dasha_ctx* c) {
     if (!c) return;
+    if (c->group) c->group->members[c->slab] = nullptr;
     if (c->eng) { cudaStreamSynchronize(c->st); delete c->eng; }
+    c->halo.reset();
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }
 
 const char* dasha_last_error(dasha_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
-int dasha_set_equilibrium(dasha_ctx* c, const double* rho0, const double* b0, const double* p0) {
-    CAPI_GUARD(c);
-    if (!rho0 || !b0 || !p0) return fail(c, DASHA_E_INVALID, "null equilibrium profile");
+// a z-slab takes the global grid's profiles (nprof arrays of mzg values, one after another)
+// and keeps its own planes
+static std::vector<double> slab_profiles(const dasha_ctx* c, const double* f, int nprof) {
+    std::vector<double> v((size_t)nprof * c->mz);
+    for (int m = 0; m < nprof; ++m)
+        for (int k = 0; k < c->mz; ++k) v[(size_t)m * c->mz + k] = f[(size_t)m * c->mzg + (c->zfirst - 2) + k];
+    return v;
+}
+
+// the profiles of the context's own planes
+static int set_equilibrium_local(dasha_ctx* c, const double* rho0, const double* b0, const double* p0) {
     for (int k = 0; k < c->mz; ++k)
         if (!(rho0[k] > 0.0)) return fail(c, DASHA_E_INVALID, "rho0 must be positive");
     try {
@@ -260,8 +332,19 @@ int dasha_set_equilibrium(dasha_ctx* c, const double* rho0, const double* b0, co
     } catch (...) { return fail(c, DASHA_E_NOMEM, "host allocation failed"); }
 }
 
+int dasha_set_equilibrium(dasha_ctx* c, const double* rho0, const double* b0, const double* p0) {
+    CAPI_GUARD(c);
+    if (!rho0 || !b0 || !p0) return fail(c, DASHA_E_INVALID, "null equilibrium profile");
+    if (!c->is_slab()) return set_equilibrium_local(c, rho0, b0, p0);
+    return host_call(c, [&] {
+        const std::vector<double> r = slab_profiles(c, rho0, 1), b = slab_profiles(c, b0, 3), q = slab_profiles(c, p0, 1);
+        return set_equilibrium_local(c, r.data(), b.data(), q.data());
+    });
+}
+
 int dasha_set_equilibrium_3d(dasha_ctx* c, const double* eq_f, long ld1, long ld2) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_set_equilibrium_3d");
     if (!eq_f || ld1 < c->mx + 4 || ld2 < c->my) return fail(c, DASHA_E_INVALID, "bad equilibrium arguments");
     const int rc = engine_call(c, [&] { return c->eng->set_equilibrium_3d(eq_f, ld1, ld2); });
     if (rc == DASHA_OK) c->eq_set = true;
@@ -273,6 +356,12 @@ int dasha_set_equilibrium_current(dasha_ctx* c, const double* j0) {
     CAPI_GUARD(c);
     if (!j0) return fail(c, DASHA_E_INVALID, "null j0");
     if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium first");
+    if (c->is_slab()) {
+        return host_call(c, [&] {
+            const std::vector<double> v = slab_profiles(c, j0, 3);
+            return from_status(c, c->eng->set_j0(v.data()));
+        });
+    }
     return engine_call(c, [&] { return c->eng->set_j0(j0); });
 }
 
@@ -320,6 +409,7 @@ static void pack_state_header(unsigned char* h, const dasha_ctx* c, int nf, int 
 int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, double time, int nst,
                      long max_subrecord) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_checkpoint");
     if (!path || max_subrecord < 0) return fail(c, DASHA_E_INVALID, "bad checkpoint arguments");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return host_call(c, [&]() -> int {
@@ -370,6 +460,7 @@ int dasha_checkpoint(dasha_ctx* c, const char* path, int ncase, int nstep, doubl
 
 int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double* time, int* nst) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_restore");
     if (!path || !ncase || !nstep || !time || !nst) return fail(c, DASHA_E_INVALID, "bad restore arguments");
     if (!c->eq_set) return fail(c, DASHA_E_STATE, "set the equilibrium before the state");
     bool touched = false;   // set once the device state starts to change
@@ -434,6 +525,7 @@ int dasha_restore(dasha_ctx* c, const char* path, int* ncase, int* nstep, double
 
 int dasha_stream_out(dasha_ctx* c, int what, dasha_chunk_fn fn, void* user) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_stream_out");
     if (!fn || (what != 0 && what != 1)) return fail(c, DASHA_E_INVALID, "bad stream arguments");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return engine_call(c, [&] {
@@ -447,6 +539,7 @@ int dasha_stream_out(dasha_ctx* c, int what, dasha_chunk_fn fn, void* user) {
 // next chunk's transfer runs; the text equals dasha_m3d_write of the get_state / current arrays.
 int dasha_m3d_write_ctx(dasha_ctx* c, const char* path, double time) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_m3d_write_ctx");
     if (!path) return fail(c, DASHA_E_INVALID, "null path");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return host_call(c, [&]() -> int {
@@ -491,8 +584,18 @@ int dasha_m3d_write_ctx(dasha_ctx* c, const char* path, double time) {
     });
 }
 
+// the reference's two stop conditions of the step loop on a new dt (t3dsdsc.f:142-154, 1232)
+static int setdt_guards(dasha_ctx* c, double dt, int blowup) {
+    if (blowup) return fail(c, DASHA_E_BLOWUP, "max Jy on the mid-y plane reached 1e7 (or is not finite)");
+    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DASHA_E_DT_COLLAPSE, "dt is not a positive finite number");
+    if (!c->have_dt0) { c->dt0 = dt; c->have_dt0 = true; }
+    else if (dt < 0.1 * c->dt0) return fail(c, DASHA_E_DT_COLLAPSE, "dt fell below 0.1*dt0");
+    return DASHA_OK;
+}
+
 int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {
     CAPI_GUARD(c);
+    if (int rc = slab_single_call(c)) return rc;
     (void)time;
     if (!dt_out) return fail(c, DASHA_E_INVALID, "null dt_out");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
@@ -501,15 +604,12 @@ int dasha_setdt(dasha_ctx* c, double time, double* dt_out) {
     int rc = engine_call(c, [&] { return c->eng->setdt(&dt, &blowup); });
     if (rc) return rc;
     *dt_out = dt;
-    if (blowup) return fail(c, DASHA_E_BLOWUP, "max Jy on the mid-y plane reached 1e7 (or is not finite)");
-    if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DASHA_E_DT_COLLAPSE, "dt is not a positive finite number");
-    if (!c->have_dt0) { c->dt0 = dt; c->have_dt0 = true; }
-    else if (dt < 0.1 * c->dt0) return fail(c, DASHA_E_DT_COLLAPSE, "dt fell below 0.1*dt0");
-    return DASHA_OK;
+    return setdt_guards(c, dt, blowup);
 }
 
 int dasha_stepon(dasha_ctx* c, double time, double dt, int nstep) {
     CAPI_GUARD(c);
+    if (int rc = slab_single_call(c)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     if (!(dt > 0.0) || !std::isfinite(dt)) return fail(c, DASHA_E_INVALID, "dt must be positive and finite");
     return engine_call(c, [&] { return c->eng->stepon(time, dt, nstep); });
@@ -517,6 +617,7 @@ int dasha_stepon(dasha_ctx* c, double time, double dt, int nstep) {
 
 int dasha_current(dasha_ctx* c, double* cur_f, long ld1, long ld2) {
     CAPI_GUARD(c);
+    if (int rc = slab_single_call(c)) return rc;
     if (int rc = check_ld(c, cur_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return engine_call(c, [&] { return c->eng->current(cur_f, ld1, ld2); });
@@ -524,6 +625,7 @@ int dasha_current(dasha_ctx* c, double* cur_f, long ld1, long ld2) {
 
 int dasha_midplane(dasha_ctx* c, double* plane) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_midplane");
     if (!plane) return fail(c, DASHA_E_INVALID, "null plane");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return engine_call(c, [&] { return c->eng->midplane(plane); });
@@ -531,6 +633,7 @@ int dasha_midplane(dasha_ctx* c, double* plane) {
 
 int dasha_rhs(dasha_ctx* c, double t, double* xdif_f, long ld1, long ld2) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_rhs");
     if (int rc = check_ld(c, xdif_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return engine_call(c, [&] { return c->eng->rhs(t, xdif_f, ld1, ld2); });
@@ -538,6 +641,7 @@ int dasha_rhs(dasha_ctx* c, double t, double* xdif_f, long ld1, long ld2) {
 
 int dasha_diagnostics(dasha_ctx* c, double* out) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_diagnostics");
     if (!out) return fail(c, DASHA_E_INVALID, "null out");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return engine_call(c, [&] { return c->eng->diagnostics(out); });
@@ -546,6 +650,7 @@ int dasha_diagnostics(dasha_ctx* c, double* out) {
 int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int snaps, double* dPhi_deta,
                             double* dPhi_dpsi) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_adjoint_flux_grad");
     if (nsteps < 0 || (nsteps > 0 && !dt_seq) || snaps < 0 || !dPhi_deta || !dPhi_dpsi)
         return fail(c, DASHA_E_INVALID, "bad adjoint arguments");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
@@ -555,6 +660,7 @@ int dasha_adjoint_flux_grad(dasha_ctx* c, int nsteps, const double* dt_seq, int 
 
 int dasha_adjoint_rhs(dasha_ctx* c, const double* w_f, double* out_f, long ld1, long ld2) {
     CAPI_GUARD(c);
+    SLAB_UNSUPPORTED(c, "dasha_adjoint_rhs");
     if (int rc = check_ld(c, w_f, ld1, ld2)) return rc;
     if (int rc = check_ld(c, out_f, ld1, ld2)) return rc;
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
@@ -611,6 +717,165 @@ int dasha_profile_read(dasha_ctx* c, int* n, char* names, double* ms, long* laun
     p.recs.clear();
     p.used = 0;
     return DASHA_OK;
+}
+
+// ---- z-slab groups (halo.h) ----
+
+int dasha_slab_rows(dasha_ctx* c, int* first, int* count, int* mz_local) {
+    CAPI_GUARD(c);
+    if (!first || !count || !mz_local) return fail(c, DASHA_E_INVALID, "null argument");
+    *first = c->zfirst;
+    *count = c->mz - 4;
+    *mz_local = c->mz;
+    return DASHA_OK;
+}
+
+}  // extern "C"
+
+// the slab s of every context is ctxs[s]: one grid, parameters and precision
+static int check_group(dasha_ctx* const* cs, int n) {
+    if (!cs || n < 2) return DASHA_E_INVALID;
+    for (int s = 0; s < n; ++s) {
+        const dasha_ctx* c = cs[s];
+        if (!c || c->nslabs != n || c->slab != s || c->mx != cs[0]->mx || c->my != cs[0]->my ||
+            c->mzg != cs[0]->mzg || c->P.precision != cs[0]->P.precision)
+            return DASHA_E_INVALID;
+        if (c->sticky) return c->sticky;
+    }
+    return DASHA_OK;
+}
+
+// runs body(ctx, s) for every slab of a linked group, one host thread per slab with its device
+// current; a slab that fails releases the others from the group's barriers
+template <class F>
+static int group_run(dasha_ctx* const* cs, int n, F body);
+
+extern "C" {
+
+int dasha_slab_link(dasha_ctx* const* cs, int n) {
+    if (int rc = check_group(cs, n)) return rc;
+    for (int s = 0; s < n; ++s)
+        if (cs[s]->halo) return fail(cs[s], DASHA_E_STATE, "slab already joined to a group");
+    try {
+        auto grp = std::make_shared<LocalGroup>(n);
+        std::vector<std::unique_ptr<Halo>> hs;
+        for (int s = 0; s < n; ++s) {
+            auto h = std::make_unique<HaloLocal>(grp);
+            h->geo = cs[s]->eng->slab_geom();
+            h->geo.n = n; h->geo.s = s; h->geo.device = cs[s]->device;
+            hs.push_back(std::move(h));
+        }
+        for (int s = 0; s < n; ++s) {
+            grp->members[s] = &hs[s]->geo;
+            cs[s]->halo = std::move(hs[s]);
+            cs[s]->eng->halo = cs[s]->halo.get();
+            cs[s]->group = grp;
+        }
+    } catch (...) {
+        return DASHA_E_NOMEM;
+    }
+    return DASHA_OK;
+}
+
+}  // extern "C"
+
+template <class F>
+static int group_run(dasha_ctx* const* cs, int n, F body) {
+    if (int rc = check_group(cs, n)) return rc;
+    std::shared_ptr<LocalGroup> grp = cs[0]->group;
+    for (int s = 0; s < n; ++s)
+        if (!cs[s]->group || cs[s]->group != grp) return fail(cs[s], DASHA_E_STATE, "slabs not linked as one group");
+    grp->bar.reset();
+    std::vector<int> rc(n, DASHA_OK);
+    try {
+        std::vector<std::thread> th;
+        for (int s = 0; s < n; ++s)
+            th.emplace_back([&, s] {
+                if (cudaSetDevice(cs[s]->device) != cudaSuccess) rc[s] = fail(cs[s], DASHA_E_CUDA, "cudaSetDevice failed");
+                else rc[s] = body(cs[s], s);
+                if (rc[s]) grp->bar.fail();
+            });
+        for (auto& t : th) t.join();
+    } catch (...) {
+        grp->bar.fail();
+        return DASHA_E_NOMEM;
+    }
+    for (int s = 0; s < n; ++s)   // the first slab's own failure, not the others' release
+        if (rc[s] && cs[s]->halo && cs[s]->err.find("halo exchange") == std::string::npos) return rc[s];
+    for (int s = 0; s < n; ++s)
+        if (rc[s]) return rc[s];
+    return DASHA_OK;
+}
+
+extern "C" {
+
+int dasha_group_setdt(dasha_ctx* const* cs, int n, double time, double* dt_out) {
+    (void)time;
+    if (!dt_out) return DASHA_E_INVALID;
+    if (int rc = check_group(cs, n)) return rc;
+    for (int s = 0; s < n; ++s)
+        if (!cs[s]->state_set) return fail(cs[s], DASHA_E_STATE, "no state set");
+    std::vector<double> dt(n, 0.0);
+    std::vector<int> bl(n, 0);
+    int rc = group_run(cs, n, [&](dasha_ctx* c, int s) { return engine_call(c, [&] { return c->eng->setdt(&dt[s], &bl[s]); }); });
+    if (rc) return rc;
+    double d = dt[0];
+    int b = bl[0];
+    for (int s = 1; s < n; ++s) {   // the smallest dt (a NaN wins), any blow-up
+        d = (d != d || dt[s] != dt[s]) ? (d != d ? d : dt[s]) : std::fmin(d, dt[s]);
+        b |= bl[s];
+    }
+    *dt_out = d;
+    for (int s = 1; s < n; ++s) { cs[s]->have_dt0 = cs[0]->have_dt0; cs[s]->dt0 = cs[0]->dt0; }
+    rc = setdt_guards(cs[0], d, b);
+    for (int s = 1; s < n; ++s) { cs[s]->have_dt0 = cs[0]->have_dt0; cs[s]->dt0 = cs[0]->dt0; }
+    return rc;
+}
+
+int dasha_group_stepon(dasha_ctx* const* cs, int n, double time, double dt, int nstep) {
+    if (int rc = check_group(cs, n)) return rc;
+    if (!(dt > 0.0) || !std::isfinite(dt)) return DASHA_E_INVALID;
+    for (int s = 0; s < n; ++s)
+        if (!cs[s]->state_set) return fail(cs[s], DASHA_E_STATE, "no state set");
+    return group_run(cs, n, [&](dasha_ctx* c, int) { return engine_call(c, [&] { return c->eng->stepon(time, dt, nstep); }); });
+}
+
+int dasha_group_current(dasha_ctx* const* cs, int n, double* const* cur_f, long ld1, long ld2) {
+    if (int rc = check_group(cs, n)) return rc;
+    if (!cur_f) return DASHA_E_INVALID;
+    for (int s = 0; s < n; ++s) {
+        if (int rc = check_ld(cs[s], cur_f[s], ld1, ld2)) return rc;
+        if (!cs[s]->state_set) return fail(cs[s], DASHA_E_STATE, "no state set");
+    }
+    return group_run(cs, n, [&](dasha_ctx* c, int s) { return engine_call(c, [&] { return c->eng->current(cur_f[s], ld1, ld2); }); });
+}
+
+int dasha_nccl_unique_id(void* id, int nbytes) {
+    if (!id || nbytes < (int)sizeof(ncclUniqueId)) return DASHA_E_INVALID;
+    const NcclApi& a = NcclApi::get();
+    if (!a.ok()) return DASHA_E_UNSUPPORTED;
+    ncclUniqueId u;
+    if (a.get_unique_id(&u) != ncclSuccess) return DASHA_E_CUDA;
+    std::memcpy(id, &u, sizeof(u));
+    return DASHA_OK;
+}
+
+int dasha_slab_nccl(dasha_ctx* c, const void* id, int nbytes) {
+    CAPI_GUARD(c);
+    if (!id || nbytes < (int)sizeof(ncclUniqueId)) return fail(c, DASHA_E_INVALID, "the NCCL id is 128 bytes");
+    if (c->halo) return fail(c, DASHA_E_STATE, "slab already joined");
+    return host_call(c, [&] {
+        auto h = std::make_unique<HaloNccl>();
+        h->geo = c->eng->slab_geom();
+        h->geo.n = c->nslabs; h->geo.s = c->slab; h->geo.device = c->device;
+        ncclUniqueId u;
+        std::memcpy(&u, id, sizeof(u));
+        if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, DASHA_E_CUDA, "cudaSetDevice failed");
+        if (!h->init(u)) return fail(c, NcclApi::get().ok() ? DASHA_E_CUDA : DASHA_E_UNSUPPORTED, h->err);
+        c->halo = std::move(h);
+        c->eng->halo = c->halo.get();
+        return (int)DASHA_OK;
+    });
 }
 
 }  // extern "C"

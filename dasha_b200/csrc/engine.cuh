@@ -11,6 +11,7 @@
 #include "zeh.cuh"
 #include "adjoint.cuh"
 #include "checkpoint_schedule.h"
+#include "halo.h"
 #include "host_pool.h"
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
@@ -80,6 +81,11 @@ using ChunkOut = std::function<bool(int m, int k0, int k1, const double* rows)>;
 struct EngineBase {
     Profiler prof;
     cudaEvent_t t0 = nullptr, t1 = nullptr;
+    // z-slab contexts (halo.h): the ghost-plane exchange, owned by the context; null otherwise
+    Halo* halo = nullptr;
+    // the slab's pool layout for the exchange, and the first plane of its setdt region
+    virtual SlabGeom slab_geom() const { return SlabGeom(); }
+    virtual void set_cfl_k0(int) {}
     virtual ~EngineBase() {
         if (t0) cudaEventDestroy(t0);
         if (t1) cudaEventDestroy(t1);
@@ -200,6 +206,27 @@ public:
     bool j0_given = false;
     long nred = 0;
     dim3 blk, grd;
+    size_t pool_fbytes = 0;      // bytes per field in the pool (256-byte multiple)
+    std::string halo_err;        // the last failed ghost-plane exchange
+
+    SlabGeom slab_geom() const override {
+        SlabGeom sg;
+        sg.mzl = mz; sg.sz = (long)mx * my; sg.elem = sizeof(T); sg.st = st;
+        sg.pool = pool; sg.fbytes = pool_fbytes;
+        return sg;
+    }
+    void set_cfl_k0(int k0) override { g.kcfl0 = k0; }
+    // z-slab contexts: refresh the ghost planes of fields f that a later launch reads at
+    // z-neighbours (a no-op on a whole-grid context)
+    void hx(T* const* f, int nf) {
+        if (!halo) return;
+        void* v[16];
+        for (int q = 0; q < nf; ++q) v[q] = f[q];
+        if (!halo->exchange(v, nf) && !launch_err) {
+            halo_err = "halo exchange: " + halo->err;
+            launch_err = halo_err.c_str();
+        }
+    }
 
     ~Engine() override {
         xbuf_free();
@@ -223,6 +250,7 @@ public:
         if ((double)fbytes * nfield > 0.97 * (double)freeb)
             return Status::err(DASHA_E_NOMEM, "grid needs " + std::to_string((double)fbytes * nfield / 1e9) +
                                                   " GB of device memory, " + std::to_string(freeb / 1e9) + " GB free");
+        pool_fbytes = fbytes;
         cudaError_t e = cudaMalloc(&pool, fbytes * nfield);
         if (e != cudaSuccess) { pool = nullptr; cudaGetLastError(); return Status::err(DASHA_E_NOMEM, "cudaMalloc of the field pool failed"); }
         char* q = (char*)pool;
@@ -816,6 +844,7 @@ public:
         T* t[8];
         tmp8(t);
         pass8("k_zpv_X", 16.0, k, [&](int lo) { return st4(t, lo); });
+        hx(t, 8);
         auto mk = [&](int lo) {
             RK4 er;
             for (int m = 0; m < 4; ++m) {
@@ -827,6 +856,7 @@ public:
             return er;
         };
         pass8(names[stage - 1], 8.0 * (1.0 + rk_io(stage)), t, mk);
+        if (stage < 4) hx(x, 8);   // the next stage's state
     }
 
     // avrgtt on the compensated FP32 state (X, C): pass 1 writes its increment of X - C into
@@ -841,6 +871,7 @@ public:
             else if (lo == 4) zp<4, KIND_P45, 1>("k_zpv_F1", by, a, o);
             else zp<4, KIND_P67, 1>("k_zpv_F1", by, a, o);
         }
+        hx(t, 8);
         for (int lo = 0; lo < 8; lo += 4) {
             SrcFields<T, 4> d;
             VKF<T, 4, ZVX> e;
@@ -855,7 +886,11 @@ public:
     T** Ef = nullptr;     // total E after launch_rhs_raw
 
     // n smoothing passes of 3 fields, ping-pong between a and b starting from a; returns the
-    // buffer holding the result.
+    // buffer holding the result.  On a z-slab every pass output that a later pass reads has its
+    // ghost planes refreshed, the last one too when xlast (a later launch reads it at
+    // z-neighbours), and the Hall pairs run as single passes: k_zpv2 forms its first pass on the
+    // planes next to the slab ends from the wall rule.  Both give the same values: the fused
+    // pair rounds as two single passes.
     // Pass pairs of the Hall chain (constant coefficient 1/8) run fused in k_zpv2.  Measured on
     // B200 (FP32 1024x512x1024 / FP64 512x256x512 step): Hall pairs fused 436.0 / 107.7 ms,
     // nothing fused 442.1 / 108.4; fusing the radial-coefficient chains J and E as well 437.3 /
@@ -863,23 +898,25 @@ public:
     // 114.1: where the coefficient is evaluated per node, or the epilogue is heavy, the doubled
     // per-node work and the lower occupancy of the 320-thread CTA outweigh the saved traffic.
     template <unsigned KINDS>
-    T** passes3(const char* tag, T** a, T** b, int n) {
+    T** passes3(const char* tag, T** a, T** b, int n, bool xlast) {
         if constexpr (KINDS == KIND_H) {
-            for (int p = 0; p < n; p += 2) {   // pairs of passes in one k_zpv2 launch, a lone last one by k_zpv
-                T** in = ((p / 2) & 1) ? b : a;
-                T** out = ((p / 2) & 1) ? a : b;
-                if (p + 1 < n) zp2<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
-                else zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+            if (!halo) {
+                for (int p = 0; p < n; p += 2) {   // pairs of passes in one k_zpv2 launch, a lone last one by k_zpv
+                    T** in = ((p / 2) & 1) ? b : a;
+                    T** out = ((p / 2) & 1) ? a : b;
+                    if (p + 1 < n) zp2<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+                    else zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+                }
+                return (((n + 1) / 2) & 1) ? b : a;
             }
-            return (((n + 1) / 2) & 1) ? b : a;
-        } else {
-            for (int p = 0; p < n; ++p) {
-                T** in = (p & 1) ? b : a;
-                T** out = (p & 1) ? a : b;
-                zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
-            }
-            return (n & 1) ? b : a;
         }
+        for (int p = 0; p < n; ++p) {
+            T** in = (p & 1) ? b : a;
+            T** out = (p & 1) ? a : b;
+            zp<3, KINDS>(tag, 6.0 * N * sizeof(T), src3(in), st3(out));
+            if (p < n - 1 || xlast) hx(out, 3);
+        }
+        return (n & 1) ? b : a;
     }
 
     // smoothed current of state xs (current, t3dsdsc.f:2452-2500): curl, 4 passes
@@ -906,7 +943,8 @@ public:
     void launch_current(T* const* xs) {
         T* bb[3] = {xs[4], xs[5], xs[6]};
         zcurl<1>("k_curl", src3(bb), f3(cur[0]));
-        curF = passes3<0u>("k_zpv_J", cur[0], cur[1], 4);
+        hx(cur[0], 3);
+        curF = passes3<0u>("k_zpv_J", cur[0], cur[1], 4, false);
         if (P.j0_mode == 1) DASHA_LAUNCH("k_add_j0", 6.0 * N * sizeof(T), k_add_j0<T><<<grd, blk, 0, st>>>(g, f3(curF)));
     }
 
@@ -927,22 +965,25 @@ public:
             int che = zchunk(ge.x * ge.y, 16);
             ge.z = (mz + che - 1) / che;
             DASHA_LAUNCH("k_efield_hall", 17.0 * N * sizeof(T), (k_zeh<T, ZVX, 8, 2><<<ge, 256, ZEHc::smem(), st>>>(g, eh, che)));
+            hx(Hh[0], 3);
         } else {
             DASHA_LAUNCH("k_efield", 13.0 * N * sizeof(T), k_efield<T><<<grd, blk, 0, st>>>(g, f8(xs), f3(curF), f3(E[0])));
         }
+        hx(E[0], 3);
         if (P.hall) {
             // avrgh passes 1-4, avrgE passes 1-3, then one 6-field launch: the 4th E pass and the
             // 5th Hall pass, summed into E (the two chains are independent until that sum)
-            T** h = passes3<KIND_H>("k_zpv_H", Hh[0], Hh[1], 4);
-            T** e3 = passes3<0u>("k_zpv_E", E[0], E[1], 3);
+            T** h = passes3<KIND_H>("k_zpv_H", Hh[0], Hh[1], 4, true);
+            T** e3 = passes3<0u>("k_zpv_E", E[0], E[1], 3, true);
             T** eo = e3 == E[0] ? E[1] : E[0];
             SrcFields<T, 6> se;
             VSum<T, 3, ZVX> es;
             for (int q = 0; q < 3; ++q) { se.f[q] = e3[q]; se.f[3 + q] = h[q]; es.f[q] = eo[q]; }
             zp<6, KIND_EH>("k_zpv_EH", 9.0 * N * sizeof(T), se, es);
             Ef = eo;
+            hx(Ef, 3);
         } else {
-            Ef = passes3<0u>("k_zpv_E", E[0], E[1], 4);
+            Ef = passes3<0u>("k_zpv_E", E[0], E[1], 4, true);
         }
         // right-hand side: hydro part (xdif 0..3, 7) and induction (xdif 4..6)
         dim3 gg(mx / ZTX, (my + 7) / 8, 1);
@@ -976,6 +1017,7 @@ public:
         }
         T* kb[3] = {K[4], K[5], K[6]};
         zcurl<-1>("k_rhs_induction", src3(Ef), f3(kb));
+        hx(K, 8);
     }
     // 8 scratch fields that are free once the RHS is written
     void tmp8(T** t) {
@@ -1007,7 +1049,10 @@ public:
         // its own sweep).
         const int every = P.filter_every > 0 ? P.filter_every : 1;
         const bool filt = nstep % every == 0;
+        // a z-slab takes setdt's rate by its own sweep (the tap would also read the ghost planes)
+        const bool tap = !halo;
         rate_ok = false;
+        hx(X, 8);
         for (int stage = 1; stage <= 4; ++stage) {
             launch_rhs_raw(stage == 1 ? X : S);
             rk_passes(stage, dt, K, X, S, A, KAHAN ? C : nullptr);
@@ -1016,18 +1061,23 @@ public:
         if (filt) {   // avrgtt on the perturbation (t3dsdsc.f:1135-1165)
             T* t[8];
             tmp8(t);
+            hx(X, 8);
             if constexpr (KAHAN) {
-                filter_compensated(t, true);
+                hx(C, 8);
+                filter_compensated(t, tap);
             } else {
                 pass8("k_zpv_F", 16.0, X, [&](int lo) { return st4(t, lo); });
+                hx(t, 8);
                 SrcFields<T, 4> a, b;
                 for (int q = 0; q < 4; ++q) { a.f[q] = t[q]; b.f[q] = t[4 + q]; }
                 zp<4, 0u>("k_zpv_F", 8.0 * N * sizeof(T), a, st4(S, 0));
-                zp<4, KIND_B4>("k_zpv_F", 8.0 * N * sizeof(T) + tap_bytes(), b, with_cfl(st4(S, 4), S));
+                if (tap) zp<4, KIND_B4>("k_zpv_F", 8.0 * N * sizeof(T) + tap_bytes(), b, with_cfl(st4(S, 4), S));
+                else zp<4, KIND_B4>("k_zpv_F", 8.0 * N * sizeof(T), b, st4(S, 4));
                 for (int m = 0; m < 8; ++m) std::swap(X[m], S[m]);
             }
         }
         if (nstep % 10 == 0) {      // diagn blow-up guard (t3dsdsc.f:1174-1182, 1232)
+            hx(X + 4, 3);           // the current reads B at z-neighbours
             Status s = launch_diag(true);
             if (s.code) return s;
         }
@@ -1037,7 +1087,7 @@ public:
             launch_err = nullptr;
             return Status::err(DASHA_E_CUDA, e);
         }
-        rate_ok = filt;
+        rate_ok = filt && tap;
         return Status::ok();
     }
 
@@ -1077,7 +1127,7 @@ public:
             std::memcpy(&fl, hpin + 13, sizeof(int));
             *dt = (v != v) ? v : std::fmin(100.0, 1.0 / v);   // as k_reduce_rate
             *blowup = fl;
-            return Status::ok();
+            return slab_reduce(dt, blowup);
         }
         dim3 g2(1, my, mz);
         const long nt = (long)mx + my + mz;
@@ -1093,12 +1143,25 @@ public:
         std::memcpy(&fl, hpin + 13, sizeof(int));
         *dt = hpin[12];
         *blowup = fl;
+        return slab_reduce(dt, blowup);
+    }
+    // a slab of a one-process-per-GPU run: the smallest dt and any blow-up of all slabs (the
+    // group entry points of the slabs of one process reduce on the host)
+    Status slab_reduce(double* dt, int* blowup) {
+        if (halo && halo->per_process() && !halo->reduce(dt, blowup))
+            return Status::err(DASHA_E_CUDA, "slab dt reduction: " + halo->err);
         return Status::ok();
     }
 
     Status current(double* curh, long ld1, long ld2) override {
+        hx(X + 4, 3);
         launch_current(X);
         DASHA_CK(cudaGetLastError());
+        if (launch_err) {
+            const char* e = launch_err;
+            launch_err = nullptr;
+            return Status::err(DASHA_E_CUDA, e);
+        }
         return transfer_out(curh, ld1, ld2, curF, 3, false);
     }
 

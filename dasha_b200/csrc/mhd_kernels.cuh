@@ -38,6 +38,9 @@ struct Geo {
     const double *dzp0r;              // Dz p0 / rho0 (interior rows)
     T eta, di, gamma, mu, drho, dp;
     int hall, viscos, diffu;
+    // first plane of setdt's region: 0, except on a z-slab above the lowest one, whose planes 0
+    // and 1 are ghost copies of the slab below (halo.h)
+    int kcfl0;
 };
 
 template <class T>
@@ -327,7 +330,7 @@ __global__ void k_cfl_rate(Geo<T> g, F8<T> x, const double* ich, const double* v
     const double* ihx = ih;
     const double* ihy = ih + nx;
     const double* ihz = ih + nx + g.my;
-    if (k <= g.mz - 3 && jj <= g.my - 2) {
+    if (k >= g.kcfl0 && k <= g.mz - 3 && jj <= g.my - 2) {
         const double r0 = g.rho0[k], bx0 = g.bx0[k], by0 = g.by0[k], bz0 = g.bz0[k], p0 = g.p0[k];
         const double cy = ichy[jj], vy_ = vvy[jj], cz = ichz[k], vz_ = vvz[k], hy = ihy[jj], hz = ihz[k];
         for (int i = threadIdx.x; i <= g.mx - 3; i += blockDim.x) {

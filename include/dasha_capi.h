@@ -241,6 +241,55 @@ int dasha_profile_read(dasha_ctx* ctx, int* n, char* names, double* ms, long* la
 #define DASHA_NOALLOC_SCRATCH_DOUBLES (3L * DASHA_NOALLOC_MAX_CELLS + 3L * 7 * DASHA_NOALLOC_MAX_AXIS)
 int dasha_current_noalloc(const dasha_grid_c* grid, const double* db_dev, double* cur_dev, void* stream);
 
+/* ---- z-slab decomposition over several GPUs ----
+ * The multi-GPU form of the reference's domain decomposition (mhd01.for:5-6: nprx x nprz MPI
+ * ranks, each with a 2-node halo refreshed by message4, t3dsdsc.f:6354-6419), cut in z only:
+ * the interior rows 2..mz-3 are split into nslabs slabs of consecutive rows, and slab s is a
+ * context over its own rows plus two planes on each side (global rows first-2 .. first+count+1:
+ * the wall rows at a global wall, ghost copies of the neighbour's edge rows elsewhere).  The
+ * ghost planes are refreshed after every launch whose output a later launch reads at
+ * z-neighbours, so every slab's own rows take the values of the one-context run, bit for bit.
+ * Periodic (1,1,0) contexts only; the whole-grid calls (dasha_checkpoint, dasha_restore,
+ * dasha_stream_out, dasha_m3d_write_ctx, dasha_midplane, dasha_rhs, dasha_diagnostics, the
+ * adjoint, dasha_set_equilibrium_3d) return DASHA_E_UNSUPPORTED on a slab.
+ *
+ * dasha_slab_partition: own rows of slab `slab` (host only): count = (mz-4)/nslabs, the first
+ *   (mz-4)%nslabs slabs one more; DASHA_E_INVALID unless every slab gets at least 3 rows.
+ * dasha_create_slab: grid = the GLOBAL grid; the context is created on the current device.  Its
+ *   dasha_set_equilibrium / dasha_set_equilibrium_current take the global profiles (mz values
+ *   each) and keep the slab's planes; dasha_set_state / dasha_get_state / dasha_current carry
+ *   the slab's local array, mz_local = count + 4 planes (global rows first-2 ..), in the usual
+ *   halo layout; the ghost planes of the input are not read.
+ * dasha_slab_rows: the slab's first own global row, own row count and local plane count. */
+int dasha_slab_partition(int mz, int nslabs, int slab, int* first, int* count);
+int dasha_create_slab(const dasha_grid_c* grid, const dasha_params_c* params, int nslabs, int slab, dasha_ctx** out);
+int dasha_slab_rows(dasha_ctx* ctx, int* first, int* count, int* mz_local);
+
+/* One process, every slab (one per GPU, or several on one GPU): dasha_slab_link joins
+ * ctxs[0..n-1] (slab s at ctxs[s]) into a group whose ghost planes are copied between the
+ * slabs' memories (cudaMemcpyPeerAsync).  A linked group steps through the dasha_group_*
+ * calls, which run every slab in its own host thread: dasha_group_setdt returns the smallest
+ * dt of the slabs (the guards of dasha_setdt apply), dasha_group_stepon is one RK4 step of the
+ * whole grid (synchronous), dasha_group_current writes slab s's current to cur_f[s].  The
+ * single-context dasha_setdt / dasha_stepon / dasha_current of a linked slab return
+ * DASHA_E_STATE; a slab that is joined to nothing also returns DASHA_E_STATE there. */
+int dasha_slab_link(dasha_ctx* const* ctxs, int n);
+int dasha_group_setdt(dasha_ctx* const* ctxs, int n, double time, double* dt_out);
+int dasha_group_stepon(dasha_ctx* const* ctxs, int n, double time, double dt, int nstep);
+int dasha_group_current(dasha_ctx* const* ctxs, int n, double* const* cur_f, long ld1, long ld2);
+
+/* One process per GPU, each with one slab (the reference's one MPI rank per process): rank 0
+ * makes an NCCL id (dasha_nccl_unique_id, 128 bytes), every rank receives it by its own means
+ * (MPI_Bcast, torch.distributed) and joins with dasha_slab_nccl (collective: it returns once
+ * all nslabs ranks have joined).  Then each rank calls dasha_setdt / dasha_stepon /
+ * dasha_current on its slab as on a whole-grid context; the ghost planes travel by ncclSend /
+ * ncclRecv on the context's stream and setdt's dt is the minimum over the ranks
+ * (ncclAllReduce).  Every rank must make the same calls in the same order.  NCCL is loaded
+ * at run time (libnccl.so.2 of the process, else the system's); without it both calls return
+ * DASHA_E_UNSUPPORTED. */
+int dasha_nccl_unique_id(void* id, int nbytes);
+int dasha_slab_nccl(dasha_ctx* ctx, const void* id, int nbytes);
+
 /* Host-side files of the reference's output routines (no context, no GPU).  Each returns
  * DASHA_OK or DASHA_E_INVALID (bad argument, an I/O error, or a file that does not match).
  *

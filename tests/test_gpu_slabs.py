@@ -1,0 +1,99 @@
+"""The z-slab decomposition on a B200 (dasha_b200/slabs.py): the grid cut into 2 and 3 slabs
+whose ghost planes the library refreshes between launches must reproduce the one-context run
+bit for bit (every slab computes its own rows with the same operations in the same order), in
+FP64 and in the FP32 compensated form, with and without the post-step filter, across the
+blow-up guard's step and with the Hall term off.
+
+All slabs of a group run on the one GPU of this test in one process (the group's host threads
+order the copies against each slab's launches; no kernel waits on another).  The NCCL form is
+run with one rank: its ghost exchange has no neighbour there, so this checks its loading, its
+communicator and its dt reduction."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from dasha_b200 import capi, harris, slabs
+
+pytestmark = pytest.mark.gpu
+
+SINH = harris.RunConfig("slab-64x12x41-sinh", 64, 12, 41, True, 0.003, 1.0, 4, dt_whistler=1)
+UNIF = harris.RunConfig("slab-32x8x36", 32, 8, 36, False, 0.005, 0.5, 4)
+
+
+def run(d, steps, nstep0=0):
+    t, dts = 0.0, []
+    for n in range(nstep0, nstep0 + steps):
+        dt = d.setdt(t)
+        d.stepon(t, dt, n)
+        t += dt
+        dts.append(dt)
+    return dts, d.get_state()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("nslabs", [2, 3])
+@pytest.mark.parametrize("cfg,over", [(SINH, {}), (UNIF, {"filter_every": 3}), (UNIF, {"hall": 0})])
+def test_slab_group_equals_one_context(cfg, over, nslabs, precision):
+    one = capi.gem_context(cfg, precision, **over)
+    grp = slabs.gem_slab_group(cfg, nslabs, precision, **over)
+    try:
+        assert np.array_equal(grp.get_state(), one.get_state())
+        # steps 8..11: the guard (nstep % 10 == 0) runs at step 10
+        d1, x1 = run(one, 4, 8)
+        d2, x2 = run(grp, 4, 8)
+        assert d1 == d2, (d1, d2)
+        assert np.array_equal(x1, x2), np.abs(x1 - x2).max()
+        assert np.array_equal(grp.current(), one.current())
+    finally:
+        grp.close()
+        one.close()
+
+
+def test_slab_calls_refused_where_they_need_the_whole_grid():
+    grp = slabs.gem_slab_group(UNIF, 2, 0)
+    try:
+        s0 = grp.slabs[0]
+        with pytest.raises(capi.DashaError) as e:
+            s0.stepon(0.0, 1e-3, 0)       # a linked slab steps with its group
+        assert e.value.code == capi.E_STATE
+        with pytest.raises(capi.DashaError) as e:
+            s0.diagnostics()
+        assert e.value.code == capi.E_UNSUPPORTED
+        with pytest.raises(capi.DashaError) as e:
+            s0.midplane()
+        assert e.value.code == capi.E_UNSUPPORTED
+        first, count, mzl = C.c_int(), C.c_int(), C.c_int()
+        assert s0.lib.dasha_slab_rows(s0.h, C.byref(first), C.byref(count), C.byref(mzl)) == capi.OK
+        assert (first.value, count.value, mzl.value) == (2, 16, 20)
+        # the group still steps after the refusals
+        dt = grp.setdt(0.0)
+        grp.stepon(0.0, dt, 0)
+    finally:
+        grp.close()
+    # a slab joined to nothing cannot step
+    x, y, z = harris.make_grid(UNIF.mx, UNIF.my, UNIF.mz, UNIF.stretch)
+    lone = slabs._Slab(capi.load(), x, y, z, capi.make_params(UNIF, 0), 2, 1, slabs.partition(UNIF.mz, 2)[1])
+    try:
+        rho0, b0, p0, _ = harris.harris_profiles(z)
+        lone.set_equilibrium(rho0, b0, p0)
+        lone.set_state(slabs.split(harris.gem_state(x, y, z), slabs.partition(UNIF.mz, 2))[1])
+        with pytest.raises(capi.DashaError) as e:
+            lone.setdt(0.0)
+        assert e.value.code == capi.E_STATE
+    finally:
+        lone.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_nccl_slab_one_rank_equals_one_context(precision):
+    one = capi.gem_context(SINH, precision)
+    sl = slabs.gem_nccl_slab(SINH, 0, 1, slabs.new_id(), precision)
+    try:
+        d1, x1 = run(one, 3, 9)
+        d2, x2 = run(sl, 3, 9)
+        assert d1 == d2
+        assert np.array_equal(x1, x2)
+    finally:
+        sl.close()
+        one.close()
