@@ -1,7 +1,7 @@
 """Benchmark of the RK4 Hall-MHD step (the reference's stepon/setdt loop, t3dsdsc.f:136-202).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dasha|reference]
-                    [--config c0..c4] [--precision fp32|fp64]
+                    [--config c0..c4] [--precision fp32|fp64] [--slabs S]
 
 One "step" is one RK4 step (setdt + stepon) of the whole grid.  Default workload: the largest
 precision-form throughput configuration, 1024x512x1024 sinh-stretched Harris sheet, FP32
@@ -437,6 +437,48 @@ def run_dasha(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+def run_slab_group(args):
+    """The grid of --config cut into --slabs z-slabs stepped as one in-process group (every slab
+    on the current GPU unless several are visible): the cost of the slab machinery against the
+    one-context run of the same grid.  Wall clock around K group steps, the last setdt
+    synchronising every slab's stream."""
+    import torch
+    from dasha_b200 import harris, slabs
+    cfg = harris.CONFIGS[args.config]
+    ndev = max(1, torch.cuda.device_count())
+    devices = [s % ndev for s in range(args.slabs)]
+    grp = slabs.gem_slab_group(cfg, args.slabs, 1 if args.precision == "fp32" else 0, devices=devices)
+    t, n = 0.0, 0
+    for _ in range(args.warmup):
+        dt = grp.setdt(t)
+        grp.stepon(t, dt, n)
+        t += dt
+        n += 1
+    dt = grp.setdt(t)
+    clocks = Clocks()
+    clocks.start()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        grp.stepon(t, dt, n)
+        t += dt
+        n += 1
+        dt = grp.setdt(t)
+    el = time.perf_counter() - t0
+    ck = clocks.stop()
+    grp.close()
+    line = {"metric": METRIC, "value": cfg.cells * args.steps / el, "unit": "cell-updates/s", "n_gpus": ndev,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": el * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded Harris sheet + GEM perturbation)",
+            "config": {"workload": cfg.name, "grid": [cfg.mx, cfg.my, cfg.mz], "precision": args.precision,
+                       "parallelism": f"zslabs{args.slabs}-in-process", "devices": devices,
+                       "slab_rows": slabs.partition(cfg.mz, args.slabs),
+                       "timing": "wall clock, group calls synchronise every slab"},
+            "clocks": ck}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -448,8 +490,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--acc-steps", type=int, default=100,
                     help="steps of the 512x256x512 FP32-vs-FP64 check after the timed region (0: skip)")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="> 1: the grid as that many z-slabs stepped as one in-process group (one process)")
     args = ap.parse_args()
     rank, world, local = env_rank()
+    if args.slabs > 1 and args.impl == "dasha":
+        run_slab_group(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -97,3 +97,54 @@ def test_nccl_slab_one_rank_equals_one_context(precision):
     finally:
         sl.close()
         one.close()
+
+
+def _nccl_rank(rank, world, port, cfg, precision, steps, q):
+    import datetime
+    import os
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      NCCL_NVLS_ENABLE="0")
+    torch.cuda.set_device(rank)
+    dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=120))
+    try:
+        nid = slabs.share_id(slabs.new_id, rank)
+        sl = slabs.gem_nccl_slab(cfg, rank, world, nid, precision)
+        dts, x = run(sl, steps, 8)
+        q.put((rank, dts, x))
+        sl.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_nccl_slabs_on_several_gpus_equal_one_context(precision):
+    """One process per GPU, ghost planes by NCCL (runs where at least two GPUs are visible)."""
+    import socket
+    import torch
+    import torch.multiprocessing as mp
+    world = min(torch.cuda.device_count(), 3)
+    if world < 2:
+        pytest.skip("needs two GPUs")
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_nccl_rank, args=(r, world, port, SINH, precision, 4, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=300) for _ in procs), key=lambda r: r[0])
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    one = capi.gem_context(SINH, precision)
+    try:
+        d1, x1 = run(one, 4, 8)
+    finally:
+        one.close()
+    parts = slabs.partition(SINH.mz, world)
+    assert all(r[1] == d1 for r in res)
+    assert np.array_equal(slabs.assemble([r[2] for r in res], parts, SINH.mz), x1)
