@@ -196,7 +196,12 @@ static int create_ctx(const dasha_grid_c* grid, const dasha_params_c* params, in
     if (!grid || !params || !grid->x || !grid->y || !grid->z) return DASHA_E_INVALID;
     if (grid->mx < 5 || grid->my < 5 || grid->mz < 7) return DASHA_E_INVALID;
     const bool bounded = grid->periodic[0] == 0 && grid->periodic[1] == 0 && grid->periodic[2] == 0;
-    if (!bounded && grid->mx % 32 != 0) return DASHA_E_UNSUPPORTED;   // the z-marching tiles are 32 nodes wide in x
+    // rows move as 16-byte copies (4 FP32 or 2 FP64 values, row starts 16-byte aligned) and FP32
+    // float pairs; the z-marching kernels take a narrower last x tile, except the viscous /
+    // diffusive right-hand side (k_zst2), whose launch covers whole 32-node tiles
+    if (!bounded && grid->mx % 4 != 0) return DASHA_E_UNSUPPORTED;
+    const bool viscous = (params->viscos && params->mu != 0.0) || (params->diffu && (params->drho != 0.0 || params->dp != 0.0));
+    if (!bounded && viscous && grid->mx % 32 != 0) return DASHA_E_UNSUPPORTED;
     if (!bounded && !(grid->periodic[0] == 1 && grid->periodic[1] == 1 && grid->periodic[2] == 0)) return DASHA_E_UNSUPPORTED;
     const dasha_params_c& p = *params;
     if (p.precision != 0 && p.precision != 1) return DASHA_E_INVALID;

@@ -27,7 +27,7 @@
 // avrgtt on a compensated FP32 state (x, comp) whose value is x - comp: MODE 1 reads x in
 // fields 0..NF/2-1 and comp in the rest and writes the first pass's increment d of x - comp;
 // MODE 2 reads d and hands the two-pass increment 2 d + coef L(d) to a Kahan epilogue.
-// Needs mx % 32 == 0 (a tile narrower than 32*VX at the x end is handled).
+// Needs mx % 4 == 0 (16-byte row copies; a tile narrower than 32*VX at the x end is handled).
 #pragma once
 
 #include <type_traits>

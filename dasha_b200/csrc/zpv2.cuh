@@ -23,7 +23,7 @@
 // the result's wall rows are written with the result.
 //
 // KINDS: 2 bits per field, 0 radial coefficient, 1 constant 1/8, 2 x-profile cbx; the same
-// kind for both passes.  Needs mx % 32 == 0.
+// kind for both passes.  Needs mx % 4 == 0 (16-byte row copies; a narrower last x tile is handled).
 #pragma once
 
 #include <type_traits>

@@ -38,9 +38,10 @@ enum {
     DASHA_OK = 0,
     DASHA_E_INVALID = 1,      /* bad argument (null pointer, size, leading dimension) */
     DASHA_E_UNSUPPORTED = 2,  /* an option the library does not implement: periodicity other than
-                                 {1,1,0} or {0,0,0}, mx not a multiple of 32 or rcr > 0 on a periodic
-                                 context, FP32 on a bounded one, total_e != 1, the adjoint on an FP32
-                                 context, or a call a bounded context does not offer */
+                                 {1,1,0} or {0,0,0}, on a periodic context mx not a multiple of 4
+                                 (of 32 with viscosity or diffusion on) or rcr > 0, FP32 on a
+                                 bounded one, total_e != 1, the adjoint on an FP32 context, or a
+                                 call a bounded context does not offer */
     DASHA_E_CUDA = 3,         /* a CUDA runtime error; the context should be destroyed */
     DASHA_E_NOMEM = 4,        /* the grid does not fit in device memory */
     DASHA_E_DT_COLLAPSE = 5,  /* dt < 0.1*dt0 or not finite: the guard of t3dsdsc.f:142-154 */
@@ -285,8 +286,10 @@ int dasha_group_current(dasha_ctx* const* ctxs, int n, double* const* cur_f, lon
  * dasha_current on its slab as on a whole-grid context; the ghost planes travel by ncclSend /
  * ncclRecv on the context's stream and setdt's dt is the minimum over the ranks
  * (ncclAllReduce).  Every rank must make the same calls in the same order.  NCCL is loaded
- * at run time (libnccl.so.2 of the process, else the system's); without it both calls return
- * DASHA_E_UNSUPPORTED. */
+ * at run time: the libnccl.so.2 already in the process, else the one the loader finds; without
+ * it both calls return DASHA_E_UNSUPPORTED.  A process holds one libnccl.so.2 and libraries
+ * loaded later bind to it, so a process that also uses another NCCL user (torch) loads that one
+ * first. */
 int dasha_nccl_unique_id(void* id, int nbytes);
 int dasha_slab_nccl(dasha_ctx* ctx, const void* id, int nbytes);
 

@@ -107,6 +107,12 @@ def test_argument_checks_need_no_device():
     y = np.arange(8.0)
     g = capi.GridC(8, 8, 8, capi._dp(y), capi._dp(y), capi._dp(y), (ctypes.c_int * 3)(0, 1, 0))
     assert lib.dasha_create(ctypes.byref(g), ctypes.byref(p), ctypes.byref(h)) == capi.E_UNSUPPORTED
+    # periodic contexts: mx a multiple of 4 (16-byte rows), of 32 with viscosity or diffusion
+    for mx, visc in ((38, 0), (36, 1), (100, 1)):
+        xs = np.arange(float(mx))
+        gm = capi.GridC(mx, 8, 8, capi._dp(xs), capi._dp(y), capi._dp(y), (ctypes.c_int * 3)(1, 1, 0))
+        pv = capi.ParamsC(gamma=5 / 3, cfl=0.4, total_e=1, viscos=visc, mu=1e-3 * visc)
+        assert lib.dasha_create(ctypes.byref(gm), ctypes.byref(pv), ctypes.byref(h)) == capi.E_UNSUPPORTED
     dt = ctypes.c_double()
     assert lib.dasha_setdt(None, 0.0, ctypes.byref(dt)) == capi.E_INVALID
     assert lib.dasha_stepon(None, 0.0, 0.1, 0) == capi.E_INVALID

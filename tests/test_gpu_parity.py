@@ -24,6 +24,9 @@ RAGGED = harris.RunConfig("ragged-96x12x36-sinh", 96, 12, 36, True, 0.003, 1.0, 
 MINI = harris.RunConfig("mini-32x5x7", 32, 5, 7, False, 0.005, 0.5, 4)
 ODD = harris.RunConfig("odd-160x7x9-sinh", 160, 7, 9, True, 0.003, 1.0, 4, dt_whistler=1)
 TALL = harris.RunConfig("tall-32x8x300-sinh", 32, 8, 300, True, 0.003, 1.0, 4)
+# x tiles narrower than 32 nodes (mx % 32 != 0); checked in bounds by tests/test_gpu_bounds.py first
+NARROW = harris.RunConfig("narrow-36x8x20", 36, 8, 20, False, 0.005, 0.5, 4)
+NARROW_S = harris.RunConfig("narrow-100x6x12-sinh", 100, 6, 12, True, 0.003, 1.0, 4, dt_whistler=1)
 
 
 def rel_err(a, b):
@@ -46,14 +49,15 @@ def test_state_roundtrip(cfg):
     assert rel_err(d.get_state(), o.get_state()).max() < 1e-15
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED, MINI, ODD, TALL, NARROW, NARROW_S], ids=lambda c: c.name)
 def test_current_parity(cfg):
     o, d = pair(cfg)
     e = rel_err(d.current(), o.current())
     assert e.max() < 1e-11, e
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, harris.CONFIGS["c0"], RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, harris.CONFIGS["c0"], RAGGED, MINI, ODD, TALL, NARROW, NARROW_S],
+                         ids=lambda c: c.name)
 @pytest.mark.parametrize("t", [0.0, 0.5])
 def test_rhs_parity(cfg, t):
     o, d = pair(cfg)
@@ -103,7 +107,7 @@ def test_setdt_parity_whistler_option():
     assert d.setdt() < 0.5 * plain
 
 
-@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED, MINI, ODD, TALL], ids=lambda c: c.name)
+@pytest.mark.parametrize("cfg", [SMALL, SMALL_S, RAGGED, MINI, ODD, TALL, NARROW, NARROW_S], ids=lambda c: c.name)
 def test_steps_parity(cfg):
     o, d = pair(cfg)
     t = 0.0
@@ -143,8 +147,8 @@ def test_diagnostics_parity(cfg):
 SMALL_SW = harris.RunConfig("small-32x16x40-sinh-whistler", 32, 16, 40, True, 0.003, 1.0, 4, dt_whistler=1)
 
 
-@pytest.mark.parametrize("cfg,steps", [(harris.CONFIGS["c0"], 200), (SMALL_SW, 300), (RAGGED, 200)],
-                         ids=["c0-200", "sinh-whistler-300", "ragged-200"])
+@pytest.mark.parametrize("cfg,steps", [(harris.CONFIGS["c0"], 200), (SMALL_SW, 300), (RAGGED, 200), (NARROW_S, 200)],
+                         ids=["c0-200", "sinh-whistler-300", "ragged-200", "narrow-200"])
 def test_fp32_path_close_to_fp64(cfg, steps):
     """FP32 perturbation + Kahan RK4 + compensated filter against the FP64 path on the same dt
     sequence: every field within 1e-6 relative L2 (measured: <= 1.4e-7).  The di = 1 stretched
