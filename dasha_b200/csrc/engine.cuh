@@ -700,10 +700,19 @@ public:
     }
     // k_zpv2 (two passes in one launch): tile 32*ZVX x 8, one row per warp plus two halo-row
     // warps, D planes in flight
+    // (measurement builds may set the tile height and depth: -DDASHA_ZP2_TY=.. -DDASHA_ZP2_D=..)
     template <int NF>
     struct ZC2 {
+#ifdef DASHA_ZP2_TY
+        static constexpr int TY = DASHA_ZP2_TY;
+#else
         static constexpr int TY = 8;
+#endif
+#ifdef DASHA_ZP2_D
+        static constexpr int D = DASHA_ZP2_D;
+#else
         static constexpr int D = sizeof(T) == 4 ? 3 : 2;
+#endif
     };
     template <int NF>
     using ZV2c = ZV2<T, NF, ZVX, ZC2<NF>::TY, ZC2<NF>::D>;

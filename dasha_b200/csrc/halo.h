@@ -208,12 +208,15 @@ struct NcclApi {
     decltype(&ncclGetErrorString) error_string = nullptr;
     std::string why;
     bool ok() const { return send != nullptr; }
-    // the process's NCCL: an already loaded libnccl.so.2 (torch's, for instance) or the system one
+    // The process's NCCL: the libnccl.so.2 already loaded (torch's, for instance), else the one
+    // the loader finds.  A process holds one object of that name, and a library loaded later
+    // that needs libnccl.so.2 binds to it: a process that also uses torch imports torch first.
     static const NcclApi& get() {
         static NcclApi api = [] {
             NcclApi a;
-            void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_GLOBAL);
-            if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_GLOBAL);
+            void* h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_NOLOAD);
+            if (!h) h = dlopen("libnccl.so.2", RTLD_NOW | RTLD_LOCAL);
+            if (!h) h = dlopen("libnccl.so", RTLD_NOW | RTLD_LOCAL);
             if (!h) { a.why = std::string("libnccl.so.2 not found: ") + (dlerror() ? dlerror() : ""); return a; }
             auto sym = [&](const char* n) { return dlsym(h, n); };
             a.get_unique_id = (decltype(a.get_unique_id))sym("ncclGetUniqueId");

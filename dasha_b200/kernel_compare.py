@@ -2,6 +2,7 @@
 
     python -m dasha_b200.kernel_compare [--grid MX MY MZ] [--precision fp32|fp64] [--steps K]
                                         [--warmup W] [--check-grid MX MY MZ]
+                                        [--extra NAME=PATH ...] [--only-extra]
 
 The builds: the default library (ring planes of the FP64 passes, the FP32 passes of 4 and 6
 fields and the hydro RHS loaded by TMA, the FP32 3-field passes by cp.async) and the one whose
@@ -79,8 +80,17 @@ def main(argv=None):
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--extra", nargs="*", default=[], metavar="NAME=PATH",
+                    help="further builds of the library to time beside the default (tiling variants)")
+    ap.add_argument("--only-extra", action="store_true", help="the default and the --extra builds only")
     a = ap.parse_args(argv)
-    libs = {name: capi.bind(path) for name, path in BUILDS.items() if name == "default" or os.path.exists(path)}
+    builds = dict(BUILDS)
+    if a.only_extra:
+        builds = {"default": capi.LIB_PATH}
+    for e in a.extra:
+        name, path = e.split("=", 1)
+        builds[name] = path
+    libs = {name: capi.bind(path) for name, path in builds.items() if name == "default" or os.path.exists(path)}
     cfg, prec = _cfg(a.grid, a.precision)
     out = {"grid": a.grid, "precision": a.precision, "steps": a.steps, "warmup": a.warmup, "builds": {}}
     for name, lib in libs.items():

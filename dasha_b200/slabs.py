@@ -165,8 +165,18 @@ def gem_slab_group(cfg: harris.RunConfig, nslabs: int, precision: int = 0, seed_
 
 # ---- one slab per process ----
 
+def _nccl_first():
+    """torch's libnccl.so.2 into the process before the library looks for one: a process holds
+    one libnccl.so.2, and torch needs its own (newer) one."""
+    try:
+        import torch  # noqa: F401
+    except ImportError:
+        pass
+
+
 def new_id(lib=None) -> bytes:
     """A fresh 128-byte NCCL id (rank 0 makes it, every rank joins with it)."""
+    _nccl_first()
     lib = lib if lib is not None else capi.load()
     buf = C.create_string_buffer(128)
     rc = lib.dasha_nccl_unique_id(buf, 128)
@@ -190,6 +200,7 @@ class NcclSlab(_Slab):
     same calls in the same order."""
 
     def __init__(self, x, y, z, params, rank: int, world: int, nccl_id: bytes, lib=None):
+        _nccl_first()
         lib = lib if lib is not None else capi.load()
         x = np.ascontiguousarray(x, np.float64)
         y = np.ascontiguousarray(y, np.float64)
