@@ -19,6 +19,8 @@ pytestmark = pytest.mark.gpu
 
 SINH = harris.RunConfig("slab-64x12x41-sinh", 64, 12, 41, True, 0.003, 1.0, 4, dt_whistler=1)
 UNIF = harris.RunConfig("slab-32x8x36", 32, 8, 36, False, 0.005, 0.5, 4)
+# four slabs of the smallest size, 3 own rows each (local grids of 7 planes)
+THIN = harris.RunConfig("slab-64x8x16-sinh", 64, 8, 16, True, 0.003, 1.0, 4, dt_whistler=1)
 
 
 def run(d, steps, nstep0=0):
@@ -83,6 +85,21 @@ def test_slab_calls_refused_where_they_need_the_whole_grid():
         assert e.value.code == capi.E_STATE
     finally:
         lone.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("cfg,nslabs,over", [(THIN, 4, {}), (UNIF, 2, {"j0_mode": 1})], ids=["thin-4", "full-j0-2"])
+def test_slab_group_edge_cases(cfg, nslabs, over, precision):
+    one = capi.gem_context(cfg, precision, **over)
+    grp = slabs.gem_slab_group(cfg, nslabs, precision, **over)
+    try:
+        d1, x1 = run(one, 6, 7)
+        d2, x2 = run(grp, 6, 7)
+        assert d1 == d2
+        assert np.array_equal(x1, x2), np.abs(x1 - x2).max()
+    finally:
+        grp.close()
+        one.close()
 
 
 @pytest.mark.parametrize("precision", [0, 1])
