@@ -770,6 +770,19 @@ int dasha_slab_link(dasha_ctx* const* cs, int n) {
             h->geo.n = n; h->geo.s = s; h->geo.device = cs[s]->device;
             hs.push_back(std::move(h));
         }
+        // neighbours on different GPUs copy over NVLink: peer access both ways where the pair has it
+        int cur = 0;
+        cudaGetDevice(&cur);
+        for (int s = 0; s + 1 < n; ++s) {
+            const int a = cs[s]->device, b = cs[s + 1]->device;
+            if (a == b) continue;
+            int ab = 0, ba = 0;
+            cudaDeviceCanAccessPeer(&ab, a, b);
+            cudaDeviceCanAccessPeer(&ba, b, a);
+            if (ab && cudaSetDevice(a) == cudaSuccess && cudaDeviceEnablePeerAccess(b, 0) != cudaSuccess) cudaGetLastError();
+            if (ba && cudaSetDevice(b) == cudaSuccess && cudaDeviceEnablePeerAccess(a, 0) != cudaSuccess) cudaGetLastError();
+        }
+        cudaSetDevice(cur);
         for (int s = 0; s < n; ++s) {
             grp->members[s] = &hs[s]->geo;
             cs[s]->halo = std::move(hs[s]);
