@@ -1,7 +1,7 @@
 """Benchmark of the RK4 Hall-MHD step (the reference's stepon/setdt loop, t3dsdsc.f:136-202).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dasha|reference]
-                    [--config c0..c4] [--precision fp32|fp64] [--slabs S]
+                    [--config c0..c4] [--precision fp32|fp64] [--slabs S] [--layout replicas|slabs]
 
 One "step" is one RK4 step (setdt + stepon) of the whole grid.  Default workload: the largest
 precision-form throughput configuration, 1024x512x1024 sinh-stretched Harris sheet, FP32
@@ -13,7 +13,8 @@ fields, 17 GB in FP32) are far larger than L2, so no L2 flush is needed between 
          Fortran caller runs it: dasha_set_state from host memory, K x (dasha_setdt with its
          dt read-back + dasha_stepon), dasha_get_state back to host memory.
 Multi-GPU: the path does not shard (one on-device domain), so N ranks run N replicas;
-`value` is the total over ranks and the time is the max over ranks.
+`value` is the total over ranks and the time is the max over ranks.  `--layout slabs` instead
+stacks the grid N times in z as one grid of N z-slabs (one per rank, ghost planes by NCCL).
 """
 from __future__ import annotations
 
@@ -479,6 +480,64 @@ def run_slab_group(args):
     print(json.dumps(line), flush=True)
 
 
+def run_nccl_slabs(args, rank, world):
+    """One z-slab per rank, one process per GPU (torchrun): the grid of --config stacked N times
+    in z (N (mz-4) + 4 planes, every rank owning the one-GPU workload's mz-4 interior rows: weak
+    scaling), ghost planes by NCCL inside the library.  CUDA events on each rank's stream, the
+    max over ranks; value = all ranks' cell-updates / that time."""
+    import datetime
+    from dasha_b200 import capi, harris, slabs
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=600))
+    cfg = harris.CONFIGS[args.config]
+    mzg = world * (cfg.mz - 4) + 4
+    x, y, z = harris.make_grid(cfg.mx, cfg.my, mzg, cfg.stretch)
+    nid = slabs.share_id(slabs.new_id, rank) if dist else slabs.new_id()
+    sl = slabs.NcclSlab(x, y, z, capi.make_params(cfg, 1 if args.precision == "fp32" else 0), rank, world, nid)
+    rho0, b0, p0, _ = harris.harris_profiles(z)
+    sl.set_equilibrium(rho0, b0, p0)
+    first, count = sl.part
+    H = harris.gem_state_halo(x, y, z, threads=os.cpu_count() or 8, planes=(first - 2, first + count + 2))
+    sl.set_state_halo(H)
+    del H
+    t, n = 0.0, 0
+    for _ in range(args.warmup):
+        dt = sl.setdt(t)
+        sl.stepon(t, dt, n)
+        t += dt
+        n += 1
+    sl.setdt(t)
+    if dist:
+        dist.barrier()
+    clocks = Clocks()
+    clocks.start()
+    sl.timer_start()
+    for _ in range(args.steps):
+        dt = sl.setdt(t)
+        sl.stepon(t, dt, n)
+        t += dt
+        n += 1
+    ms = sl.timer_stop()
+    ck = clocks.stop()
+    ms = max_over_ranks(ms, dist)
+    sl.close()
+    cells = cfg.mx * cfg.my * mzg
+    line = {"metric": METRIC, "value": cells * args.steps / (ms / 1e3), "unit": "cell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded Harris sheet + GEM perturbation)",
+            "config": {"workload": f"{cfg.name} stacked x{world} in z", "grid": [cfg.mx, cfg.my, mzg],
+                       "precision": args.precision, "parallelism": f"zslabs{world}-nccl",
+                       "own_rows_per_rank": count, "l2": "inputs larger than L2 (no flush)"},
+            "clocks": ck}
+    if dist:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -492,10 +551,16 @@ def main():
                     help="steps of the 512x256x512 FP32-vs-FP64 check after the timed region (0: skip)")
     ap.add_argument("--slabs", type=int, default=0,
                     help="> 1: the grid as that many z-slabs stepped as one in-process group (one process)")
+    ap.add_argument("--layout", default="replicas", choices=["replicas", "slabs"],
+                    help="multi-GPU form: independent replicas (default) or one z-slab per rank over NCCL")
     args = ap.parse_args()
     rank, world, local = env_rank()
     if args.slabs > 1 and args.impl == "dasha":
         run_slab_group(args)
+        return
+    if args.layout == "slabs" and args.impl == "dasha":
+        pin_device(local, world)
+        run_nccl_slabs(args, rank, world)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

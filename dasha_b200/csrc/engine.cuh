@@ -216,6 +216,8 @@ public:
         return sg;
     }
     void set_cfl_k0(int k0) override { g.kcfl0 = k0; }
+    // a z-slab with a neighbour: its ghost planes are copies (a lone slab's are the walls)
+    bool cut() const { return halo && (halo->geo.lower() || halo->geo.upper()); }
     // z-slab contexts: refresh the ghost planes of fields f that a later launch reads at
     // z-neighbours (a no-op on a whole-grid context)
     void hx(T* const* f, int nf) {
@@ -909,7 +911,7 @@ public:
     template <unsigned KINDS>
     T** passes3(const char* tag, T** a, T** b, int n, bool xlast) {
         if constexpr (KINDS == KIND_H) {
-            if (!halo) {
+            if (!cut()) {
                 for (int p = 0; p < n; p += 2) {   // pairs of passes in one k_zpv2 launch, a lone last one by k_zpv
                     T** in = ((p / 2) & 1) ? b : a;
                     T** out = ((p / 2) & 1) ? a : b;
@@ -1059,7 +1061,7 @@ public:
         const int every = P.filter_every > 0 ? P.filter_every : 1;
         const bool filt = nstep % every == 0;
         // a z-slab takes setdt's rate by its own sweep (the tap would also read the ghost planes)
-        const bool tap = !halo;
+        const bool tap = !cut();
         rate_ok = false;
         hx(X, 8);
         for (int stage = 1; stage <= 4; ++stage) {

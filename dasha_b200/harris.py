@@ -142,23 +142,28 @@ CONFIGS = {
 }
 
 
-def gem_state_halo(x, y, z, seed_v: int = SEED_V, noise_amp: float = 1e-3, threads: int = 8) -> np.ndarray:
+def gem_state_halo(x, y, z, seed_v: int = SEED_V, noise_amp: float = 1e-3, threads: int = 8,
+                   planes: tuple[int, int] | None = None) -> np.ndarray:
     """gem_state written straight into the reference layout (8, mz+4, my, mx+4), z-plane by
     z-plane on a thread pool: the same numbers as to_halo(gem_state(...)) without the
-    compact temporary (the largest grid's state is 35 GB in this layout)."""
+    compact temporary (the largest grid's state is 35 GB in this layout).  planes = (k0, k1):
+    only the global planes k0..k1-1, as an array of k1-k0 planes (a z-slab's local planes), with
+    the same numbers as those planes of the whole state."""
     from concurrent.futures import ThreadPoolExecutor
     mx, my, mz = x.size, y.size, z.size
+    k0, k1 = planes if planes is not None else (0, mz)
+    ml = k1 - k0
     rho0, b0, p0, _ = harris_profiles(z)
-    H = np.empty((8, mz + 4, my, mx + 4))
+    H = np.empty((8, ml + 4, my, mx + 4))
     H[:, :2] = np.nan
-    H[:, mz + 2:] = np.nan
+    H[:, ml + 2:] = np.nan
     H[:, :, :, :2] = np.nan
     H[:, :, :, mx + 2:] = np.nan
     kx, kz = 2 * np.pi / LX, np.pi / LZ
     n = mx * my * mz
 
     def plane(k):
-        hk = k + 2
+        hk = k - k0 + 2
         H[0, hk, :, 2:mx + 2] = rho0[k]
         dbx = 0.1 * np.cos(kx * x) * kz * np.sin(kz * z[k])
         dbz = -0.1 * kx * np.sin(kx * x) * np.cos(kz * z[k])
@@ -174,7 +179,7 @@ def gem_state_halo(x, y, z, seed_v: int = SEED_V, noise_amp: float = 1e-3, threa
                 H[1 + c, hk, :, 2:mx + 2] = 0.0
 
     with ThreadPoolExecutor(max_workers=threads) as ex:
-        list(ex.map(plane, range(mz)))
+        list(ex.map(plane, range(k0, k1)))
     return H
 
 
