@@ -84,6 +84,8 @@ SIGNATURES = {
     "dasha_m3d_write": ([C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, _D, _D, _D, _D, _D,
                          C.c_long, C.c_long], C.c_int),
     "dasha_slab_partition": ([C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "dasha_slab_halo_plan": ([C.c_int, C.c_int, C.c_int, C.c_long, C.POINTER(C.c_int), C.POINTER(C.c_long),
+                              C.POINTER(C.c_long), C.POINTER(C.c_long)], C.c_int),
     "dasha_create_slab": ([C.POINTER(GridC), C.POINTER(ParamsC), C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "dasha_slab_rows": ([_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
     "dasha_slab_link": ([C.POINTER(C.c_void_p), C.c_int], C.c_int),

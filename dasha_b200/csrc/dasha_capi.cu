@@ -179,6 +179,21 @@ int dasha_slab_partition(int mz, int nslabs, int slab, int* first, int* count) {
     return DASHA_OK;
 }
 
+int dasha_slab_halo_plan(int mz, int nslabs, int slab, long plane, int* peer, long* send_off, long* recv_off,
+                         long* count) {
+    SlabPart sp;
+    if (!peer || !send_off || !recv_off || !count || plane < 1 || !slab_partition(mz, nslabs, slab, sp))
+        return DASHA_E_INVALID;
+    SlabGeom g;   // offsets in values: one byte per value
+    g.n = nslabs; g.s = slab; g.mzl = sp.count + 4; g.sz = plane; g.elem = 1;
+    peer[0] = g.lower() ? slab - 1 : -1;
+    peer[1] = g.upper() ? slab + 1 : -1;
+    send_off[0] = (long)g.send_lo(); recv_off[0] = (long)g.recv_lo();
+    send_off[1] = (long)g.send_hi(); recv_off[1] = (long)g.recv_hi();
+    *count = (long)g.span();
+    return DASHA_OK;
+}
+
 int dasha_create_slab(const dasha_grid_c* grid, const dasha_params_c* params, int nslabs, int slab, dasha_ctx** out) {
     if (!out) return DASHA_E_INVALID;
     *out = nullptr;

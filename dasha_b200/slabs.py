@@ -42,6 +42,19 @@ def partition(mz: int, nslabs: int, lib=None) -> list[tuple[int, int]]:
     return out
 
 
+def halo_plan(mz: int, nslabs: int, slab: int, plane: int, lib=None):
+    """The library's ghost exchange of one slab, in values of one field of `plane` values per
+    z plane: [(peer, send_off, recv_off, count)] for the slab below and above (peer -1: a wall)."""
+    lib = lib if lib is not None else capi.load()
+    peer = (C.c_int * 2)()
+    so, ro = (C.c_long * 2)(), (C.c_long * 2)()
+    n = C.c_long()
+    rc = lib.dasha_slab_halo_plan(mz, nslabs, slab, plane, peer, so, ro, C.byref(n))
+    if rc != OK:
+        raise DashaError(rc, "dasha_slab_halo_plan")
+    return [(peer[q], so[q], ro[q], n.value) for q in range(2)]
+
+
 def local_rows(part: tuple[int, int]) -> slice:
     """The global planes a slab's context holds: its own rows and two planes on each side."""
     first, count = part

@@ -263,6 +263,12 @@ int dasha_current_noalloc(const dasha_grid_c* grid, const double* db_dev, double
  *   halo layout; the ghost planes of the input are not read.
  * dasha_slab_rows: the slab's first own global row, own row count and local plane count. */
 int dasha_slab_partition(int mz, int nslabs, int slab, int* first, int* count);
+/* The ghost exchange of slab `slab` (host only), in values of one field whose planes hold `plane`
+ * values (mx*my): peer[0] / peer[1] the slab below / above (-1 at a wall); it sends `count`
+ * values from send_off[q] to peer[q] and receives `count` values at recv_off[q] from peer[q].
+ * The NCCL and the in-process exchanges move exactly these ranges. */
+int dasha_slab_halo_plan(int mz, int nslabs, int slab, long plane, int* peer, long* send_off, long* recv_off,
+                         long* count);
 int dasha_create_slab(const dasha_grid_c* grid, const dasha_params_c* params, int nslabs, int slab, dasha_ctx** out);
 int dasha_slab_rows(dasha_ctx* ctx, int* first, int* count, int* mz_local);
 

@@ -116,3 +116,72 @@ def test_rank_zero_id_reaches_every_rank():
         assert p.exitcode == 0
     assert res[0][1] == res[1][1] and len(res[0][1]) == 128
     assert [r[2] for r in res] == [(2, 512), (514, 512)]
+
+
+def _exchange_rank(rank, world, port, mz, q):
+    """One slab per gloo rank: the global field's local planes with the ghost planes poisoned,
+    then the library's exchange plan as point-to-point messages (the NCCL group's sends and
+    receives, here isend/irecv of torch tensors)."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", init_method="env://", timeout=datetime.timedelta(seconds=60))
+    try:
+        my, mx = 3, 4
+        X = np.arange(2 * mz * my * mx, dtype=np.float64).reshape(2, mz, my, mx)
+        parts = slabs.partition(mz, world)
+        P = slabs.split(X, parts)[rank].copy()
+        first, count = parts[rank]
+        if rank > 0:
+            P[:, :2] = -1.0
+        if rank < world - 1:
+            P[:, -2:] = -1.0
+        flat = [torch.from_numpy(P[f].reshape(-1)) for f in range(2)]
+        reqs = []
+        for f in range(2):                       # the fields in the same order on every rank
+            for peer, so, ro, n in slabs.halo_plan(mz, world, rank, my * mx):
+                if peer < 0:
+                    continue
+                reqs.append(dist.isend(flat[f][so:so + n].clone(), peer))
+                buf = torch.empty(n, dtype=torch.float64)
+                reqs.append((dist.irecv(buf, peer), f, ro, buf))
+        for r in reqs:
+            if isinstance(r, tuple):
+                r[0].wait()
+                flat[r[1]][r[2]:r[2] + r[3].numel()] = r[3]
+            else:
+                r.wait()
+        got = np.stack([t.numpy().reshape(P.shape[1:]) for t in flat])
+        q.put((rank, bool(np.array_equal(got, X[:, first - 2:first + count + 2]))))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,mz", [(2, 12), (3, 17)])
+def test_halo_plan_exchange_between_gloo_ranks(world, mz):
+    """After one exchange every slab's ghost planes hold its neighbours' edge rows: its local
+    planes equal the global field's rows first-2 .. first+count+1."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_exchange_rank, args=(r, world, port, mz, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert res == [(r, True) for r in range(world)]
+
+
+def test_halo_plan_ranges():
+    plane = 6
+    for mz, n in ((12, 2), (17, 3), (1028, 8)):
+        parts = slabs.partition(mz, n)
+        for s, (first, count) in enumerate(parts):
+            (pl, slo, rlo, c0), (pu, shi, rhi, c1) = slabs.halo_plan(mz, n, s, plane)
+            assert c0 == c1 == 2 * plane
+            assert pl == (s - 1 if s > 0 else -1) and pu == (s + 1 if s < n - 1 else -1)
+            assert slo == 2 * plane and rlo == 0                      # own rows first, first+1 / ghosts
+            assert shi == count * plane and rhi == (count + 2) * plane   # own last two rows / ghosts
