@@ -15,8 +15,8 @@
 // Two exchanges implement it:
 //   HaloLocal  every slab in this process (one host thread per slab while a group call runs):
 //              each slab copies its neighbours' edge planes into its ghost planes
-//              (cudaMemcpyPeerAsync, NVLink between GPUs); a host barrier on both sides of the
-//              copies orders them against the neighbours' kernels.
+//              (cudaMemcpyPeerAsync, NVLink between GPUs), ordered against the neighbours'
+//              launches by events its stream waits on (no host synchronisation).
 //   HaloNccl   one process per GPU: ncclSend / ncclRecv of the edge planes of each field in one
 //              NCCL group on the context's stream (no host synchronisation), and the dt
 //              reduction of setdt as ncclAllReduce.  NCCL is opened at run time (dlopen), so
@@ -141,9 +141,16 @@ private:
 };
 
 struct LocalGroup {
-    explicit LocalGroup(int n) : bar(n), members(n, nullptr) {}
+    explicit LocalGroup(int n) : bar(n), members(n, nullptr), wr(n, nullptr), cp(n, nullptr) {}
+    ~LocalGroup() {
+        for (cudaEvent_t e : wr) if (e) cudaEventDestroy(e);
+        for (cudaEvent_t e : cp) if (e) cudaEventDestroy(e);
+    }
     GroupBarrier bar;
     std::vector<const SlabGeom*> members;   // slab s's geometry
+    // slab s's events: its writes before an exchange, its ghost copies of an exchange (each
+    // slab records only its own; the others read them after a barrier)
+    std::vector<cudaEvent_t> wr, cp;
     double limit_s = 300.0;                 // a barrier wait longer than this fails the group call
 };
 
@@ -154,34 +161,44 @@ public:
 
     bool per_process() const override { return false; }
 
+    // Stream order, no host synchronisation: the copies wait (cudaStreamWaitEvent) on the
+    // neighbours' writes, and this slab's next launches on the neighbours' copies out of its edge
+    // planes; the host barriers only order each event's record before the waits on it.
     bool exchange(void* const* f, int nf) override {
         if (grp->bar.failed()) return fail("an earlier exchange of the group failed");
-        // every slab's writes of these fields are finished before any copy reads them
-        if (cudaStreamSynchronize(geo.st) != cudaSuccess) return fail("a launch before the exchange failed");
+        const int s = geo.s;
+        if (!grp->wr[s] && (cudaEventCreateWithFlags(&grp->wr[s], cudaEventDisableTiming) != cudaSuccess ||
+                            cudaEventCreateWithFlags(&grp->cp[s], cudaEventDisableTiming) != cudaSuccess))
+            return fail("event creation failed");
+        if (cudaEventRecord(grp->wr[s], geo.st) != cudaSuccess) return fail("event record failed");
         if (!grp->bar.arrive(grp->limit_s)) return fail("a slab of the group did not reach the exchange");
+        if ((geo.lower() && !grp->members[s - 1]) || (geo.upper() && !grp->members[s + 1]))
+            return fail("a neighbouring slab of the group was destroyed");
+        if (geo.lower() && cudaStreamWaitEvent(geo.st, grp->wr[s - 1], 0) != cudaSuccess) return fail("event wait failed");
+        if (geo.upper() && cudaStreamWaitEvent(geo.st, grp->wr[s + 1], 0) != cudaSuccess) return fail("event wait failed");
         for (int q = 0; q < nf; ++q) {
             const size_t off = (size_t)((const char*)f[q] - (const char*)geo.pool);
             if ((const char*)f[q] < (const char*)geo.pool || off % geo.fbytes != 0) return fail("field outside the pool");
             const size_t idx = off / geo.fbytes;
             char* dst = (char*)f[q];
-            if ((geo.lower() && !grp->members[geo.s - 1]) || (geo.upper() && !grp->members[geo.s + 1]))
-                return fail("a neighbouring slab of the group was destroyed");
             if (geo.lower()) {
-                const SlabGeom& o = *grp->members[geo.s - 1];
+                const SlabGeom& o = *grp->members[s - 1];
                 const char* src = (const char*)o.pool + idx * o.fbytes + o.send_hi();
                 if (cudaMemcpyPeerAsync(dst + geo.recv_lo(), geo.device, src, o.device, geo.span(), geo.st) != cudaSuccess)
                     return fail("ghost copy from the lower slab failed");
             }
             if (geo.upper()) {
-                const SlabGeom& o = *grp->members[geo.s + 1];
+                const SlabGeom& o = *grp->members[s + 1];
                 const char* src = (const char*)o.pool + idx * o.fbytes + o.send_lo();
                 if (cudaMemcpyPeerAsync(dst + geo.recv_hi(), geo.device, src, o.device, geo.span(), geo.st) != cudaSuccess)
                     return fail("ghost copy from the upper slab failed");
             }
         }
-        // the neighbours read nothing of ours until every copy has landed
-        if (cudaStreamSynchronize(geo.st) != cudaSuccess) return fail("a ghost copy failed");
+        if (cudaEventRecord(grp->cp[s], geo.st) != cudaSuccess) return fail("event record failed");
         if (!grp->bar.arrive(grp->limit_s)) return fail("a slab of the group did not finish the exchange");
+        // the neighbours' copies out of this slab's edge planes end before its next launch
+        if (geo.lower() && cudaStreamWaitEvent(geo.st, grp->cp[s - 1], 0) != cudaSuccess) return fail("event wait failed");
+        if (geo.upper() && cudaStreamWaitEvent(geo.st, grp->cp[s + 1], 0) != cudaSuccess) return fail("event wait failed");
         return true;
     }
     bool reduce(double*, int*) override { return true; }   // the group entry point reduces on the host
