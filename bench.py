@@ -378,24 +378,30 @@ def run_dasha(args, rank, world):
         dist.barrier()
     t0 = time.perf_counter()
     d.set_state_halo(H)
+    t_set = time.perf_counter() - t0
     te, ne = 0.0, 0
     for _ in range(args.steps):
         dt = d.setdt(te)
         d.stepon(te, dt, ne)
         te += dt
         ne += 1
+    d.setdt(te)   # the steps are done (the dt of the next step, read back as the loop would)
+    t1 = time.perf_counter()
     from dasha_b200 import capi
     lib = d.lib
     rc = lib.dasha_get_state(d.h, H.ctypes.data_as(capi._D), H.shape[3], H.shape[2])
     if rc:
         raise capi.DashaError(rc, "get_state")
+    t_get = time.perf_counter() - t1
     e2e_s = time.perf_counter() - t0
     e2e_s = max_over_ranks(e2e_s, dist)
     state_bytes = 8 * cells * 8
     e2e = {"value": world * cells * args.steps / e2e_s, "unit": "cell-updates/s",
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps + 8,
-           "note": "set_state from host + K x (setdt with dt read-back + stepon) + get_state to host, wall clock"}
+           "note": "set_state from host + K x (setdt with dt read-back + stepon) + setdt + get_state to host, wall clock",
+           "set_state_s": t_set, "get_state_s": t_get,
+           "set_state_GBps": state_bytes / t_set / 1e9, "get_state_GBps": state_bytes / t_get / 1e9}
 
     line = {"metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
