@@ -238,5 +238,6 @@ def gem_nccl_slab(cfg: harris.RunConfig, rank: int, world: int, nccl_id: bytes, 
     sl.set_equilibrium(rho0, b0, p0)
     if sl.params.j0_mode == 1:
         sl.set_equilibrium_current(j0)
-    sl.set_global_state(harris.gem_state(x, y, z, seed_v))
+    first, count = sl.part   # only this rank's planes of the seeded state are generated
+    sl.set_state_halo(harris.gem_state_halo(x, y, z, seed_v, planes=(first - 2, first + count + 2)))
     return sl
