@@ -92,6 +92,7 @@ SIGNATURES = {
     "dasha_group_setdt": ([C.POINTER(C.c_void_p), C.c_int, C.c_double, _D], C.c_int),
     "dasha_group_stepon": ([C.POINTER(C.c_void_p), C.c_int, C.c_double, C.c_double, C.c_int], C.c_int),
     "dasha_group_current": ([C.POINTER(C.c_void_p), C.c_int, C.POINTER(_D), C.c_long, C.c_long], C.c_int),
+    "dasha_group_diagnostics": ([C.POINTER(C.c_void_p), C.c_int, _D], C.c_int),
     "dasha_nccl_unique_id": ([C.c_void_p, C.c_int], C.c_int),
     "dasha_slab_nccl": ([_P, C.c_void_p, C.c_int], C.c_int),
     "dasha_last_error": ([_P], C.c_char_p),

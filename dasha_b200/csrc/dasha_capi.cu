@@ -661,7 +661,7 @@ int dasha_rhs(dasha_ctx* c, double t, double* xdif_f, long ld1, long ld2) {
 
 int dasha_diagnostics(dasha_ctx* c, double* out) {
     CAPI_GUARD(c);
-    SLAB_UNSUPPORTED(c, "dasha_diagnostics");
+    if (int rc = slab_single_call(c)) return rc;
     if (!out) return fail(c, DASHA_E_INVALID, "null out");
     if (!c->state_set) return fail(c, DASHA_E_STATE, "no state set");
     return engine_call(c, [&] { return c->eng->diagnostics(out); });
@@ -783,6 +783,7 @@ int dasha_slab_link(dasha_ctx* const* cs, int n) {
             auto h = std::make_unique<HaloLocal>(grp);
             h->geo = cs[s]->eng->slab_geom();
             h->geo.n = n; h->geo.s = s; h->geo.device = cs[s]->device;
+            h->geo.zfirst = cs[s]->zfirst; h->geo.mzg = cs[s]->mzg;
             hs.push_back(std::move(h));
         }
         // neighbours on different GPUs copy over NVLink: peer access both ways where the pair has it
@@ -883,6 +884,25 @@ int dasha_group_current(dasha_ctx* const* cs, int n, double* const* cur_f, long 
     return group_run(cs, n, [&](dasha_ctx* c, int s) { return engine_call(c, [&] { return c->eng->current(cur_f[s], ld1, ld2); }); });
 }
 
+int dasha_group_diagnostics(dasha_ctx* const* cs, int n, double* out) {
+    if (int rc = check_group(cs, n)) return rc;
+    if (!out) return DASHA_E_INVALID;
+    for (int s = 0; s < n; ++s)
+        if (!cs[s]->state_set) return fail(cs[s], DASHA_E_STATE, "no state set");
+    std::vector<double> part((size_t)n * DASHA_NDIAG, 0.0);
+    int rc = group_run(cs, n, [&](dasha_ctx* c, int s) {
+        return engine_call(c, [&] { return c->eng->diagnostics(part.data() + (size_t)s * DASHA_NDIAG); });
+    });
+    if (rc) return rc;
+    for (int q = 0; q < DASHA_NDIAG; ++q) out[q] = part[q];
+    for (int s = 1; s < n; ++s) {   // sums of mass, energy, flux; extrema of J
+        const double* p = part.data() + (size_t)s * DASHA_NDIAG;
+        for (int q = 0; q < 3; ++q) out[q] += p[q];
+        for (int q = 3; q < 9; q += 2) { out[q] = std::fmax(out[q], p[q]); out[q + 1] = std::fmin(out[q + 1], p[q + 1]); }
+    }
+    return DASHA_OK;
+}
+
 int dasha_nccl_unique_id(void* id, int nbytes) {
     if (!id || nbytes < (int)sizeof(ncclUniqueId)) return DASHA_E_INVALID;
     const NcclApi& a = NcclApi::get();
@@ -901,6 +921,7 @@ int dasha_slab_nccl(dasha_ctx* c, const void* id, int nbytes) {
         auto h = std::make_unique<HaloNccl>();
         h->geo = c->eng->slab_geom();
         h->geo.n = c->nslabs; h->geo.s = c->slab; h->geo.device = c->device;
+        h->geo.zfirst = c->zfirst; h->geo.mzg = c->mzg;
         ncclUniqueId u;
         std::memcpy(&u, id, sizeof(u));
         if (cudaSetDevice(c->device) != cudaSuccess) return fail(c, DASHA_E_CUDA, "cudaSetDevice failed");

@@ -1109,21 +1109,44 @@ public:
         double* jext = fl + my;
         double* out = red + nred;
         (void)guard_only;
+        // the planes this context accounts for and its planes of the central z plane(s): all of
+        // them on a whole grid; on a z-slab its own planes (and the walls it holds), and the
+        // flux where it owns the (first) central plane, the second one an own or ghost plane
+        int klo = 0, khi = mz - 1, ka, kb;
+        {
+            const int mg = halo ? halo->geo.mzg : mz, z0 = halo ? halo->geo.zfirst - 2 : 0;
+            if (halo && halo->geo.lower()) klo = 2;
+            if (halo && halo->geo.upper()) khi = mz - 3;
+            const int ga = mg % 2 ? (mg - 1) / 2 : mg / 2 - 1, gb = mg % 2 ? ga : mg / 2;
+            const bool own = ga - z0 >= klo && ga - z0 <= khi;
+            ka = own ? ga - z0 : -1;
+            kb = own ? gb - z0 : -1;
+        }
         dim3 g2(1, my, mz);
-        DASHA_LAUNCH("k_diag_rows", 8.0 * N * sizeof(T), k_diag_rows<T><<<g2, 128, 0, st>>>(g, f8(X), wx, wy, wz, P.gamma, rows));
-        k_diag_flux<T><<<my, 128, 0, st>>>(g, f8(X), wx, fl);
-        k_diag_jext<T><<<mz, 128, 0, st>>>(g, f3(curF), my / 2, jext);
+        DASHA_LAUNCH("k_diag_rows", 8.0 * N * sizeof(T),
+                     k_diag_rows<T><<<g2, 128, 0, st>>>(g, f8(X), wx, wy, wz, P.gamma, rows, klo, khi));
+        k_diag_flux<T><<<my, 128, 0, st>>>(g, f8(X), wx, fl, ka, kb);
+        k_diag_jext<T><<<mz, 128, 0, st>>>(g, f3(curF), my / 2, jext, klo, khi);
         k_diag_final<<<1, 256, 0, st>>>(rows, (long)my * mz, fl, my, jext, mz, out, flag);
         DASHA_CK(cudaGetLastError());
         return Status::ok();
     }
 
     Status diagnostics(double* outh) override {
+        hx(X + 4, 3);   // a z-slab: the current and a central plane may read B's ghost planes
         Status s = launch_diag(false);
         if (s.code) return s;
         DASHA_CK(cudaMemcpyAsync(hpin, red + nred, sizeof(double) * DASHA_NDIAG, cudaMemcpyDeviceToHost, st));
         DASHA_CK(cudaStreamSynchronize(st));
+        if (launch_err) {
+            const char* e = launch_err;
+            launch_err = nullptr;
+            return Status::err(DASHA_E_CUDA, e);
+        }
         for (int q = 0; q < DASHA_NDIAG; ++q) outh[q] = hpin[q];
+        int none = 0;
+        if (halo && halo->per_process() && !halo->reduce_diag(outh, &none))
+            return Status::err(DASHA_E_CUDA, "slab diagnostics reduction: " + halo->err);
         return Status::ok();
     }
 

@@ -61,6 +61,7 @@ inline bool slab_partition(int mz, int n, int s, SlabPart& out) {
 // The geometry of one slab's exchange: the local grid has mzl planes of sz nodes.
 struct SlabGeom {
     int n = 1, s = 0, mzl = 0, device = 0;
+    int zfirst = 2, mzg = 0;      // the first own row and the plane count of the global grid
     long sz = 0;
     size_t elem = 0;
     cudaStream_t st = nullptr;
@@ -87,6 +88,9 @@ struct Halo {
     virtual bool exchange(void* const* f, int nf) = 0;
     // the group's minimum dt and maximum flag, from this slab's values (a NaN dt wins)
     virtual bool reduce(double* dt, int* flag) = 0;
+    // the group's diagnostics from this slab's (sums of [0..2], maxima of [3], [5], [7], minima
+    // of [4], [6], [8]) and the maximum blow-up flag
+    virtual bool reduce_diag(double* out9, int* flag) = 0;
     // true when each slab runs in its own process (the entry points of one context are called
     // per process); false for a group of slabs driven by the group entry points
     virtual bool per_process() const = 0;
@@ -201,7 +205,8 @@ public:
         if (geo.upper() && cudaStreamWaitEvent(geo.st, grp->cp[s + 1], 0) != cudaSuccess) return fail("event wait failed");
         return true;
     }
-    bool reduce(double*, int*) override { return true; }   // the group entry point reduces on the host
+    bool reduce(double*, int*) override { return true; }   // the group entry points reduce on the host
+    bool reduce_diag(double*, int*) override { return true; }
 
 private:
     bool fail(const char* m) {
@@ -267,7 +272,7 @@ public:
     bool init(const ncclUniqueId& id) {
         const NcclApi& a = NcclApi::get();
         if (!a.ok()) { err = a.why; return false; }
-        if (cudaMalloc(&dbuf, 16) != cudaSuccess || cudaMallocHost(&hbuf, 16) != cudaSuccess) {
+        if (cudaMalloc(&dbuf, 10 * sizeof(double)) != cudaSuccess || cudaMallocHost(&hbuf, 10 * sizeof(double)) != cudaSuccess) {
             err = "device or pinned buffer of the dt reduction";
             return false;
         }
@@ -322,6 +327,34 @@ public:
         *dt = std::isinf(hbuf[0]) && hbuf[0] < 0 ? std::numeric_limits<double>::quiet_NaN() : hbuf[0];
         std::memcpy(&fl, hbuf + 1, sizeof(int));
         *flag = fl;
+        return true;
+    }
+
+    bool reduce_diag(double* out9, int* flag) override {
+        const NcclApi& a = NcclApi::get();
+        if (!comm) { err = "no NCCL communicator"; return false; }
+        // [0..2] summed, the maxima as they are, the minima negated (one max), the flag as a double
+        for (int q = 0; q < 3; ++q) hbuf[q] = out9[q];
+        for (int q = 0; q < 3; ++q) { hbuf[3 + q] = out9[3 + 2 * q]; hbuf[6 + q] = -out9[4 + 2 * q]; }
+        hbuf[9] = (double)*flag;
+        if (cudaMemcpyAsync(dbuf, hbuf, 10 * sizeof(double), cudaMemcpyHostToDevice, geo.st) != cudaSuccess) {
+            err = "diagnostics upload";
+            return false;
+        }
+        ncclResult_t r = a.group_start();
+        if (r == ncclSuccess) r = a.all_reduce(dbuf, dbuf, 3, ncclFloat64, ncclSum, comm, geo.st);
+        if (r == ncclSuccess) r = a.all_reduce(dbuf + 3, dbuf + 3, 7, ncclFloat64, ncclMax, comm, geo.st);
+        ncclResult_t e = a.group_end();
+        if (r != ncclSuccess) return nccl_fail("ncclAllReduce", r);
+        if (e != ncclSuccess) return nccl_fail("ncclGroupEnd", e);
+        if (cudaMemcpyAsync(hbuf, dbuf, 10 * sizeof(double), cudaMemcpyDeviceToHost, geo.st) != cudaSuccess ||
+            cudaStreamSynchronize(geo.st) != cudaSuccess) {
+            err = "diagnostics download";
+            return false;
+        }
+        for (int q = 0; q < 3; ++q) out9[q] = hbuf[q];
+        for (int q = 0; q < 3; ++q) { out9[3 + 2 * q] = hbuf[3 + q]; out9[4 + 2 * q] = -hbuf[6 + q]; }
+        *flag = hbuf[9] != 0.0;
         return true;
     }
 

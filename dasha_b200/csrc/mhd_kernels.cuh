@@ -377,11 +377,20 @@ static __global__ void k_reduce_rate(const double* partial, long n, double* out)
 
 // Diagnostics partial sums per (j,k) row: mass, energy (trapezoid weights), and the
 // per-row extrema of J on the mid-y plane; partial layout [row][5]: mass, energy, jmax/jmin
-// handled separately.
+// handled separately.  Planes klo..khi count (a z-slab's own planes and the walls it holds);
+// the others give zero.
 template <class T>
 __global__ void k_diag_rows(Geo<T> g, F8<T> x, const double* wx, const double* wy, const double* wz,
-                            double gamma, double* part) {
+                            double gamma, double* part, int klo, int khi) {
     int jj = blockIdx.y, k = blockIdx.z;
+    if (k < klo || k > khi) {
+        if (threadIdx.x == 0) {
+            long row = (long)k * gridDim.y + jj;
+            part[2 * row] = 0.;
+            part[2 * row + 1] = 0.;
+        }
+        return;
+    }
     const double r0 = g.rho0[k], bx0 = g.bx0[k], by0 = g.by0[k], bz0 = g.bz0[k], p0 = g.p0[k];
     double sm = 0., se = 0.;
     for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
@@ -412,18 +421,18 @@ __global__ void k_diag_rows(Geo<T> g, F8<T> x, const double* wx, const double* w
     }
 }
 
-// Reconnected flux partials per y row (one block per j): sum_x sqrt(Bz(z=0)^2+eps^2)*wx.
+// Reconnected flux partials per y row (one block per j): sum_x sqrt(Bz(z=0)^2+eps^2)*wx, with
+// Bz on the central plane ka (odd mz, kb = ka) or the mean of the two central planes ka, kb =
+// ka + 1 (even mz); ka < 0: a z-slab that does not own the (first) central plane.
 template <class T>
-__global__ void k_diag_flux(Geo<T> g, F8<T> x, const double* wx, double* part) {
+__global__ void k_diag_flux(Geo<T> g, F8<T> x, const double* wx, double* part, int ka, int kb) {
     int jj = blockIdx.x;
     double s = 0.;
-    for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
+    for (int i = threadIdx.x; i < g.mx && ka >= 0; i += blockDim.x) {
         double bz;
-        if (g.mz % 2) {
-            int kc = (g.mz - 1) / 2;
-            bz = g.bz0[kc] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)kc * g.sz];
+        if (ka == kb) {
+            bz = g.bz0[ka] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)ka * g.sz];
         } else {
-            int ka = g.mz / 2 - 1, kb = g.mz / 2;
             double za = g.bz0[ka] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)ka * g.sz];
             double zb = g.bz0[kb] + (double)x.f[6][(long)i + (long)jj * g.sy + (long)kb * g.sz];
             bz = 0.5 * (za + zb);
@@ -445,10 +454,10 @@ __global__ void k_diag_flux(Geo<T> g, F8<T> x, const double* wx, double* part) {
 
 // J extrema on the mid-y plane (diagn t3dsdsc.f:1199-1214): one block per k row.
 template <class T>
-__global__ void k_diag_jext(Geo<T> g, F3<T> cur, int jm, double* part) {
+__global__ void k_diag_jext(Geo<T> g, F3<T> cur, int jm, double* part, int klo, int khi) {
     int k = blockIdx.x;
     double mx[3] = {-1e300, -1e300, -1e300}, mn[3] = {1e300, 1e300, 1e300};
-    for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
+    for (int i = threadIdx.x; i < g.mx && k >= klo && k <= khi; i += blockDim.x) {
         long c = (long)i + (long)jm * g.sy + (long)k * g.sz;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {

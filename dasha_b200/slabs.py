@@ -157,6 +157,12 @@ class SlabGroup:
     def stepon(self, time: float, dt: float, nstep: int):
         self._check(self.lib.dasha_group_stepon(self._hs, len(self.slabs), time, dt, nstep))
 
+    def diagnostics(self) -> np.ndarray:
+        """capi.Dasha.diagnostics of the whole grid: sums and extrema over the slabs."""
+        out = np.zeros(capi.NDIAG)
+        self._check(self.lib.dasha_group_diagnostics(self._hs, len(self.slabs), _dp(out)))
+        return out
+
     def current(self) -> np.ndarray:
         bufs = [harris.to_halo(np.zeros((3, sl.mz, self.my, self.mx))) for sl in self.slabs]
         ptrs = (C.POINTER(C.c_double) * len(bufs))(*[_dp(b) for b in bufs])

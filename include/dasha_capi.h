@@ -251,8 +251,9 @@ int dasha_current_noalloc(const dasha_grid_c* grid, const double* db_dev, double
  * ghost planes are refreshed after every launch whose output a later launch reads at
  * z-neighbours, so every slab's own rows take the values of the one-context run, bit for bit.
  * Periodic (1,1,0) contexts only; the whole-grid calls (dasha_checkpoint, dasha_restore,
- * dasha_stream_out, dasha_m3d_write_ctx, dasha_midplane, dasha_rhs, dasha_diagnostics, the
- * adjoint, dasha_set_equilibrium_3d) return DASHA_E_UNSUPPORTED on a slab.
+ * dasha_stream_out, dasha_m3d_write_ctx, dasha_midplane, dasha_rhs, the adjoint,
+ * dasha_set_equilibrium_3d) return DASHA_E_UNSUPPORTED on a slab; dasha_diagnostics reduces
+ * over the slabs.
  *
  * dasha_slab_partition: own rows of slab `slab` (host only): count = (mz-4)/nslabs, the first
  *   (mz-4)%nslabs slabs one more; DASHA_E_INVALID unless every slab gets at least 3 rows.
@@ -284,6 +285,11 @@ int dasha_slab_link(dasha_ctx* const* ctxs, int n);
 int dasha_group_setdt(dasha_ctx* const* ctxs, int n, double time, double* dt_out);
 int dasha_group_stepon(dasha_ctx* const* ctxs, int n, double time, double dt, int nstep);
 int dasha_group_current(dasha_ctx* const* ctxs, int n, double* const* cur_f, long ld1, long ld2);
+/* dasha_diagnostics of the whole grid from a linked group: mass, energy and flux summed over the
+ * slabs' own planes (and the walls the end slabs hold; the flux from the slab that owns the
+ * first central plane), the J extrema over all of them.  A slab of a one-process-per-GPU run
+ * takes dasha_diagnostics itself (reduced over the ranks by ncclAllReduce). */
+int dasha_group_diagnostics(dasha_ctx* const* ctxs, int n, double* out);
 
 /* One process per GPU, each with one slab (the reference's one MPI rank per process): rank 0
  * makes an NCCL id (dasha_nccl_unique_id, 128 bytes), every rank receives it by its own means
