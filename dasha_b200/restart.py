@@ -139,7 +139,11 @@ def write_m3d(path: str, time: float, x: np.ndarray, y: np.ndarray, z: np.ndarra
 
 
 def write_m3d_ctx(d: "capi.Dasha", path: str, time: float):
-    """recrd3's data/m3dNNN from a GPU context, streamed (no host copy of the volume)."""
+    """recrd3's data/m3dNNN from a GPU context, streamed (no host copy of the volume); from a
+    z-slab group through the assembled state and current."""
+    if getattr(d, "host_outputs", False):
+        write_m3d(path, time, d.x, d.y, d.z, harris.to_halo(d.get_state()), harris.to_halo(d.current()))
+        return
     d._check(d.lib.dasha_m3d_write_ctx(d.h, os.fsencode(path), float(time)))
 
 
@@ -162,18 +166,24 @@ def write_step_logs(stepnm_path: str, dtlog_path: str, nstep: int, time: float, 
 
 def checkpoint(d: "capi.Dasha", directory: str, ncase: int, nstep: int, time: float, nst: int,
                max_subrecord: int = 0) -> str:
-    """recrd for a GPU context: streams the state into <directory>/mhdNNN000 (no full host copy)."""
+    """recrd for a GPU context: streams the state into <directory>/mhdNNN000 (no full host copy);
+    a z-slab group writes the same file from the assembled state."""
     path = os.path.join(directory, restart_name(nst))
+    if getattr(d, "host_outputs", False):
+        checkpoint_host(d, path, ncase, nstep, time, nst, max_subrecord)
+        return path
     d._check(d.lib.dasha_checkpoint(d.h, os.fsencode(path), ncase, nstep, float(time), nst, int(max_subrecord)))
     return path
 
 
 def restore(d: "capi.Dasha", directory: str, nst: int):
-    """readin for a GPU context: streams <directory>/mhdNNN000 into the state; returns
-    (ncase, nstep, time, nst) of the file."""
+    """readin for a GPU context: streams <directory>/mhdNNN000 into the state (a z-slab group:
+    through a host copy); returns (ncase, nstep, time, nst) of the file."""
+    path = os.path.join(directory, restart_name(nst))
+    if getattr(d, "host_outputs", False):
+        return restore_host(d, path)
     a, b, n = C.c_int(), C.c_int(), C.c_int()
     t = C.c_double()
-    path = os.path.join(directory, restart_name(nst))
     d._check(d.lib.dasha_restore(d.h, os.fsencode(path), C.byref(a), C.byref(b), C.byref(t), C.byref(n)))
     return a.value, b.value, t.value, n.value
 

@@ -15,6 +15,10 @@ diagnostics of dasha_diagnostics -- mass, energy, reconnected flux, the mid-y-pl
 extrema -- and one closing object with the reason the loop ended.
 
     python -m dasha_b200.run --config c0 --out run_c0 --nend 3 --dtime 0.5
+    python -m dasha_b200.run --config c0 --out run_c0 --nend 3 --dtime 0.5 --slabs 3   # z-slabs
+
+On z-slabs (dasha_b200/slabs.py) the loop is the same; the whole-grid files go through host
+copies of the assembled state and current.
 """
 from __future__ import annotations
 
@@ -54,7 +58,7 @@ class Outputs:
     out from its working directory (restart files and current.dat, fort.20 there; m2d, m3d and
     stepnm under data/).  Method names are the reference's routines."""
 
-    def __init__(self, d: capi.Dasha, out_dir: str):
+    def __init__(self, d, out_dir: str):
         self.d, self.dir = d, out_dir
         self.data = os.path.join(out_dir, "data")
         os.makedirs(self.data, exist_ok=True)
@@ -169,11 +173,16 @@ def main(argv=None):
     ap.add_argument("--nstop", type=int, default=RunControl.nstop)
     ap.add_argument("--restart", type=int, default=None, help="nst of the restart file to start from")
     ap.add_argument("--no-m3d", action="store_true")
+    ap.add_argument("--slabs", type=int, default=0, help="> 1: the grid as that many z-slabs in this process")
     a = ap.parse_args(argv)
     ctl = RunControl(nend=a.nend, dtime=a.dtime, dnstep=a.dnstep, nstop=a.nstop, write_m3d=not a.no_m3d)
     if a.restart is not None:
         ctl.lrstrt, ctl.nst = True, a.restart
-    d = capi.gem_context(harris.CONFIGS[a.config], a.precision)
+    if a.slabs > 1:
+        from . import slabs
+        d = slabs.gem_slab_group(harris.CONFIGS[a.config], a.slabs, a.precision)
+    else:
+        d = capi.gem_context(harris.CONFIGS[a.config], a.precision)
     try:
         r = main_loop(d, ctl, Outputs(d, a.out), log=print)
         print(f"{r.reason}: nstep {r.nstep}, time {r.time}, nst {r.nst}, {len(r.outputs)} outputs")

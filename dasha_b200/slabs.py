@@ -163,6 +163,15 @@ class SlabGroup:
         self._check(self.lib.dasha_group_diagnostics(self._hs, len(self.slabs), _dp(out)))
         return out
 
+    # the whole-grid outputs of the reference's main loop through host copies of the assembled
+    # state and current (restart.checkpoint / restore / write_m3d_ctx take this path for a group)
+    host_outputs = True
+
+    def midplane(self) -> np.ndarray:
+        """capi.Dasha.midplane: the eleven fields on the plane j = my/2, (11, mz, mx)."""
+        from . import restart
+        return restart.midplane_host(harris.to_halo(self.get_state()), harris.to_halo(self.current()))
+
     def current(self) -> np.ndarray:
         bufs = [harris.to_halo(np.zeros((3, sl.mz, self.my, self.mx))) for sl in self.slabs]
         ptrs = (C.POINTER(C.c_double) * len(bufs))(*[_dp(b) for b in bufs])

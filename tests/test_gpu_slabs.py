@@ -175,3 +175,49 @@ def test_nccl_slabs_on_several_gpus_equal_one_context(precision):
     parts = slabs.partition(SINH.mz, world)
     assert all(r[1] == d1 for r in res)
     assert np.array_equal(slabs.assemble([r[2] for r in res], parts, SINH.mz), x1)
+
+
+def test_main_loop_on_slabs_writes_the_files_of_one_context(tmp_path):
+    """The reference's main loop (dasha_b200/run.py) on 3 slabs writes the files of the
+    one-context run byte for byte: restart files, m2d, m3d, current.dat, stepnm, fort.20 (a
+    group's outputs go through host copies of the assembled state; the one context streams
+    them and also writes its exact-resume records, *.state, which a group does not)."""
+    import json
+    import os
+    from dasha_b200 import run
+    one = capi.gem_context(UNIF, 0)
+    grp = slabs.gem_slab_group(UNIF, 3, 0)
+    try:
+        dt0 = capi.gem_context(UNIF, 0).setdt(0.0)
+        res = []
+        for d, name in ((one, "one"), (grp, "slabs")):
+            ctl = run.RunControl(nend=5, dtime=4 * dt0, dnstep=2)
+            res.append(run.main_loop(d, ctl, run.Outputs(d, str(tmp_path / name))))
+        a, b = res
+        assert (a.reason, a.nstep, a.time, a.nst, a.outputs) == (b.reason, b.nstep, b.time, b.nst, b.outputs)
+
+        def files(root):
+            out = []
+            for dp, _, fs in os.walk(root):
+                out += [os.path.relpath(os.path.join(dp, f), root) for f in fs
+                        if not f.endswith(".state") and f != "run.jsonl"]
+            return sorted(out)
+
+        fa, fb = files(tmp_path / "one"), files(tmp_path / "slabs")
+        assert fa == fb and len(fa) >= 6, (fa, fb)
+        assert any(f.startswith("mhd") for f in fa)
+        for f in fa:
+            assert (tmp_path / "one" / f).read_bytes() == (tmp_path / "slabs" / f).read_bytes(), f
+        ja = [json.loads(x) for x in open(tmp_path / "one" / "run.jsonl")]
+        jb = [json.loads(x) for x in open(tmp_path / "slabs" / "run.jsonl")]
+        assert len(ja) == len(jb)
+        for x, y in zip(ja, jb):
+            assert x.keys() == y.keys()
+            for k in x:
+                if k in ("mass", "energy", "flux"):
+                    assert abs(x[k] - y[k]) <= 1e-12 * abs(x[k]), (k, x[k], y[k])
+                else:
+                    assert x[k] == y[k], (k, x[k], y[k])
+    finally:
+        grp.close()
+        one.close()
