@@ -54,7 +54,8 @@ def test_product_never_uses_the_oracle():
 def test_header_is_plain_c_and_links(tmp_path):
     """include/dasha_capi.h as a C99 caller sees it (the Fortran ISO_C_BINDING module binds the
     same symbols): compiled with -Wall -Werror -pedantic, every declared function taken by
-    address, linked against the built library, and run through the host-only file calls."""
+    address, linked against the built library, and run through the host-only file and z-slab
+    calls."""
     names = declared_functions()
     src = tmp_path / "caller.c"
     body = "\n".join(f"    p[{i}] = (void (*)(void)){n};" for i, n in enumerate(names))
@@ -73,6 +74,14 @@ int main(void) {{
     if (dasha_restart_read("{tmp_path}/mhd001000", &ncase, &nstep, &t, &nst, 12, 4, 4, x, 16, 4) != DASHA_OK) return 2;
     if (ncase != 3 || nstep != 40 || t != 1.5 || nst != 1 || x[100] != 25.0) return 3;
     if (dasha_setdt(NULL, 0.0, &t) != DASHA_E_INVALID) return 4;
+    /* the z-slab host calls: 3 slabs of 1028 planes, slab 1 exchanges 2 planes each way */
+    int first = 0, count = 0, peer[2];
+    long so[2], ro[2], n = 0;
+    if (dasha_slab_partition(1028, 3, 1, &first, &count) != DASHA_OK || first != 344 || count != 341) return 5;
+    if (dasha_slab_halo_plan(1028, 3, 1, 64, peer, so, ro, &n) != DASHA_OK) return 6;
+    if (peer[0] != 0 || peer[1] != 2 || n != 128 || so[0] != 128 || ro[0] != 0 || so[1] != 341 * 64 ||
+        ro[1] != 343 * 64) return 7;
+    if (dasha_slab_partition(10, 3, 0, &first, &count) != DASHA_E_INVALID) return 8;
     printf("%d\\n", (int)(sizeof p / sizeof p[0]));
     return 0;
 }}
