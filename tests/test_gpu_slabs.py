@@ -160,13 +160,20 @@ def test_nccl_slabs_on_several_gpus_equal_one_context(precision):
     s.close()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_nccl_rank, args=(r, world, port, SINH, precision, 4, q)) for r in range(world)]
+    procs = [ctx.Process(target=_nccl_rank, args=(r, world, port, SINH, precision, 4, q), daemon=True)
+             for r in range(world)]
     for p in procs:
         p.start()
-    res = sorted((q.get(timeout=300) for _ in procs), key=lambda r: r[0])
-    for p in procs:
-        p.join(timeout=120)
-        assert p.exitcode == 0
+    try:
+        res = sorted((q.get(timeout=300) for _ in procs), key=lambda r: r[0])
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+    finally:
+        for p in procs:   # a rank still waiting in a collective does not outlive the test
+            if p.is_alive():
+                p.kill()
+                p.join(timeout=30)
     one = capi.gem_context(SINH, precision)
     try:
         d1, x1 = run(one, 4, 8)
