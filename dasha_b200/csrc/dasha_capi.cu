@@ -821,19 +821,21 @@ static int group_run(dasha_ctx* const* cs, int n, F body) {
         if (!cs[s]->group || cs[s]->group != grp) return fail(cs[s], DASHA_E_STATE, "slabs not linked as one group");
     grp->bar.reset();
     std::vector<int> rc(n, DASHA_OK);
+    std::vector<std::thread> th;
+    bool started = true;
     try {
-        std::vector<std::thread> th;
         for (int s = 0; s < n; ++s)
             th.emplace_back([&, s] {
                 if (cudaSetDevice(cs[s]->device) != cudaSuccess) rc[s] = fail(cs[s], DASHA_E_CUDA, "cudaSetDevice failed");
                 else rc[s] = body(cs[s], s);
                 if (rc[s]) grp->bar.fail();
             });
-        for (auto& t : th) t.join();
     } catch (...) {
+        started = false;    // a thread could not start: the started ones leave the barriers
         grp->bar.fail();
-        return DASHA_E_NOMEM;
     }
+    for (auto& t : th) t.join();
+    if (!started) return DASHA_E_NOMEM;
     for (int s = 0; s < n; ++s)   // the first slab's own failure, not the others' release
         if (rc[s] && cs[s]->halo && cs[s]->err.find("halo exchange") == std::string::npos) return rc[s];
     for (int s = 0; s < n; ++s)
