@@ -275,10 +275,12 @@ int dasha_slab_rows(dasha_ctx* ctx, int* first, int* count, int* mz_local);
 
 /* One process, every slab (one per GPU, or several on one GPU): dasha_slab_link joins
  * ctxs[0..n-1] (slab s at ctxs[s]) into a group whose ghost planes are copied between the
- * slabs' memories (cudaMemcpyPeerAsync).  A linked group steps through the dasha_group_*
- * calls, which run every slab in its own host thread: dasha_group_setdt returns the smallest
- * dt of the slabs (the guards of dasha_setdt apply), dasha_group_stepon is one RK4 step of the
- * whole grid (synchronous), dasha_group_current writes slab s's current to cur_f[s].  The
+ * slabs' memories (cudaMemcpyPeerAsync, ordered against the neighbours' launches by events, and
+ * peer access enabled between neighbouring GPUs).  A linked group steps through the
+ * dasha_group_* calls, which run every slab in its own host thread: dasha_group_setdt returns
+ * the smallest dt of the slabs (the guards of dasha_setdt apply; it synchronises),
+ * dasha_group_stepon enqueues one RK4 step of the whole grid, dasha_group_current writes slab
+ * s's current to cur_f[s].  The
  * single-context dasha_setdt / dasha_stepon / dasha_current of a linked slab return
  * DASHA_E_STATE; a slab that is joined to nothing also returns DASHA_E_STATE there. */
 int dasha_slab_link(dasha_ctx* const* ctxs, int n);
