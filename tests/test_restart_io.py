@@ -369,3 +369,41 @@ def test_bad_arguments_rejected(tmp_path):
     i, t = ctypes.c_int(), ctypes.c_double()
     assert lib.dasha_restore(None, b"x", ctypes.byref(i), ctypes.byref(i), ctypes.byref(t), ctypes.byref(i)) == capi.E_INVALID
     assert lib.dasha_restart_write(str(tmp_path / "no" / "dir").encode(), 0, 0, 0.0, 0, 4, 4, 4, capi._dp(H), 8, 4, 0) == capi.E_INVALID
+
+
+class _HostGroup:
+    """A stand-in for a z-slab group (dasha_b200/slabs.py SlabGroup): the whole-grid state and
+    current as host arrays, and the marker that sends the output helpers down the host path."""
+    host_outputs = True
+
+    def __init__(self, mx, my, mz):
+        self.x, self.y, self.z = harris.make_grid(mx, my, mz, True)
+        self.mx, self.my, self.mz = mx, my, mz
+        self.X, self.cur = _state(mx, my, mz, seed=11)
+
+    def get_state(self):
+        return self.X.copy()
+
+    def set_state(self, X):
+        self.X = np.array(X)
+
+    def current(self):
+        return self.cur.copy()
+
+
+def test_group_outputs_through_host_copies(tmp_path):
+    """restart.checkpoint / restore / write_m3d_ctx on a slab group write and read the files the
+    host helpers write for the same arrays."""
+    g = _HostGroup(12, 4, 9)
+    path = restart.checkpoint(g, str(tmp_path), 2, 30, 1.25, 4)
+    ref = tmp_path / "ref"
+    restart.write_restart(str(ref), 2, 30, 1.25, 4, restart.restart_array(g.X))
+    assert path.endswith("mhd004000") and open(path, "rb").read() == ref.read_bytes()
+    X0 = g.X.copy()
+    g.X = np.zeros_like(g.X)
+    assert restart.restore(g, str(tmp_path), 4) == (2, 30, 1.25, 4)
+    # the file holds v = (rho v)/rho; the state comes back as rho v to within rounding
+    np.testing.assert_allclose(g.X, X0, rtol=1e-14, atol=1e-14)
+    restart.write_m3d_ctx(g, str(tmp_path / "m3d_group"), 1.25)
+    restart.write_m3d(str(tmp_path / "m3d_host"), 1.25, g.x, g.y, g.z, harris.to_halo(g.X), harris.to_halo(g.cur))
+    assert (tmp_path / "m3d_group").read_bytes() == (tmp_path / "m3d_host").read_bytes()
